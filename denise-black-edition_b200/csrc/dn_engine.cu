@@ -1,0 +1,1287 @@
+// Engine of the B200 P-SV propagator: device-resident models and shots,
+// batched time loop (one launch per operation for all shots of a batch,
+// captured in a CUDA graph), plain single-shot loop, gradient assembly and the
+// C ABI declared in include/denise_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dn_internal.h"
+#include "dn_kernels.cuh"
+
+using namespace dn;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local char g_err[512] = "";
+
+extern "C" int dn_fail(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+extern "C" const char *dn_last_error(void) { return g_err; }
+
+extern "C" int dn_version(int *major, int *minor)
+{
+    if (major) *major = DN_VERSION_MAJOR;
+    if (minor) *minor = DN_VERSION_MINOR;
+    return DN_OK;
+}
+
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            return dn_fail(e_ == cudaErrorMemoryAllocation ? DN_ENOMEM : DN_EDEVICE, "%s: %s (%s:%d)", \
+                           #call, cudaGetErrorString(e_), __FILE__, __LINE__);                     \
+        }                                                                                          \
+    } while (0)
+
+extern "C" int dn_device_count(int *count)
+{
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) n = 0;
+    if (count) *count = n;
+    return DN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// per-device state: one stream, a zero step counter for direct launches
+// ---------------------------------------------------------------------------
+struct DevState {
+    cudaStream_t stream = nullptr;
+    int *d_zero = nullptr;     // 0, used as the step base of direct launches
+    int *d_step = nullptr;     // step base advanced by graph replays
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+static std::mutex g_dev_mu;
+static std::map<int, DevState> g_dev;
+static thread_local double g_last_ms = 0.0;
+static thread_local long long g_last_launches = 0;
+
+static int dev_state(int device, DevState **out)
+{
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    auto it = g_dev.find(device);
+    if (it == g_dev.end()) {
+        DevState st;
+        CU(cudaSetDevice(device));
+        CU(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
+        CU(cudaMalloc(&st.d_zero, 2 * sizeof(int)));
+        CU(cudaMemset(st.d_zero, 0, 2 * sizeof(int)));
+        st.d_step = st.d_zero + 1;
+        CU(cudaEventCreate(&st.ev0));
+        CU(cudaEventCreate(&st.ev1));
+        it = g_dev.emplace(device, st).first;
+    }
+    *out = &it->second;
+    return DN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// model / shot objects
+// ---------------------------------------------------------------------------
+struct Layout {
+    int nx, ny, pitch, rows;
+    long long plane;   // floats per padded field
+    long long origin;  // offset of the origin pointer inside a padded field
+};
+
+static Layout make_layout(int nx, int ny)
+{
+    Layout L;
+    L.nx = nx;
+    L.ny = ny;
+    L.pitch = ((nx + 2 * DN_HX) + 31) / 32 * 32;
+    L.rows = ny + 2 * DN_HZ;
+    L.plane = (long long)L.pitch * L.rows;
+    L.origin = (long long)(DN_HZ - 1) * L.pitch + (DN_HX - 1);
+    return L;
+}
+
+enum { MF_RIP, MF_RJP, MF_UIPJP, MF_MU, MF_LAM, MF_RHO, MF_VP, MF_VS, MF_GMUSS, MF_GLAMSS,
+       MF_CMUIPJP, MF_CTAUSIPJP, MF_CMU, MF_CTAUS, MF_CPI, MF_CTAUP, MF_COUNT };
+
+struct dn_model {
+    dn_params p;
+    int device;
+    float hc[7];
+    Layout lay;
+    int nfields;
+    float *dmat = nullptr;         // nfields padded planes
+    float *dpml = nullptr;         // 12 CPML vectors of 2 fw
+    float *dsurf = nullptr;        // visco surface constants: 4 x nx
+    float eta[DN_MAX_L], bip[DN_MAX_L], cip[DN_MAX_L], s_bjm[DN_MAX_L];
+    void *dgrad = nullptr;         // stacked gradient: 3 x nx*ny (float or double), row-major [j][i]
+    int grad64;
+    int nshots = 0;
+    float *field(int f) const { return dmat + (long long)f * lay.plane + lay.origin; }
+};
+
+struct dn_shot {
+    dn_model *m;
+    dn_params p;                   // copy of the model parameters at creation
+    // acquisition (host copies)
+    int nsrc, ntr;
+    std::vector<int> src_i, src_j, src_type, rec_i, rec_j;
+    std::vector<float> src_azi, signals;
+    int quelltyp_last;
+    // device state
+    char *dstate = nullptr;        // fields + psi + rpq, zeroed per run
+    size_t state_bytes = 0;
+    float *f[7];                   // vx vy sxx syy sxy vxp1 vyp1 (origin pointers)
+    float *r = nullptr, *pmv = nullptr, *q = nullptr;
+    float *psi[9];
+    char *dacq = nullptr;          // source / receiver tables + signals
+    int nsrc_cells;
+    int *d_cell_i, *d_cell_j, *d_cell_start, *d_cell_count, *d_perm, *d_src_type, *d_rec_i, *d_rec_j;
+    double *d_nsin, *d_cos;
+    float *d_signals;
+    float *d_sec = nullptr;        // [ncomp=5][nt][ntr]
+    float *d_res = nullptr;        // [3][ntr][nt]
+    int has_res[3] = {0, 0, 0};
+    void *d_snap = nullptr;
+    float *d_snap_scale = nullptr;
+    int nsnap = 0, zch = 16, bx = 128, tiles_x = 0, tiles = 0;
+    void *d_acc = nullptr;         // wc, wcu, wcrho (float or double) + Ws, Wr
+    int acc64;
+    int *d_flag = nullptr;
+    int stored = 0;                // a mode-0 run with snapshots completed
+    int correlated = 0;            // a mode-1 run completed
+};
+
+static size_t snap_elem_bytes(int prec) { return prec == DN_SNAP_F32 ? 4 : 2; }
+
+static int validate_params(const dn_params *p)
+{
+    if (!p) return dn_fail(DN_EINVAL, "null params");
+    if (p->nx < 1 || p->ny < 1) return dn_fail(DN_EINVAL, "NX and NY must be positive (got %d x %d)", p->nx, p->ny);
+    if (p->fdorder < 2 || p->fdorder > 12 || (p->fdorder & 1))
+        return dn_fail(DN_EINVAL, "Error in selection of FD coefficients: wrong FDORDER (%d)", p->fdorder);
+    if (p->maxrelerror < 0 || p->maxrelerror > 4)
+        return dn_fail(DN_EINVAL, "Error in selection of FD coefficients: wrong choice of maximum relative error (%d)",
+                       p->maxrelerror);
+    if (p->nt < 2) return dn_fail(DN_EINVAL, "NT must be at least 2 (got %d)", p->nt);
+    if (!(p->dt > 0.0f) || !(p->dh > 0.0f)) return dn_fail(DN_EINVAL, "DT and DH must be positive");
+    if (p->fw < 0) return dn_fail(DN_EINVAL, "FW must be >= 0");
+    if (p->boundary != 0) return dn_fail(DN_ENOTSUP, "BOUNDARY=%d (periodic edges) is not built; use 0", p->boundary);
+    if (p->L < 0 || p->L > DN_MAX_L) return dn_fail(DN_EINVAL, "L must be in 0..%d", DN_MAX_L);
+    if (p->invmat1 != 1) return dn_fail(DN_ENOTSUP, "INVMAT1=%d is not built; use 1 (vp, vs, rho)", p->invmat1);
+    if (p->grad_form != 1) return dn_fail(DN_ENOTSUP, "GRAD_FORM=%d is not built; use 1", p->grad_form);
+    if (p->store_snapshots && p->dtinv < 1) return dn_fail(DN_EINVAL, "DTINV must be >= 1");
+    if (p->snap_precision < 0 || p->snap_precision > 2) return dn_fail(DN_EINVAL, "bad snapshot precision");
+    if (p->seismo < 0 || p->seismo > 4) return dn_fail(DN_EINVAL, "SEISMO must be 0..4");
+    if (p->L > 0 && !(p->ts > 0.0f) && p->free_surf)
+        return dn_fail(DN_EINVAL, "TS (1 / max source frequency) is needed by the viscoelastic free surface");
+    for (int l = 0; l < p->L; l++)
+        if (!(p->fl[l] > 0.0f)) return dn_fail(DN_EINVAL, "relaxation frequency FL[%d] must be positive", l + 1);
+    return DN_OK;
+}
+
+static void file_to_padded(const Layout &L, const float *file, std::vector<float> &pad, long long plane_off)
+{
+    for (int i = 1; i <= L.nx; i++)
+        for (int j = 1; j <= L.ny; j++)
+            pad[plane_off + L.origin + (long long)j * L.pitch + i] = file[(size_t)(i - 1) * L.ny + (j - 1)];
+}
+
+extern "C" int dn_model_footprint(const dn_params *p, size_t *bytes)
+{
+    int st = validate_params(p);
+    if (st) return st;
+    Layout L = make_layout(p->nx, p->ny);
+    int nf = p->L > 0 ? MF_COUNT : MF_CMUIPJP;
+    size_t b = (size_t)nf * L.plane * 4 + 12 * 2 * (size_t)std::max(p->fw, 1) * 4 + 4 * (size_t)p->nx * 4;
+    b += 3 * (size_t)p->nx * p->ny * (p->grad_accum == DN_ACC_F64 ? 8 : 4);
+    if (bytes) *bytes = b;
+    return DN_OK;
+}
+
+extern "C" int dn_model_create(const dn_params *p, const float *vp, const float *vs, const float *rho,
+                               const float *qp, const float *qs, int device, dn_model **out)
+{
+    if (!out) return dn_fail(DN_EINVAL, "dn_model_create: null out");
+    *out = nullptr;
+    int st = validate_params(p);
+    if (st) return st;
+    if (!vp || !vs || !rho) return dn_fail(DN_EINVAL, "dn_model_create: vp, vs and rho are required");
+    if (p->L > 0 && p->honor_q && (!qp || !qs)) return dn_fail(DN_EINVAL, "dn_model_create: honor_q needs qp and qs");
+    dn_model *m = new dn_model();
+    m->p = *p;
+    m->device = device;
+    m->lay = make_layout(p->nx, p->ny);
+    m->nfields = p->L > 0 ? MF_COUNT : MF_CMUIPJP;
+    m->grad64 = p->grad_accum == DN_ACC_F64;
+    st = dn_holbergcoeff(p->fdorder, p->maxrelerror, m->hc);
+    if (st) {
+        delete m;
+        return st;
+    }
+    const Layout &L = m->lay;
+    const size_t n = (size_t)p->nx * p->ny;
+    std::vector<float> host((size_t)m->nfields * L.plane, 0.0f);
+    std::vector<float> uipjp(n), rip(n), rjp(n), mu(n), lam(n), gmuss(n), glamss(n);
+    st = dn_average_materials(p, vp, vs, rho, uipjp.data(), rip.data(), rjp.data());
+    if (st) {
+        delete m;
+        return st;
+    }
+    for (size_t k = 0; k < n; k++) {
+        // update_s_elastic_PML_PSV.c:442-444 and psv.c:333-334 (float, with the 2.0 promotion)
+        float u = vs[k], pi = vp[k], r = rho[k];
+        mu[k] = r * u * u;
+        lam[k] = r * ((pi * pi) - 2 * u * u);
+        float muss = r * u * u;
+        gmuss[k] = muss;
+        glamss[k] = (float)((double)(r * pi * pi) - 2.0 * (double)muss);
+    }
+    file_to_padded(L, rip.data(), host, MF_RIP * L.plane);
+    file_to_padded(L, rjp.data(), host, MF_RJP * L.plane);
+    file_to_padded(L, uipjp.data(), host, MF_UIPJP * L.plane);
+    file_to_padded(L, mu.data(), host, MF_MU * L.plane);
+    file_to_padded(L, lam.data(), host, MF_LAM * L.plane);
+    file_to_padded(L, rho, host, MF_RHO * L.plane);
+    file_to_padded(L, vp, host, MF_VP * L.plane);
+    file_to_padded(L, vs, host, MF_VS * L.plane);
+    file_to_padded(L, gmuss.data(), host, MF_GMUSS * L.plane);
+    file_to_padded(L, glamss.data(), host, MF_GLAMSS * L.plane);
+    std::vector<float> surf;
+    if (p->L > 0) {
+        std::vector<float> a(n), b(n), c(n), d(n), e(n), f(n);
+        st = dn_visc_cell_factors(p, vp, vs, rho, qp, qs, a.data(), b.data(), c.data(), d.data(), e.data(), f.data());
+        if (st) {
+            delete m;
+            return st;
+        }
+        file_to_padded(L, a.data(), host, MF_CMUIPJP * L.plane);
+        file_to_padded(L, b.data(), host, MF_CTAUSIPJP * L.plane);
+        file_to_padded(L, c.data(), host, MF_CMU * L.plane);
+        file_to_padded(L, d.data(), host, MF_CTAUS * L.plane);
+        file_to_padded(L, e.data(), host, MF_CPI * L.plane);
+        file_to_padded(L, f.data(), host, MF_CTAUP * L.plane);
+        float eta[DN_MAX_L];
+        dn_visc_eta(p, eta, nullptr);
+        for (int l = 0; l < p->L; l++) {
+            m->eta[l] = eta[l];
+            m->bip[l] = 1.0 / (1.0 + (eta[l] * 0.5));
+            m->cip[l] = 1.0 - (eta[l] * 0.5);
+            m->s_bjm[l] = eta[l] / (1.0 + (eta[l] * 0.5));   // surface_visc_PML_PSV.c:158
+        }
+        // surface row j = 1 (surface_visc_PML_PSV.c:34-49, 136-143): ws = 2 pi / TS
+        surf.assign(4 * (size_t)p->nx, 0.0f);
+        if (p->free_surf) {
+            float ws = 2.0 * 3.141592653589793 * (1.0 / p->ts);
+            float sumu = dn_visc_sum(p, ws), sumpi = sumu;
+            for (int i = 1; i <= p->nx; i++) {
+                size_t o = (size_t)(i - 1) * p->ny;   // j = 1
+                float qsv = p->honor_q ? qs[o] : 30.0f, qpv = p->honor_q ? qp[o] : 30.0f;
+                float taus = dn_visc_tau_from_q(qsv), taup = dn_visc_tau_from_q(qpv);
+                float pu = vs[o], ppi = vp[o], prho = rho[o];
+                float smu = (pu * pu * prho) / (1.0 + sumu * taus);
+                float spi = (ppi * ppi * prho) / (1.0 + sumpi * taup);
+                surf[0 * p->nx + i - 1] = smu;
+                surf[1 * p->nx + i - 1] = spi;
+                surf[2 * p->nx + i - 1] = taus;
+                surf[3 * p->nx + i - 1] = taup;
+            }
+        }
+    }
+    std::vector<float> pml(12 * 2 * (size_t)std::max(p->fw, 1), 0.0f);
+    if (p->fw > 0) {
+        const size_t w = 2 * (size_t)p->fw;
+        std::vector<float> scratch(8 * w);
+        dn_pml P;
+        P.d_x = &scratch[0 * w];
+        P.alpha_prime_x = &scratch[1 * w];
+        P.d_x_half = &scratch[2 * w];
+        P.alpha_prime_x_half = &scratch[3 * w];
+        P.d_y = &scratch[4 * w];
+        P.alpha_prime_y = &scratch[5 * w];
+        P.d_y_half = &scratch[6 * w];
+        P.alpha_prime_y_half = &scratch[7 * w];
+        P.K_x = &pml[0 * w];
+        P.a_x = &pml[1 * w];
+        P.b_x = &pml[2 * w];
+        P.K_x_half = &pml[3 * w];
+        P.a_x_half = &pml[4 * w];
+        P.b_x_half = &pml[5 * w];
+        P.K_y = &pml[6 * w];
+        P.a_y = &pml[7 * w];
+        P.b_y = &pml[8 * w];
+        P.K_y_half = &pml[9 * w];
+        P.a_y_half = &pml[10 * w];
+        P.b_y_half = &pml[11 * w];
+        st = dn_pml_profiles(p, &P);
+        if (st) {
+            delete m;
+            return st;
+        }
+    }
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete m;
+        return dn_fail(DN_EDEVICE, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+    }
+    size_t gbytes = 3 * n * (m->grad64 ? 8 : 4);
+    if (cudaMalloc(&m->dmat, host.size() * 4) != cudaSuccess || cudaMalloc(&m->dpml, pml.size() * 4) != cudaSuccess ||
+        cudaMalloc(&m->dgrad, gbytes) != cudaSuccess ||
+        (!surf.empty() && cudaMalloc(&m->dsurf, surf.size() * 4) != cudaSuccess)) {
+        cudaGetLastError();
+        dn_model_destroy(m);
+        return dn_fail(DN_ENOMEM, "dn_model_create: device allocation failed");
+    }
+    if (cudaMemcpy(m->dmat, host.data(), host.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(m->dpml, pml.data(), pml.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(m->dgrad, 0, gbytes) != cudaSuccess ||
+        (!surf.empty() && cudaMemcpy(m->dsurf, surf.data(), surf.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)) {
+        dn_model_destroy(m);
+        return dn_fail(DN_EDEVICE, "dn_model_create: upload failed");
+    }
+    *out = m;
+    return DN_OK;
+}
+
+extern "C" int dn_model_destroy(dn_model *m)
+{
+    if (!m) return DN_OK;
+    cudaSetDevice(m->device);
+    cudaFree(m->dmat);
+    cudaFree(m->dpml);
+    cudaFree(m->dsurf);
+    cudaFree(m->dgrad);
+    delete m;
+    return DN_OK;
+}
+
+extern "C" int dn_model_params(const dn_model *m, dn_params *out)
+{
+    if (!m || !out) return dn_fail(DN_EINVAL, "null argument");
+    *out = m->p;
+    return DN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// shots
+// ---------------------------------------------------------------------------
+static void tile_shape(const dn_params *p, int &bx, int &zch)
+{
+    // Tile shapes measured on B200 per grid; small grids favour short tiles
+    // (more CTAs), large ones long register streams.
+    bx = 128;
+    long long cells = (long long)p->nx * p->ny;
+    zch = cells < (1 << 19) ? 8 : 32;
+    const char *ev = getenv("DN_TILE");
+    if (ev) {
+        int a = 0, b = 0;
+        if (sscanf(ev, "%dx%d", &a, &b) == 2 && a >= 32 && a <= 256 && (a % 32) == 0 && b >= 1 && b <= 256) {
+            bx = a;
+            zch = b;
+        }
+    }
+}
+
+static int shot_counts(const dn_params *p, int bx, int zch, int &tiles_x, int &tiles, int &nsnap)
+{
+    tiles_x = (p->nx + bx - 1) / bx;
+    tiles = tiles_x * ((p->ny + zch - 1) / zch);
+    nsnap = p->store_snapshots ? (int)ceil((float)p->nt / (float)p->dtinv) : 0;   // FD_PSV.c:82
+    return DN_OK;
+}
+
+extern "C" int dn_shot_footprint(const dn_params *p, int ntr, int store, size_t *bytes)
+{
+    int st = validate_params(p);
+    if (st) return st;
+    Layout L = make_layout(p->nx, p->ny);
+    int bx, zch, tx, tiles, nsnap;
+    tile_shape(p, bx, zch);
+    dn_params q = *p;
+    q.store_snapshots = store;
+    shot_counts(&q, bx, zch, tx, tiles, nsnap);
+    size_t b = (size_t)(7 + 3 * p->L) * L.plane * 4;
+    b += (size_t)9 * 2 * std::max(p->fw, 1) * std::max(p->nx, p->ny) * 4;
+    b += (size_t)5 * p->nt * std::max(ntr, 1) * 4 + (size_t)3 * p->nt * std::max(ntr, 1) * 4;
+    b += (size_t)nsnap * 5 * tiles * bx * zch * snap_elem_bytes(p->snap_precision);
+    b += (size_t)p->nx * p->ny * (3 * (p->grad_accum == DN_ACC_F64 ? 8 : 4) + 8);
+    if (bytes) *bytes = b;
+    return DN_OK;
+}
+
+template <typename T> static T *carve(char *&cur, size_t count)
+{
+    T *r = (T *)cur;
+    size_t b = (count * sizeof(T) + 255) & ~(size_t)255;
+    cur += b;
+    return r;
+}
+static size_t carve_size(size_t count, size_t elem) { return (count * elem + 255) & ~(size_t)255; }
+
+extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
+{
+    if (!m || !acq || !out) return dn_fail(DN_EINVAL, "dn_shot_create: null argument");
+    *out = nullptr;
+    const dn_params *p = &m->p;
+    if (acq->nsrc < 0 || acq->ntr < 0) return dn_fail(DN_EINVAL, "negative source/receiver count");
+    if (acq->nsrc > 0 && (!acq->src_i || !acq->src_j || !acq->signals))
+        return dn_fail(DN_EINVAL, "sources need src_i, src_j and signals");
+    if (acq->ntr > 0 && (!acq->rec_i || !acq->rec_j)) return dn_fail(DN_EINVAL, "receivers need rec_i and rec_j");
+    for (int l = 0; l < acq->nsrc; l++) {
+        if (acq->src_i[l] < 1 || acq->src_i[l] > p->nx || acq->src_j[l] < 1 || acq->src_j[l] > p->ny)
+            return dn_fail(DN_EINVAL, "source %d at grid point (%d,%d) lies outside the %d x %d grid", l + 1,
+                           acq->src_i[l], acq->src_j[l], p->nx, p->ny);
+        int ty = acq->src_type ? acq->src_type[l] : 1;
+        if (ty < 1 || ty > 5) return dn_fail(DN_ENOTSUP, "source type QUELLTYP=%d is not built", ty);
+        if (ty == 5 && (acq->src_i[l] < 2 || acq->src_j[l] < 2))
+            return dn_fail(DN_EINVAL, "moment-tensor source %d needs i, j >= 2", l + 1);
+    }
+    for (int l = 0; l < acq->ntr; l++)
+        if (acq->rec_i[l] < 1 || acq->rec_i[l] > p->nx || acq->rec_j[l] < 1 || acq->rec_j[l] > p->ny)
+            return dn_fail(DN_EINVAL, "receiver %d at grid point (%d,%d) lies outside the grid", l + 1, acq->rec_i[l],
+                           acq->rec_j[l]);
+    dn_shot *s = new dn_shot();
+    s->m = m;
+    s->p = *p;
+    s->nsrc = acq->nsrc;
+    s->ntr = acq->ntr;
+    s->src_i.assign(acq->src_i, acq->src_i + acq->nsrc);
+    s->src_j.assign(acq->src_j, acq->src_j + acq->nsrc);
+    s->src_type.resize(acq->nsrc);
+    s->src_azi.resize(acq->nsrc);
+    for (int l = 0; l < acq->nsrc; l++) {
+        s->src_type[l] = acq->src_type ? acq->src_type[l] : 1;
+        s->src_azi[l] = acq->src_azi ? acq->src_azi[l] : 0.0f;
+    }
+    s->signals.assign(acq->signals, acq->signals + (size_t)acq->nsrc * p->nt);
+    s->rec_i.assign(acq->rec_i, acq->rec_i + acq->ntr);
+    s->rec_j.assign(acq->rec_j, acq->rec_j + acq->ntr);
+    s->quelltyp_last = acq->nsrc > 0 ? s->src_type[acq->nsrc - 1] : 0;
+    tile_shape(p, s->bx, s->zch);
+    shot_counts(p, s->bx, s->zch, s->tiles_x, s->tiles, s->nsnap);
+    s->acc64 = p->grad_accum == DN_ACC_F64;
+
+    // unique source cells, list order kept inside a cell
+    std::vector<int> perm(acq->nsrc);
+    for (int l = 0; l < acq->nsrc; l++) perm[l] = l;
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
+        if (s->src_j[a] != s->src_j[b]) return s->src_j[a] < s->src_j[b];
+        return s->src_i[a] < s->src_i[b];
+    });
+    std::vector<int> ci, cj, cs, cc;
+    for (int k = 0; k < acq->nsrc; k++) {
+        int l = perm[k];
+        if (ci.empty() || ci.back() != s->src_i[l] || cj.back() != s->src_j[l]) {
+            ci.push_back(s->src_i[l]);
+            cj.push_back(s->src_j[l]);
+            cs.push_back(k);
+            cc.push_back(0);
+        }
+        cc.back()++;
+    }
+    s->nsrc_cells = (int)ci.size();
+    std::vector<double> nsin(acq->nsrc), cosv(acq->nsrc);
+    for (int l = 0; l < acq->nsrc; l++) {
+        float azi_rad = s->src_azi[l] * 3.141592653589793 / 180;   // update_v_PML_PSV.c:743
+        nsin[l] = -sin(azi_rad);
+        cosv[l] = cos(azi_rad);
+    }
+
+    const Layout &L = m->lay;
+    const int fw = p->fw;
+    const size_t xf = (size_t)p->ny * 2 * std::max(fw, 1), zf = (size_t)2 * std::max(fw, 1) * p->nx;
+    s->state_bytes = carve_size(L.plane, 4) * (7 + 3 * p->L) + carve_size(xf, 4) * 5 + carve_size(zf, 4) * 4;
+    size_t acq_bytes = carve_size(std::max((size_t)s->nsrc_cells, (size_t)1), 4) * 4 +
+                       carve_size(std::max((size_t)acq->nsrc, (size_t)1), 4) * 2 +
+                       carve_size(std::max((size_t)acq->ntr, (size_t)1), 4) * 2 +
+                       carve_size(std::max((size_t)acq->nsrc, (size_t)1), 8) * 2 +
+                       carve_size(std::max((size_t)acq->nsrc * p->nt, (size_t)1), 4) + carve_size(1, 4);
+    const size_t sec_n = (size_t)5 * p->nt * std::max(acq->ntr, 1);
+    const size_t res_n = (size_t)3 * std::max(acq->ntr, 1) * p->nt;
+    const size_t ncell = (size_t)p->nx * p->ny;
+    const size_t acc_bytes = carve_size(ncell, s->acc64 ? 8 : 4) * 3 + carve_size(ncell, 4) * 2;
+    const size_t snap_n = (size_t)s->nsnap * 5 * s->tiles * s->bx * s->zch;
+
+    cudaError_t e = cudaSetDevice(m->device);
+    if (e != cudaSuccess) {
+        delete s;
+        return dn_fail(DN_EDEVICE, "cudaSetDevice: %s", cudaGetErrorString(e));
+    }
+    bool ok = cudaMalloc(&s->dstate, s->state_bytes) == cudaSuccess && cudaMalloc(&s->dacq, acq_bytes) == cudaSuccess &&
+              cudaMalloc(&s->d_sec, sec_n * 4) == cudaSuccess && cudaMalloc(&s->d_res, res_n * 4) == cudaSuccess &&
+              cudaMalloc(&s->d_acc, acc_bytes) == cudaSuccess;
+    if (ok && s->nsnap > 0) {
+        ok = cudaMalloc(&s->d_snap, std::max(snap_n, (size_t)1) * snap_elem_bytes(p->snap_precision)) == cudaSuccess &&
+             cudaMalloc(&s->d_snap_scale, std::max((size_t)s->nsnap * 5 * s->tiles, (size_t)1) * 4) == cudaSuccess;
+    }
+    if (!ok) {
+        cudaGetLastError();
+        dn_shot_destroy(s);
+        return dn_fail(DN_ENOMEM, "dn_shot_create: device allocation failed (%.1f MB of snapshots)",
+                       snap_n * snap_elem_bytes(p->snap_precision) / 1e6);
+    }
+    char *cur = s->dstate;
+    for (int k = 0; k < 7; k++) s->f[k] = carve<float>(cur, L.plane) + L.origin;
+    if (p->L > 0) {
+        s->r = carve<float>(cur, L.plane * p->L) + L.origin;
+        s->pmv = carve<float>(cur, L.plane * p->L) + L.origin;
+        s->q = carve<float>(cur, L.plane * p->L) + L.origin;
+        // carve reserved one plane per array above; the remaining planes follow contiguously
+    }
+    for (int k = 0; k < 5; k++) s->psi[k] = carve<float>(cur, xf);
+    for (int k = 5; k < 9; k++) s->psi[k] = carve<float>(cur, zf);
+    // (the visco planes were carved with their full size)
+    char *ac = s->dacq;
+    s->d_cell_i = carve<int>(ac, std::max(s->nsrc_cells, 1));
+    s->d_cell_j = carve<int>(ac, std::max(s->nsrc_cells, 1));
+    s->d_cell_start = carve<int>(ac, std::max(s->nsrc_cells, 1));
+    s->d_cell_count = carve<int>(ac, std::max(s->nsrc_cells, 1));
+    s->d_perm = carve<int>(ac, std::max(acq->nsrc, 1));
+    s->d_src_type = carve<int>(ac, std::max(acq->nsrc, 1));
+    s->d_rec_i = carve<int>(ac, std::max(acq->ntr, 1));
+    s->d_rec_j = carve<int>(ac, std::max(acq->ntr, 1));
+    s->d_nsin = carve<double>(ac, std::max(acq->nsrc, 1));
+    s->d_cos = carve<double>(ac, std::max(acq->nsrc, 1));
+    s->d_signals = carve<float>(ac, std::max((size_t)acq->nsrc * p->nt, (size_t)1));
+    s->d_flag = carve<int>(ac, 1);
+    ok = true;
+    auto up = [&](void *dst, const void *src, size_t b) {
+        if (b && ok) ok = cudaMemcpy(dst, src, b, cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    up(s->d_cell_i, ci.data(), ci.size() * 4);
+    up(s->d_cell_j, cj.data(), cj.size() * 4);
+    up(s->d_cell_start, cs.data(), cs.size() * 4);
+    up(s->d_cell_count, cc.data(), cc.size() * 4);
+    up(s->d_perm, perm.data(), perm.size() * 4);
+    up(s->d_src_type, s->src_type.data(), s->src_type.size() * 4);
+    up(s->d_rec_i, s->rec_i.data(), s->rec_i.size() * 4);
+    up(s->d_rec_j, s->rec_j.data(), s->rec_j.size() * 4);
+    up(s->d_nsin, nsin.data(), nsin.size() * 8);
+    up(s->d_cos, cosv.data(), cosv.size() * 8);
+    up(s->d_signals, s->signals.data(), s->signals.size() * 4);
+    if (ok) ok = cudaMemset(s->d_flag, 0, 4) == cudaSuccess && cudaMemset(s->d_sec, 0, sec_n * 4) == cudaSuccess &&
+                 cudaMemset(s->d_res, 0, res_n * 4) == cudaSuccess && cudaMemset(s->d_acc, 0, acc_bytes) == cudaSuccess &&
+                 cudaMemset(s->dstate, 0, s->state_bytes) == cudaSuccess;
+    if (!ok) {
+        dn_shot_destroy(s);
+        return dn_fail(DN_EDEVICE, "dn_shot_create: upload failed");
+    }
+    m->nshots++;
+    *out = s;
+    return DN_OK;
+}
+
+static void forget_shot(const dn_shot *s);
+
+extern "C" int dn_shot_destroy(dn_shot *s)
+{
+    if (!s) return DN_OK;
+    forget_shot(s);
+    cudaSetDevice(s->m->device);
+    cudaFree(s->dstate);
+    cudaFree(s->dacq);
+    cudaFree(s->d_sec);
+    cudaFree(s->d_res);
+    cudaFree(s->d_snap);
+    cudaFree(s->d_snap_scale);
+    cudaFree(s->d_acc);
+    s->m->nshots--;
+    delete s;
+    return DN_OK;
+}
+
+// accumulator views
+static void *acc_ptr(const dn_shot *s, int k)
+{
+    const size_t ncell = (size_t)s->p.nx * s->p.ny;
+    const size_t a = carve_size(ncell, s->acc64 ? 8 : 4);
+    const size_t w = carve_size(ncell, 4);
+    char *b = (char *)s->d_acc;
+    if (k < 3) return b + k * a;
+    return b + 3 * a + (k - 3) * w;
+}
+
+static Inst make_inst(const dn_shot *s, int mode)
+{
+    const dn_model *m = s->m;
+    const dn_params &p = s->p;
+    Inst I;
+    memset(&I, 0, sizeof(I));
+    I.nx = p.nx;
+    I.ny = p.ny;
+    I.nt = p.nt;
+    I.pitch = m->lay.pitch;
+    I.fw = p.fw;
+    I.free_surf = p.free_surf;
+    I.L = p.L;
+    I.mode = mode;
+    I.zch = s->zch;
+    I.tiles_x = s->tiles_x;
+    I.tiles = s->tiles;
+    I.store = (mode == 0) && p.store_snapshots && s->nsnap > 0;
+    I.dtinv = std::max(p.dtinv, 1);
+    I.nsnap = s->nsnap;
+    I.snap_prec = p.snap_precision;
+    I.acc64 = s->acc64;
+    I.eprecond = p.eprecond;
+    I.seismo = p.seismo;
+    I.DT = p.dt;
+    I.DH = p.dh;
+    I.dhi_el = p.dt / p.dh;
+    I.dhi_vi = 1.0 / p.dh;
+    I.dh1 = 1.0 / p.dh;
+    I.dthalbe = p.dt / 2.0;
+    for (int k = 0; k < 7; k++) I.hc[k] = m->hc[k];
+    I.vx = s->f[0];
+    I.vy = s->f[1];
+    I.sxx = s->f[2];
+    I.syy = s->f[3];
+    I.sxy = s->f[4];
+    I.vxp1 = s->f[5];
+    I.vyp1 = s->f[6];
+    I.r = s->r;
+    I.p = s->pmv;
+    I.q = s->q;
+    I.plane = m->lay.plane;
+    I.rip = m->field(MF_RIP);
+    I.rjp = m->field(MF_RJP);
+    I.uipjp = m->field(MF_UIPJP);
+    I.mu = m->field(MF_MU);
+    I.lam = m->field(MF_LAM);
+    I.rho = m->field(MF_RHO);
+    I.vp = m->field(MF_VP);
+    I.vs = m->field(MF_VS);
+    I.gmuss = m->field(MF_GMUSS);
+    I.glamss = m->field(MF_GLAMSS);
+    if (p.L > 0) {
+        I.c_muipjp = m->field(MF_CMUIPJP);
+        I.c_tausipjp = m->field(MF_CTAUSIPJP);
+        I.c_mu = m->field(MF_CMU);
+        I.c_taus = m->field(MF_CTAUS);
+        I.c_pi = m->field(MF_CPI);
+        I.c_taup = m->field(MF_CTAUP);
+        for (int l = 0; l < p.L; l++) {
+            I.eta[l] = m->eta[l];
+            I.bip[l] = m->bip[l];
+            I.cip[l] = m->cip[l];
+            I.s_bjm[l] = m->s_bjm[l];
+        }
+        if (m->dsurf) {
+            I.s_mu = m->dsurf;
+            I.s_pi = m->dsurf + p.nx;
+            I.s_taus = m->dsurf + 2 * p.nx;
+            I.s_taup = m->dsurf + 3 * p.nx;
+        }
+    }
+    const size_t w = 2 * (size_t)std::max(p.fw, 1);
+    I.K_x = m->dpml + 0 * w;
+    I.a_x = m->dpml + 1 * w;
+    I.b_x = m->dpml + 2 * w;
+    I.K_xh = m->dpml + 3 * w;
+    I.a_xh = m->dpml + 4 * w;
+    I.b_xh = m->dpml + 5 * w;
+    I.K_y = m->dpml + 6 * w;
+    I.a_y = m->dpml + 7 * w;
+    I.b_y = m->dpml + 8 * w;
+    I.K_yh = m->dpml + 9 * w;
+    I.a_yh = m->dpml + 10 * w;
+    I.b_yh = m->dpml + 11 * w;
+    I.psi_sxx_x = s->psi[0];
+    I.psi_sxy_x = s->psi[1];
+    I.psi_vxx = s->psi[2];
+    I.psi_vyx = s->psi[3];
+    I.psi_vxxs = s->psi[4];
+    I.psi_syy_y = s->psi[5];
+    I.psi_sxy_y = s->psi[6];
+    I.psi_vyy = s->psi[7];
+    I.psi_vxy = s->psi[8];
+    I.nsrc_cells = s->nsrc_cells;
+    I.src_cell_i = s->d_cell_i;
+    I.src_cell_j = s->d_cell_j;
+    I.src_cell_start = s->d_cell_start;
+    I.src_cell_count = s->d_cell_count;
+    I.src_perm = s->d_perm;
+    I.src_type = s->d_src_type;
+    I.src_nsin = s->d_nsin;
+    I.src_cos = s->d_cos;
+    I.signals = s->d_signals;
+    I.quelltyp_last = s->quelltyp_last;
+    I.nsrc = s->nsrc;
+    I.quelltypb = p.quelltypb;
+    const size_t rs = (size_t)std::max(s->ntr, 1) * p.nt;
+    I.res_vx = s->d_res;
+    I.res_vy = s->d_res + rs;
+    I.res_p = s->d_res + 2 * rs;
+    I.ntr = s->ntr;
+    I.rec_i = s->d_rec_i;
+    I.rec_j = s->d_rec_j;
+    I.sec = s->d_sec;
+    I.snap = s->d_snap;
+    I.snap_scale = s->d_snap_scale;
+    I.wc = acc_ptr(s, 0);
+    I.wcu = acc_ptr(s, 1);
+    I.wcrho = acc_ptr(s, 2);
+    I.Ws = (float *)acc_ptr(s, 3);
+    I.Wr = (float *)acc_ptr(s, 4);
+    I.flag = s->d_flag;
+    return I;
+}
+
+// ---------------------------------------------------------------------------
+// kernel dispatch
+// ---------------------------------------------------------------------------
+struct LaunchCfg {
+    dim3 tile_grid, src_grid, surf_grid, rec_grid;
+    int bx;
+    int R, L;
+    bool exact;
+    bool any_surf, any_src_s, any_store, any_adj, any_rec;
+};
+
+template <int R, bool X>
+static void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int *ntb, int off, long long &nl)
+{
+    k_update_v<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
+    k_inject_v<<<c.src_grid, 128, 0, st>>>(d, ntb, off);
+    nl += 2;
+    if (c.L == 0) {
+        k_update_s_el<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
+    } else {
+        switch (c.L) {
+        case 1: k_update_s_vi<R, 1, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
+        case 2: k_update_s_vi<R, 2, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
+        case 3: k_update_s_vi<R, 3, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
+        case 4: k_update_s_vi<R, 4, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
+        default: k_update_s_vi<R, 5, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
+        }
+    }
+    nl++;
+    if (c.any_src_s) {
+        k_inject_s<<<c.src_grid, 128, 0, st>>>(d, ntb, off);
+        nl++;
+    }
+    if (c.any_surf) {
+        if (c.L == 0) {
+            k_surface_el<R, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off);
+        } else {
+            switch (c.L) {
+            case 1: k_surface_vi<R, 1, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off); break;
+            case 2: k_surface_vi<R, 2, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off); break;
+            case 3: k_surface_vi<R, 3, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off); break;
+            case 4: k_surface_vi<R, 4, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off); break;
+            default: k_surface_vi<R, 5, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off); break;
+            }
+        }
+        nl++;
+    }
+    k_seismo<R><<<c.rec_grid, 128, 0, st>>>(d, ntb, off);
+    nl++;
+    if (c.any_store) {
+        k_snap_store<<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
+        nl++;
+    }
+    if (c.any_adj) {
+        k_correlate<<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
+        nl++;
+    }
+}
+
+template <bool X>
+static void launch_step_X(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int *ntb, int off, long long &nl)
+{
+    switch (c.R) {
+    case 1: launch_step_R<1, X>(c, st, d, ntb, off, nl); break;
+    case 2: launch_step_R<2, X>(c, st, d, ntb, off, nl); break;
+    case 3: launch_step_R<3, X>(c, st, d, ntb, off, nl); break;
+    case 4: launch_step_R<4, X>(c, st, d, ntb, off, nl); break;
+    case 5: launch_step_R<5, X>(c, st, d, ntb, off, nl); break;
+    default: launch_step_R<6, X>(c, st, d, ntb, off, nl); break;
+    }
+}
+
+static void launch_step(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int *ntb, int off, long long &nl)
+{
+    if (c.exact) launch_step_X<true>(c, st, d, ntb, off, nl);
+    else launch_step_X<false>(c, st, d, ntb, off, nl);
+}
+
+__global__ void k_advance(int *ntb, int by) { *ntb += by; }
+
+// ---------------------------------------------------------------------------
+// batch runner
+// ---------------------------------------------------------------------------
+struct Batch {
+    int device;
+    std::vector<const dn_shot *> shots;
+    int mode;
+    Inst *d_insts = nullptr;
+    std::vector<Inst> h_insts;
+    cudaGraphExec_t exec = nullptr;
+    int chunk = 0;
+    long long launches_per_chunk = 0;
+};
+static std::mutex g_batch_mu;
+static std::vector<Batch *> g_batches;   // small cache of captured graphs
+
+static void batch_free(Batch *b)
+{
+    cudaSetDevice(b->device);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    cudaFree(b->d_insts);
+    delete b;
+}
+
+static void forget_shot(const dn_shot *s)
+{
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    for (size_t k = 0; k < g_batches.size();) {
+        Batch *b = g_batches[k];
+        if (std::find(b->shots.begin(), b->shots.end(), s) != b->shots.end()) {
+            batch_free(b);
+            g_batches.erase(g_batches.begin() + k);
+        } else {
+            k++;
+        }
+    }
+}
+
+static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c)
+{
+    if (!shots || n < 1) return dn_fail(DN_EINVAL, "dn_run: empty batch");
+    if (mode < 0 || mode > 2) return dn_fail(DN_EINVAL, "dn_run: bad mode %d", mode);
+    const dn_params &p0 = shots[0]->p;
+    c.R = p0.fdorder / 2;
+    c.L = p0.L;
+    c.exact = p0.arith == DN_ARITH_EXACT;
+    c.bx = shots[0]->bx;
+    c.any_surf = c.any_src_s = c.any_store = c.any_adj = c.any_rec = false;
+    int maxtiles = 0, maxsrc = 1, maxnx = 1, maxtr = 1;
+    for (int k = 0; k < n; k++) {
+        const dn_shot *s = shots[k];
+        if (!s) return dn_fail(DN_EINVAL, "dn_run: null shot %d", k);
+        if (s->m->device != shots[0]->m->device) return dn_fail(DN_EINVAL, "dn_run: shots on different devices");
+        if (s->p.fdorder != p0.fdorder || s->p.L != p0.L)
+            return dn_fail(DN_EINVAL, "dn_run: a batch must share FDORDER and L (shot %d differs)", k);
+        if (s->p.arith != p0.arith || s->bx != c.bx) return dn_fail(DN_EINVAL, "dn_run: mixed arithmetic/tile width");
+        if (mode == 1) {
+            if (!s->stored) return dn_fail(DN_ESTATE, "dn_run: adjoint run of shot %d without a stored forward run", k);
+            for (int l = 0; l < s->nsrc; l++)
+                if (s->src_type[l] == 5)
+                    return dn_fail(DN_ENOTSUP, "moment-tensor sources are not supported in the adjoint pass");
+        }
+        maxtiles = std::max(maxtiles, s->tiles);
+        maxsrc = std::max(maxsrc, std::max(s->nsrc_cells, mode == 1 ? s->ntr : 0));
+        maxnx = std::max(maxnx, s->p.nx);
+        maxtr = std::max(maxtr, s->ntr);
+        if (s->p.free_surf) c.any_surf = true;
+        if (mode == 1 ? s->p.quelltypb >= 4 : (s->quelltyp_last == 1 || s->quelltyp_last == 5)) c.any_src_s = true;
+        if (mode == 0 && s->p.store_snapshots && s->nsnap > 0) c.any_store = true;
+        if (mode == 1) c.any_adj = true;
+    }
+    c.tile_grid = dim3(maxtiles, n);
+    c.src_grid = dim3((maxsrc + 127) / 128, n);
+    c.surf_grid = dim3((maxnx + 127) / 128, n);
+    c.rec_grid = dim3((maxtr + 127) / 128, n);
+    return DN_OK;
+}
+
+static int zero_for_run(dn_shot *s, int mode, cudaStream_t st)
+{
+    CU(cudaMemsetAsync(s->dstate, 0, s->state_bytes, st));   // zero_denise_*_PSV
+    CU(cudaMemsetAsync(s->d_flag, 0, 4, st));
+    if (mode == 0 && s->p.store_snapshots) {
+        // init_grad of the per-shot accumulators and Ws/Wr (grad_obj_psv.c:61-70)
+        const size_t ncell = (size_t)s->p.nx * s->p.ny;
+        CU(cudaMemsetAsync(s->d_acc, 0, carve_size(ncell, s->acc64 ? 8 : 4) * 3 + carve_size(ncell, 4) * 2, st));
+    }
+    return DN_OK;
+}
+
+static int finish_run(dn_shot *const *shots, int n, int mode, cudaStream_t st)
+{
+    CU(cudaStreamSynchronize(st));
+    CU(cudaGetLastError());
+    int bad = -1;
+    for (int k = 0; k < n; k++) {
+        int f = 0;
+        CU(cudaMemcpy(&f, shots[k]->d_flag, 4, cudaMemcpyDeviceToHost));
+        if (f & 1) bad = k;
+        if (mode == 0 && shots[k]->p.store_snapshots) shots[k]->stored = 1;
+        if (mode == 1) shots[k]->correlated = 1;
+    }
+    if (bad >= 0) return dn_fail(DN_EUNSTABLE, " Simulation is unstable ! (NaN in shot %d of the batch)", bad);
+    return DN_OK;
+}
+
+static int graph_chunk(int maxnt)
+{
+    const char *ev = getenv("DN_GRAPH_CHUNK");
+    int k = ev ? atoi(ev) : 50;
+    if (k < 1) k = 1;
+    return std::min(k, maxnt);
+}
+
+extern "C" int dn_run(dn_shot *const *shots, int n, int mode)
+{
+    LaunchCfg c;
+    int st = check_batch(shots, n, mode, c);
+    if (st) return st;
+    const int device = shots[0]->m->device;
+    DevState *ds;
+    st = dev_state(device, &ds);
+    if (st) return st;
+    CU(cudaSetDevice(device));
+    int maxnt = 0;
+    for (int k = 0; k < n; k++) maxnt = std::max(maxnt, shots[k]->p.nt);
+
+    // find or build the captured batch
+    Batch *b = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_batch_mu);
+        for (Batch *x : g_batches) {
+            if (x->mode == mode && x->device == device && (int)x->shots.size() == n &&
+                std::equal(x->shots.begin(), x->shots.end(), shots)) {
+                b = x;
+                break;
+            }
+        }
+    }
+    if (!b) {
+        b = new Batch();
+        b->device = device;
+        b->mode = mode;
+        b->shots.assign(shots, shots + n);
+        for (int k = 0; k < n; k++) b->h_insts.push_back(make_inst(shots[k], mode));
+        if (cudaMalloc(&b->d_insts, sizeof(Inst) * n) != cudaSuccess) {
+            delete b;
+            return dn_fail(DN_ENOMEM, "dn_run: descriptor allocation failed");
+        }
+        CU(cudaMemcpy(b->d_insts, b->h_insts.data(), sizeof(Inst) * n, cudaMemcpyHostToDevice));
+        b->chunk = graph_chunk(maxnt);
+        cudaGraph_t g;
+        CU(cudaStreamBeginCapture(ds->stream, cudaStreamCaptureModeThreadLocal));
+        long long nl = 0;
+        for (int k = 0; k < b->chunk; k++) launch_step(c, ds->stream, b->d_insts, ds->d_step, k + 1, nl);
+        k_advance<<<1, 1, 0, ds->stream>>>(ds->d_step, b->chunk);
+        nl++;
+        cudaError_t e = cudaStreamEndCapture(ds->stream, &g);
+        if (e != cudaSuccess) {
+            batch_free(b);
+            return dn_fail(DN_EDEVICE, "graph capture failed: %s", cudaGetErrorString(e));
+        }
+        e = cudaGraphInstantiate(&b->exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            b->exec = nullptr;
+            batch_free(b);
+            return dn_fail(DN_EDEVICE, "graph instantiate failed: %s", cudaGetErrorString(e));
+        }
+        b->launches_per_chunk = nl;
+        std::lock_guard<std::mutex> lk(g_batch_mu);
+        if (g_batches.size() >= 8) {
+            batch_free(g_batches.front());
+            g_batches.erase(g_batches.begin());
+        }
+        g_batches.push_back(b);
+    }
+    for (int k = 0; k < n; k++) {
+        st = zero_for_run(shots[k], mode, ds->stream);
+        if (st) return st;
+    }
+    CU(cudaMemsetAsync(ds->d_step, 0, sizeof(int), ds->stream));
+    const int nchunks = (maxnt + b->chunk - 1) / b->chunk;
+    CU(cudaEventRecord(ds->ev0, ds->stream));
+    for (int k = 0; k < nchunks; k++) CU(cudaGraphLaunch(b->exec, ds->stream));
+    CU(cudaEventRecord(ds->ev1, ds->stream));
+    st = finish_run(shots, n, mode, ds->stream);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ds->ev0, ds->ev1);
+    g_last_ms = ms;
+    g_last_launches = b->launches_per_chunk * nchunks;
+    return st;
+}
+
+static int run_direct(dn_shot *s, int mode, int nt0, int nt1, bool zero)
+{
+    LaunchCfg c;
+    dn_shot *arr[1] = {s};
+    int st = check_batch(arr, 1, mode, c);
+    if (st) return st;
+    DevState *ds;
+    st = dev_state(s->m->device, &ds);
+    if (st) return st;
+    CU(cudaSetDevice(s->m->device));
+    Inst h = make_inst(s, mode);
+    Inst *d = nullptr;
+    CU(cudaMalloc(&d, sizeof(Inst)));
+    cudaMemcpy(d, &h, sizeof(Inst), cudaMemcpyHostToDevice);
+    if (zero) {
+        st = zero_for_run(s, mode, ds->stream);
+        if (st) {
+            cudaFree(d);
+            return st;
+        }
+    }
+    long long nl = 0;
+    cudaEventRecord(ds->ev0, ds->stream);
+    for (int nt = nt0; nt <= nt1; nt++) launch_step(c, ds->stream, d, ds->d_zero, nt, nl);
+    cudaEventRecord(ds->ev1, ds->stream);
+    cudaError_t le = cudaGetLastError();
+    st = finish_run(arr, 1, mode, ds->stream);
+    if (nt1 < s->p.nt) {
+        if (mode == 0 && s->p.store_snapshots) s->stored = 0;
+        if (mode == 1) s->correlated = 0;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ds->ev0, ds->ev1);
+    g_last_ms = ms;
+    g_last_launches = nl;
+    cudaFree(d);
+    if (le != cudaSuccess) return dn_fail(DN_EDEVICE, "kernel launch failed: %s", cudaGetErrorString(le));
+    return st;
+}
+
+extern "C" int dn_run_plain(dn_shot *s, int mode)
+{
+    if (!s) return dn_fail(DN_EINVAL, "null shot");
+    return run_direct(s, mode, 1, s->p.nt, true);
+}
+
+extern "C" int dn_run_steps(dn_shot *s, int mode, int nt0, int nt1)
+{
+    if (!s) return dn_fail(DN_EINVAL, "null shot");
+    if (nt0 < 1 || nt1 > s->p.nt || nt0 > nt1) return dn_fail(DN_EINVAL, "bad step range %d..%d", nt0, nt1);
+    return run_direct(s, mode, nt0, nt1, nt0 == 1);
+}
+
+extern "C" int dn_last_run_stats(double *ms, long long *launches)
+{
+    if (ms) *ms = g_last_ms;
+    if (launches) *launches = g_last_launches;
+    return DN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// results
+// ---------------------------------------------------------------------------
+extern "C" int dn_shot_get_sections(const dn_shot *s, int comp, float *out)
+{
+    if (!s || !out) return dn_fail(DN_EINVAL, "null argument");
+    if (comp < 0 || comp > 4) return dn_fail(DN_EINVAL, "bad section component %d", comp);
+    const int nt = s->p.nt, ntr = s->ntr;
+    if (ntr == 0) return DN_OK;
+    std::vector<float> tmp((size_t)nt * ntr);
+    CU(cudaSetDevice(s->m->device));
+    CU(cudaMemcpy(tmp.data(), s->d_sec + (size_t)comp * nt * ntr, tmp.size() * 4, cudaMemcpyDeviceToHost));
+    for (int t = 0; t < nt; t++)
+        for (int r = 0; r < ntr; r++) out[(size_t)r * nt + t] = tmp[(size_t)t * ntr + r];
+    return DN_OK;
+}
+
+extern "C" int dn_shot_set_residuals(dn_shot *s, const float *vxd, const float *vyd, const float *pd)
+{
+    if (!s) return dn_fail(DN_EINVAL, "null shot");
+    CU(cudaSetDevice(s->m->device));
+    const size_t rs = (size_t)std::max(s->ntr, 1) * s->p.nt;
+    const float *src[3] = {vxd, vyd, pd};
+    for (int k = 0; k < 3; k++) {
+        if (src[k] && s->ntr > 0) {
+            CU(cudaMemcpy(s->d_res + k * rs, src[k], (size_t)s->ntr * s->p.nt * 4, cudaMemcpyHostToDevice));
+            s->has_res[k] = 1;
+        } else {
+            CU(cudaMemset(s->d_res + k * rs, 0, rs * 4));
+            s->has_res[k] = 0;
+        }
+    }
+    return DN_OK;
+}
+
+extern "C" int dn_shot_get_field(const dn_shot *s, int field, float *out)
+{
+    if (!s || !out) return dn_fail(DN_EINVAL, "null argument");
+    const dn_params &p = s->p;
+    const Layout &L = s->m->lay;
+    CU(cudaSetDevice(s->m->device));
+    if (field >= 0 && field < 7) {
+        std::vector<float> h(L.plane);
+        CU(cudaMemcpy(h.data(), s->f[field] - L.origin, L.plane * 4, cudaMemcpyDeviceToHost));
+        for (int i = 1; i <= p.nx; i++)
+            for (int j = 1; j <= p.ny; j++)
+                out[(size_t)(i - 1) * p.ny + (j - 1)] = h[L.origin + (long long)j * L.pitch + i];
+        return DN_OK;
+    }
+    if (field >= 7 && field <= 11) {
+        const size_t ncell = (size_t)p.nx * p.ny;
+        const bool dbl = field <= 9 && s->acc64;
+        std::vector<char> h(ncell * (dbl ? 8 : 4));
+        CU(cudaMemcpy(h.data(), acc_ptr(s, field - 7), h.size(), cudaMemcpyDeviceToHost));
+        for (int j = 1; j <= p.ny; j++)
+            for (int i = 1; i <= p.nx; i++) {
+                size_t w = (size_t)(j - 1) * p.nx + (i - 1);
+                out[(size_t)(i - 1) * p.ny + (j - 1)] = dbl ? (float)((double *)h.data())[w] : ((float *)h.data())[w];
+            }
+        return DN_OK;
+    }
+    return dn_fail(DN_EINVAL, "bad field id %d", field);
+}
+
+extern "C" int dn_shot_get_snapshot(const dn_shot *s, int k, int field, float *out)
+{
+    if (!s || !out) return dn_fail(DN_EINVAL, "null argument");
+    if (k < 0 || k >= s->nsnap || field < 0 || field > 4) return dn_fail(DN_EINVAL, "bad snapshot index");
+    const dn_params &p = s->p;
+    const size_t tc = (size_t)s->bx * s->zch;
+    const size_t eb = snap_elem_bytes(p.snap_precision);
+    std::vector<char> h((size_t)s->tiles * tc * eb);
+    std::vector<float> sc(s->tiles, 1.0f);
+    CU(cudaSetDevice(s->m->device));
+    const size_t slot0 = ((size_t)k * 5 + field) * s->tiles;
+    CU(cudaMemcpy(h.data(), (char *)s->d_snap + slot0 * tc * eb, h.size(), cudaMemcpyDeviceToHost));
+    if (p.snap_precision != DN_SNAP_F32)
+        CU(cudaMemcpy(sc.data(), s->d_snap_scale + slot0, s->tiles * 4, cudaMemcpyDeviceToHost));
+    for (int b = 0; b < s->tiles; b++) {
+        int tx = b % s->tiles_x, tz = b / s->tiles_x;
+        for (int r = 0; r < s->zch; r++)
+            for (int c = 0; c < s->bx; c++) {
+                int i = tx * s->bx + c + 1, j = tz * s->zch + r + 1;
+                if (i > p.nx || j > p.ny) continue;
+                size_t e = (size_t)b * tc + (size_t)r * s->bx + c;
+                float v;
+                if (p.snap_precision == DN_SNAP_F32) {
+                    v = ((float *)h.data())[e];
+                } else {
+                    uint16_t bits = ((uint16_t *)h.data())[e];
+                    if (p.snap_precision == DN_SNAP_F16) {
+                        __half_raw hr;
+                        hr.x = bits;
+                        v = __half2float(__half(hr)) * sc[b];
+                    } else {
+                        uint32_t u = (uint32_t)bits << 16;
+                        float f;
+                        memcpy(&f, &u, 4);
+                        v = f * sc[b];
+                    }
+                }
+                out[(size_t)(i - 1) * p.ny + (j - 1)] = v;
+            }
+    }
+    return DN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// gradient assembly: ass_gradPSV.c:29-150 (INVMAT1 1, GRAD_FORM 1) + stacking
+// ---------------------------------------------------------------------------
+__global__ void k_ass_grad(int nx, int ny, int pitch, const float *rho, const float *vp, const float *vs,
+                           const float *gmuss, const float *glamss, const void *wc, const void *wcu, const void *wcr,
+                           int acc64, float DT, void *gsum, int out64)
+{
+    const long long n = (long long)nx * ny;
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(w / nx) + 1, i = (int)(w % nx) + 1;
+        const long long o = (long long)j * pitch + i;
+        const float r = rho[o], pi = vp[o], u = vs[o], muss = gmuss[o], lamss = glamss[o];
+        double gvp, gvs, grho;
+        if (!acc64) {
+            const float ws = ((const float *)wc)[w], wus = ((const float *)wcu)[w], wrs = ((const float *)wcr)[w];
+            float lam = __fmul_rn(-DT, ws);
+            if (muss > 0.0f || lamss > 0.0f) {
+                const float lm = __fadd_rn(lamss, muss);
+                lam = F(DMUL(DDIV(1.0, DMUL(DMUL(4.0, (double)lm), (double)lm)), (double)lam));
+            }
+            const float fvp = F(DMUL(DMUL(DMUL(2.0, (double)pi), (double)r), (double)lam));
+            const float mu = __fmul_rn(-DT, wus);
+            const float fvs = F(DADD(DMUL(DMUL(DMUL(-4.0, (double)r), (double)u), (double)lam),
+                                     DMUL(DMUL(DMUL(2.0, (double)r), (double)u), (double)mu)));
+            const float rs = __fmul_rn(-DT, wrs);
+            const double a = DSUB((double)__fmul_rn(pi, pi), DMUL(DMUL(2.0, (double)u), (double)u));
+            const float frho = F(DADD(DADD(DMUL(a, (double)lam), (double)__fmul_rn(__fmul_rn(u, u), mu)), (double)rs));
+            gvp = fvp;
+            gvs = fvs;
+            grho = frho;
+        } else {
+            const double ws = ((const double *)wc)[w], wus = ((const double *)wcu)[w], wrs = ((const double *)wcr)[w];
+            double lam = -(double)DT * ws;
+            if (muss > 0.0f || lamss > 0.0f) {
+                const double lm = (double)lamss + (double)muss;
+                lam = lam / (4.0 * lm * lm);
+            }
+            gvp = 2.0 * (double)pi * (double)r * lam;
+            const double mu = -(double)DT * wus;
+            gvs = -4.0 * (double)r * (double)u * lam + 2.0 * (double)r * (double)u * mu;
+            const double rs = -(double)DT * wrs;
+            grho = ((double)pi * pi - 2.0 * (double)u * u) * lam + (double)u * u * mu + rs;
+        }
+        if (out64) {
+            double *g = (double *)gsum;
+            g[w] += gvp;
+            g[n + w] += gvs;
+            g[2 * n + w] += grho;
+        } else {
+            float *g = (float *)gsum;
+            g[w] = __fadd_rn(g[w], (float)gvp);
+            g[n + w] = __fadd_rn(g[n + w], (float)gvs);
+            g[2 * n + w] = __fadd_rn(g[2 * n + w], (float)grho);
+        }
+    }
+}
+
+extern "C" int dn_shot_accumulate_gradient(dn_shot *s)
+{
+    if (!s) return dn_fail(DN_EINVAL, "null shot");
+    if (!s->correlated) return dn_fail(DN_ESTATE, "dn_shot_accumulate_gradient: no completed adjoint run");
+    dn_model *m = s->m;
+    DevState *ds;
+    int st = dev_state(m->device, &ds);
+    if (st) return st;
+    CU(cudaSetDevice(m->device));
+    const long long n = (long long)s->p.nx * s->p.ny;
+    int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+    k_ass_grad<<<blocks, 256, 0, ds->stream>>>(s->p.nx, s->p.ny, m->lay.pitch, m->field(MF_RHO), m->field(MF_VP),
+                                               m->field(MF_VS), m->field(MF_GMUSS), m->field(MF_GLAMSS), acc_ptr(s, 0),
+                                               acc_ptr(s, 1), acc_ptr(s, 2), s->acc64, s->p.dt, m->dgrad, m->grad64);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(ds->stream));
+    return DN_OK;
+}
+
+extern "C" int dn_model_get_gradient(const dn_model *m, float *g_vp, float *g_vs, float *g_rho)
+{
+    if (!m) return dn_fail(DN_EINVAL, "null model");
+    const int nx = m->p.nx, ny = m->p.ny;
+    const size_t n = (size_t)nx * ny;
+    std::vector<char> h(3 * n * (m->grad64 ? 8 : 4));
+    CU(cudaSetDevice(m->device));
+    CU(cudaMemcpy(h.data(), m->dgrad, h.size(), cudaMemcpyDeviceToHost));
+    float *outs[3] = {g_vp, g_vs, g_rho};
+    for (int c = 0; c < 3; c++) {
+        if (!outs[c]) continue;
+        for (int j = 1; j <= ny; j++)
+            for (int i = 1; i <= nx; i++) {
+                size_t w = c * n + (size_t)(j - 1) * nx + (i - 1);
+                outs[c][(size_t)(i - 1) * ny + (j - 1)] = m->grad64 ? (float)((double *)h.data())[w] : ((float *)h.data())[w];
+            }
+    }
+    return DN_OK;
+}
+
+extern "C" int dn_model_zero_gradient(dn_model *m)
+{
+    if (!m) return dn_fail(DN_EINVAL, "null model");
+    CU(cudaSetDevice(m->device));
+    CU(cudaMemset(m->dgrad, 0, 3 * (size_t)m->p.nx * m->p.ny * (m->grad64 ? 8 : 4)));
+    return DN_OK;
+}

@@ -1,0 +1,31 @@
+/* Internal declarations shared by the host C and CUDA translation units. */
+#ifndef DN_INTERNAL_H
+#define DN_INTERNAL_H
+
+#include "denise_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Records `msg` as the thread's last error and returns `code`. */
+int dn_fail(int code, const char *fmt, ...);
+
+int dn_visc_eta(const dn_params *p, float *eta, float *pts);
+float dn_visc_sum(const dn_params *p, float ws);
+float dn_visc_tau_from_q(float q);
+int dn_visc_cell_factors(const dn_params *p, const float *vp, const float *vs, const float *rho, const float *qp,
+                         const float *qs, float *muipjp, float *tausipjp, float *mu, float *taus, float *pi,
+                         float *taup);
+
+#ifdef __cplusplus
+}
+#endif
+
+/* Grid padding of every device field: HX columns left/right, HZ rows above/below
+ * the interior.  HZ >= FDORDER/2 covers the free-surface image rows and the
+ * stencil reach; HX = 8 keeps column i = 1 16-byte aligned. */
+#define DN_HX 8
+#define DN_HZ 8
+
+#endif

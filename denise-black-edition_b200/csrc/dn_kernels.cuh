@@ -1,0 +1,898 @@
+// Device kernels of the P-SV propagator (sm_100a).
+//
+// Every kernel works on a batch of shot instances: blockIdx.y selects the
+// instance, blockIdx.x a tile of it.  A tile is blockDim.x columns wide and
+// `zch` rows tall; each thread owns one column and streams down the rows,
+// keeping the vertical stencil of the fields it differentiates in z in a
+// register window (one new load per row per field).  Horizontal neighbours
+// come from L1 (the warp reads 32 consecutive floats, shifted by m).
+//
+// Arithmetic: with EXACT = true every float operation is issued with an
+// explicit round-to-nearest intrinsic (__fmul_rn, __fadd_rn, ...), which the
+// compiler may neither contract into FMA nor reorder, and every term the
+// reference's C promotes to double (a float meeting a double literal such as
+// 2.0*f*vxx) is evaluated in double.  The result is the IEEE float sequence
+// the reference's C source spells out, so the GPU state is bit-identical to
+// the reference's CPU state step by step.  EXACT = false allows FMA.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "denise_b200.h"
+#include "dn_internal.h"
+
+namespace dn {
+
+// ---------------------------------------------------------------------------
+// Per-instance descriptor (one shot in one mode).  Field pointers are
+// "origin" pointers: element (j, i) (1-based, the reference's indices) is
+// p[j * pitch + i].
+// ---------------------------------------------------------------------------
+struct Inst {
+    int nx, ny, nt, pitch;
+    int fw, free_surf, L, mode;       // mode: 0 forward, 1 adjoint, 2 objective
+    int zch, tiles_x, tiles;          // rows per tile, tiles across, total tiles
+    int store;                        // mode 0: store snapshots
+    int dtinv, nsnap, snap_prec, acc64, eprecond;
+    int seismo;                       // SEISMO
+    float DT, DH, dhi_el, dhi_vi, dh1, dthalbe;
+    float hc[7];
+    // wavefield state
+    float *vx, *vy, *sxx, *syy, *sxy, *vxp1, *vyp1;
+    float *r, *p, *q;                 // visco memory variables, plane l at + l * plane
+    long long plane;
+    // materials (origin pointers)
+    const float *rip, *rjp, *uipjp, *mu, *lam;
+    const float *rho, *vp, *vs;                       // raw model (gradient terms)
+    const float *c_muipjp, *c_tausipjp, *c_mu, *c_taus, *c_pi, *c_taup;   // visco
+    const float *gmuss, *glamss;                      // muss, lamss of psv.c:333-334
+    float eta[DN_MAX_L], bip[DN_MAX_L], cip[DN_MAX_L];
+    // visco free-surface constants per column i (index i-1)
+    const float *s_mu, *s_pi, *s_taus, *s_taup;
+    float s_bjm[DN_MAX_L];
+    // CPML profile vectors (index h-1)
+    const float *K_x, *a_x, *b_x, *K_xh, *a_xh, *b_xh, *K_y, *a_y, *b_y, *K_yh, *a_yh, *b_yh;
+    // CPML memory: x frame [ny][2fw], z frame [2fw][nx]
+    float *psi_sxx_x, *psi_sxy_x, *psi_syy_y, *psi_sxy_y;
+    float *psi_vxx, *psi_vyx, *psi_vyy, *psi_vxy, *psi_vxxs;
+    // sources (forward) / adjoint sources
+    int nsrc_cells;                   // unique source cells
+    const int *src_cell_i, *src_cell_j, *src_cell_start, *src_cell_count, *src_perm;
+    const int *src_type;              // per source
+    const double *src_nsin, *src_cos; // -sin(azimuth), cos(azimuth) (QUELLTYP 4)
+    const float *signals;             // [nsrc][nt]
+    int quelltyp_last;                // QUELLTYP after update_v's overwrite (last source)
+    int nsrc;
+    int quelltypb;
+    const float *res_vx, *res_vy, *res_p;   // [ntr][nt] adjoint sources (receivers)
+    // receivers
+    int ntr;
+    const int *rec_i, *rec_j;
+    float *sec;                       // [ncomp][nt][ntr]
+    // snapshots
+    void *snap;                       // [nsnap][5][tiles][tile cells] in snap_prec
+    float *snap_scale;                // [nsnap][5][tiles]
+    // per-shot correlation accumulators (float or double, origin pointers)
+    void *wc, *wcu, *wcrho;
+    float *Ws, *Wr;
+    // status
+    int *flag;                        // bit 0: NaN seen at the psv.c:99 probe
+};
+
+// ---------------------------------------------------------------------------
+// arithmetic helpers
+// ---------------------------------------------------------------------------
+template <bool X> __device__ __forceinline__ float MUL(float a, float b) { return X ? __fmul_rn(a, b) : a * b; }
+template <bool X> __device__ __forceinline__ float ADD(float a, float b) { return X ? __fadd_rn(a, b) : a + b; }
+template <bool X> __device__ __forceinline__ float SUB(float a, float b) { return X ? __fsub_rn(a, b) : a - b; }
+template <bool X> __device__ __forceinline__ float DIV(float a, float b) { return X ? __fdiv_rn(a, b) : a / b; }
+__device__ __forceinline__ double DMUL(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double DADD(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double DSUB(double a, double b) { return __dadd_rn(a, -b); }
+__device__ __forceinline__ double DDIV(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float F(double a) { return __double2float_rn(a); }
+
+// ---------------------------------------------------------------------------
+// tile location
+// ---------------------------------------------------------------------------
+struct TileLoc {
+    int i, j0, j1;
+};
+__device__ __forceinline__ bool tile_of(const Inst &I, TileLoc &t)
+{
+    int b = blockIdx.x;
+    if (b >= I.tiles) return false;
+    int tx = b % I.tiles_x, tz = b / I.tiles_x;
+    t.i = tx * blockDim.x + threadIdx.x + 1;
+    t.j0 = tz * I.zch + 1;
+    t.j1 = min(t.j0 + I.zch - 1, I.ny);
+    return t.i <= I.nx;
+}
+
+// ===========================================================================
+// Velocity update: update_v_PML_PSV.c:53-715 (FDORDER 2..12) + CPML on the
+// stress derivatives; mode 0/2: vxp1 = rip (sxx_x + sxy_y) / DH (:451-453),
+// mode 1: vxp1 += DT * vx with the old vx (:455-457).
+// ===========================================================================
+template <int R, bool X>
+__global__ void __launch_bounds__(256) k_update_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+{
+    const int nt = __ldg(ntb) + off;
+    const Inst &I = insts[blockIdx.y];
+    if (nt > I.nt) return;
+    TileLoc t;
+    if (!tile_of(I, t)) return;
+    const long long P = I.pitch;
+    const int i = t.i;
+    const float *__restrict__ sxx = I.sxx;
+    const float *__restrict__ syy = I.syy;
+    const float *__restrict__ sxy = I.sxy;
+    float hc[R + 1];
+#pragma unroll
+    for (int m = 1; m <= R; m++) hc[m] = I.hc[m];
+    const float DT = I.DT, DH = I.DH;
+    const int mode = I.mode;
+    const bool snapstep = (mode == 0) && I.store && ((nt - 1) % I.dtinv == 0);
+    const int fw = I.fw, nx = I.nx, ny = I.ny;
+
+    // window: wyy[k] = syy[j-R+1+k], wxy[k] = sxy[j-R+k]
+    float wyy[2 * R], wxy[2 * R];
+#pragma unroll
+    for (int k = 0; k < 2 * R - 1; k++) {
+        wyy[k] = syy[(long long)(t.j0 - R + 1 + k) * P + i];
+        wxy[k] = sxy[(long long)(t.j0 - R + k) * P + i];
+    }
+    for (int j = t.j0; j <= t.j1; j++) {
+        wyy[2 * R - 1] = syy[(long long)(j + R) * P + i];
+        wxy[2 * R - 1] = sxy[(long long)(j + R - 1) * P + i];
+        const float *rs = sxx + (long long)j * P + i;
+        const float *rx = sxy + (long long)j * P + i;
+        float sxx_x = MUL<X>(hc[1], SUB<X>(rs[1], rs[0]));
+        float sxy_x = MUL<X>(hc[1], SUB<X>(rx[0], rx[-1]));
+        float sxy_y = MUL<X>(hc[1], SUB<X>(wxy[R], wxy[R - 1]));
+        float syy_y = MUL<X>(hc[1], SUB<X>(wyy[R], wyy[R - 1]));
+#pragma unroll
+        for (int m = 2; m <= R; m++) {
+            sxx_x = ADD<X>(sxx_x, MUL<X>(hc[m], SUB<X>(rs[m], rs[1 - m])));
+            sxy_x = ADD<X>(sxy_x, MUL<X>(hc[m], SUB<X>(rx[m - 1], rx[-m])));
+            sxy_y = ADD<X>(sxy_y, MUL<X>(hc[m], SUB<X>(wxy[R + m - 1], wxy[R - m])));
+            syy_y = ADD<X>(syy_y, MUL<X>(hc[m], SUB<X>(wyy[R - 1 + m], wyy[R - m])));
+        }
+        if (fw > 0) {
+            if (i <= fw) {   // left frame (BOUNDARY == 0)
+                const int h = i - 1;
+                float *ps = I.psi_sxx_x + (long long)(j - 1) * 2 * fw + h;
+                float v = ADD<X>(MUL<X>(I.b_xh[h], *ps), MUL<X>(I.a_xh[h], sxx_x));
+                *ps = v;
+                sxx_x = ADD<X>(DIV<X>(sxx_x, I.K_xh[h]), v);
+                float *pq = I.psi_sxy_x + (long long)(j - 1) * 2 * fw + h;
+                float w = ADD<X>(MUL<X>(I.b_x[h], *pq), MUL<X>(I.a_x[h], sxy_x));
+                *pq = w;
+                sxy_x = ADD<X>(DIV<X>(sxy_x, I.K_x[h]), w);
+            }
+            if (i >= nx - fw + 1) {   // right frame, h1 = i - nx + 2 fw
+                const int h = i - nx + 2 * fw - 1;
+                float *ps = I.psi_sxx_x + (long long)(j - 1) * 2 * fw + h;
+                float v = ADD<X>(MUL<X>(I.b_xh[h], *ps), MUL<X>(I.a_xh[h], sxx_x));
+                *ps = v;
+                sxx_x = ADD<X>(DIV<X>(sxx_x, I.K_xh[h]), v);
+                float *pq = I.psi_sxy_x + (long long)(j - 1) * 2 * fw + h;
+                float w = ADD<X>(MUL<X>(I.b_x[h], *pq), MUL<X>(I.a_x[h], sxy_x));
+                *pq = w;
+                sxy_x = ADD<X>(DIV<X>(sxy_x, I.K_x[h]), w);
+            }
+            if (!I.free_surf && j <= fw) {   // top frame
+                const int h = j - 1;
+                float *ps = I.psi_syy_y + (long long)h * nx + (i - 1);
+                float v = ADD<X>(MUL<X>(I.b_yh[h], *ps), MUL<X>(I.a_yh[h], syy_y));
+                *ps = v;
+                syy_y = ADD<X>(DIV<X>(syy_y, I.K_yh[h]), v);
+                float *pq = I.psi_sxy_y + (long long)h * nx + (i - 1);
+                float w = ADD<X>(MUL<X>(I.b_y[h], *pq), MUL<X>(I.a_y[h], sxy_y));
+                *pq = w;
+                sxy_y = ADD<X>(DIV<X>(sxy_y, I.K_y[h]), w);
+            }
+            if (j >= ny - fw + 1) {   // bottom frame, h1 = j - ny + 2 fw
+                const int h = j - ny + 2 * fw - 1;
+                float *ps = I.psi_syy_y + (long long)h * nx + (i - 1);
+                float v = ADD<X>(MUL<X>(I.b_yh[h], *ps), MUL<X>(I.a_yh[h], syy_y));
+                *ps = v;
+                syy_y = ADD<X>(DIV<X>(syy_y, I.K_yh[h]), v);
+                float *pq = I.psi_sxy_y + (long long)h * nx + (i - 1);
+                float w = ADD<X>(MUL<X>(I.b_y[h], *pq), MUL<X>(I.a_y[h], sxy_y));
+                *pq = w;
+                sxy_y = ADD<X>(DIV<X>(sxy_y, I.K_y[h]), w);
+            }
+        }
+        const long long o = (long long)j * P + i;
+        const float s1 = ADD<X>(sxx_x, sxy_y);
+        const float s2 = ADD<X>(sxy_x, syy_y);
+        const float ripv = I.rip[o], rjpv = I.rjp[o];
+        float vxo = I.vx[o], vyo = I.vy[o];
+        if (snapstep) {
+            I.vxp1[o] = DIV<X>(MUL<X>(ripv, s1), DH);
+            I.vyp1[o] = DIV<X>(MUL<X>(rjpv, s2), DH);
+        } else if (mode == 1) {
+            I.vxp1[o] = ADD<X>(I.vxp1[o], MUL<X>(DT, vxo));
+            I.vyp1[o] = ADD<X>(I.vyp1[o], MUL<X>(DT, vyo));
+        }
+        I.vx[o] = ADD<X>(vxo, DIV<X>(MUL<X>(MUL<X>(DT, ripv), s1), DH));
+        I.vy[o] = ADD<X>(vyo, DIV<X>(MUL<X>(MUL<X>(DT, rjpv), s2), DH));
+#pragma unroll
+        for (int k = 0; k < 2 * R - 1; k++) {
+            wyy[k] = wyy[k + 1];
+            wxy[k] = wxy[k + 1];
+        }
+    }
+}
+
+// ===========================================================================
+// Force sources (update_v_PML_PSV.c:738-752) and adjoint residual forces
+// (:755-768).  One thread per unique source cell; sources sharing a cell are
+// added in their list order, as the reference's sequential loop does.
+// ===========================================================================
+__global__ void k_inject_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+{
+    const int nt = __ldg(ntb) + off;
+    const Inst &I = insts[blockIdx.y];
+    if (nt > I.nt) return;
+    const long long P = I.pitch;
+    if (I.mode == 1) {
+        const int q = I.quelltypb;
+        for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < I.ntr; l += gridDim.x * blockDim.x) {
+            const long long o = (long long)I.rec_j[l] * P + I.rec_i[l];
+            const long long s = (long long)l * I.nt + (nt - 1);
+            if (q == 1) {
+                I.vx[o] = __fadd_rn(I.vx[o], I.res_vx[s]);
+                I.vy[o] = __fadd_rn(I.vy[o], I.res_vy[s]);
+            }
+            if (q == 2 || q == 6 || q == 7) I.vy[o] = __fadd_rn(I.vy[o], I.res_vy[s]);
+            if (q == 3 || q == 5 || q == 7) I.vx[o] = __fadd_rn(I.vx[o], I.res_vx[s]);
+        }
+        return;
+    }
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < I.nsrc_cells; c += gridDim.x * blockDim.x) {
+        const long long o = (long long)I.src_cell_j[c] * P + I.src_cell_i[c];
+        float vx = I.vx[o], vy = I.vy[o];
+        const int s0 = I.src_cell_start[c], ns = I.src_cell_count[c];
+        for (int k = 0; k < ns; k++) {
+            const int l = I.src_perm[s0 + k];
+            const int ty = I.src_type[l];
+            const float s = I.signals[(long long)l * I.nt + (nt - 1)];
+            if (ty == 2) vx = __fadd_rn(vx, s);
+            if (ty == 3) vy = __fadd_rn(vy, s);
+            if (ty == 4) {
+                vx = F(DADD((double)vx, DMUL(I.src_nsin[l], (double)s)));
+                vy = F(DADD((double)vy, DMUL(I.src_cos[l], (double)s)));
+            }
+        }
+        I.vx[o] = vx;
+        I.vy[o] = vy;
+    }
+}
+
+// ===========================================================================
+// Stress derivatives shared by the elastic and viscoelastic updates:
+// vxx, vyx, vxy, vyy of update_s_*_PML_PSV.c (case 8 = :366-384 elastic),
+// multiplied by dhi, followed by the CPML correction (:386-438).
+// ===========================================================================
+template <int R, bool X>
+struct VDeriv {
+    float wx[2 * R];   // vx rows j-R+1 .. j+R
+    float wy[2 * R];   // vy rows j-R .. j+R-1
+
+    __device__ __forceinline__ void prime(const Inst &I, int i, int j0)
+    {
+        const long long P = I.pitch;
+#pragma unroll
+        for (int k = 0; k < 2 * R - 1; k++) {
+            wx[k] = I.vx[(long long)(j0 - R + 1 + k) * P + i];
+            wy[k] = I.vy[(long long)(j0 - R + k) * P + i];
+        }
+    }
+    __device__ __forceinline__ void load_row(const Inst &I, int i, int j)
+    {
+        const long long P = I.pitch;
+        wx[2 * R - 1] = I.vx[(long long)(j + R) * P + i];
+        wy[2 * R - 1] = I.vy[(long long)(j + R - 1) * P + i];
+    }
+    __device__ __forceinline__ void shift()
+    {
+#pragma unroll
+        for (int k = 0; k < 2 * R - 1; k++) {
+            wx[k] = wx[k + 1];
+            wy[k] = wy[k + 1];
+        }
+    }
+    __device__ __forceinline__ void compute(const Inst &I, const float *hc, int i, int j, float dhi, float &vxx,
+                                            float &vyx, float &vxy, float &vyy)
+    {
+        const long long P = I.pitch;
+        const float *rx = I.vx + (long long)j * P + i;
+        const float *ry = I.vy + (long long)j * P + i;
+        float a = MUL<X>(hc[1], SUB<X>(rx[0], rx[-1]));
+        float b = MUL<X>(hc[1], SUB<X>(ry[1], ry[0]));
+        float c = MUL<X>(hc[1], SUB<X>(wx[R], wx[R - 1]));
+        float d = MUL<X>(hc[1], SUB<X>(wy[R], wy[R - 1]));
+#pragma unroll
+        for (int m = 2; m <= R; m++) {
+            a = ADD<X>(a, MUL<X>(hc[m], SUB<X>(rx[m - 1], rx[-m])));
+            b = ADD<X>(b, MUL<X>(hc[m], SUB<X>(ry[m], ry[1 - m])));
+            c = ADD<X>(c, MUL<X>(hc[m], SUB<X>(wx[R - 1 + m], wx[R - m])));
+            d = ADD<X>(d, MUL<X>(hc[m], SUB<X>(wy[R + m - 1], wy[R - m])));
+        }
+        vxx = MUL<X>(a, dhi);
+        vyx = MUL<X>(b, dhi);
+        vxy = MUL<X>(c, dhi);
+        vyy = MUL<X>(d, dhi);
+        const int fw = I.fw, nx = I.nx, ny = I.ny;
+        if (fw > 0) {
+            if (i <= fw) {
+                const int h = i - 1;
+                float *p1 = I.psi_vxx + (long long)(j - 1) * 2 * fw + h;
+                float v = ADD<X>(MUL<X>(I.b_x[h], *p1), MUL<X>(I.a_x[h], vxx));
+                *p1 = v;
+                vxx = ADD<X>(DIV<X>(vxx, I.K_x[h]), v);
+                float *p2 = I.psi_vyx + (long long)(j - 1) * 2 * fw + h;
+                float w = ADD<X>(MUL<X>(I.b_xh[h], *p2), MUL<X>(I.a_xh[h], vyx));
+                *p2 = w;
+                vyx = ADD<X>(DIV<X>(vyx, I.K_xh[h]), w);
+            }
+            if (i >= nx - fw + 1) {
+                const int h = i - nx + 2 * fw - 1;
+                float *p1 = I.psi_vxx + (long long)(j - 1) * 2 * fw + h;
+                float v = ADD<X>(MUL<X>(I.b_x[h], *p1), MUL<X>(I.a_x[h], vxx));
+                *p1 = v;
+                vxx = ADD<X>(DIV<X>(vxx, I.K_x[h]), v);
+                float *p2 = I.psi_vyx + (long long)(j - 1) * 2 * fw + h;
+                float w = ADD<X>(MUL<X>(I.b_xh[h], *p2), MUL<X>(I.a_xh[h], vyx));
+                *p2 = w;
+                vyx = ADD<X>(DIV<X>(vyx, I.K_xh[h]), w);
+            }
+            if (!I.free_surf && j <= fw) {
+                const int h = j - 1;
+                float *p1 = I.psi_vyy + (long long)h * nx + (i - 1);
+                float *p2 = I.psi_vxy + (long long)h * nx + (i - 1);
+                float v = ADD<X>(MUL<X>(I.b_y[h], *p1), MUL<X>(I.a_y[h], vyy));
+                float w = ADD<X>(MUL<X>(I.b_yh[h], *p2), MUL<X>(I.a_yh[h], vxy));
+                *p1 = v;
+                *p2 = w;
+                vyy = ADD<X>(DIV<X>(vyy, I.K_y[h]), v);
+                vxy = ADD<X>(DIV<X>(vxy, I.K_yh[h]), w);
+            }
+            if (j >= ny - fw + 1) {
+                const int h = j - ny + 2 * fw - 1;
+                float *p1 = I.psi_vyy + (long long)h * nx + (i - 1);
+                float v = ADD<X>(MUL<X>(I.b_y[h], *p1), MUL<X>(I.a_y[h], vyy));
+                *p1 = v;
+                vyy = ADD<X>(DIV<X>(vyy, I.K_y[h]), v);
+                float *p2 = I.psi_vxy + (long long)h * nx + (i - 1);
+                float w = ADD<X>(MUL<X>(I.b_yh[h], *p2), MUL<X>(I.a_yh[h], vxy));
+                *p2 = w;
+                vxy = ADD<X>(DIV<X>(vxy, I.K_yh[h]), w);
+            }
+        }
+    }
+};
+
+// ===========================================================================
+// Elastic stress update: update_s_elastic_PML_PSV.c (case 8 = :335-476),
+// with f = rho vs^2 and g = rho (vp^2 - 2 vs^2) precomputed per cell
+// (:442-444) and the double-promoted 2.0*f*vxx terms (:454-456).
+// ===========================================================================
+template <int R, bool X>
+__global__ void __launch_bounds__(256) k_update_s_el(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+{
+    const int nt = __ldg(ntb) + off;
+    const Inst &I = insts[blockIdx.y];
+    if (nt > I.nt) return;
+    TileLoc t;
+    if (!tile_of(I, t)) return;
+    const long long P = I.pitch;
+    const int i = t.i;
+    float hc[R + 1];
+#pragma unroll
+    for (int m = 1; m <= R; m++) hc[m] = I.hc[m];
+    const float dhi = I.dhi_el;
+    VDeriv<R, X> D;
+    D.prime(I, i, t.j0);
+    for (int j = t.j0; j <= t.j1; j++) {
+        D.load_row(I, i, j);
+        float vxx, vyx, vxy, vyy;
+        D.compute(I, hc, i, j, dhi, vxx, vyx, vxy, vyy);
+        const long long o = (long long)j * P + i;
+        const float fipjp = I.uipjp[o];
+        const float f = I.mu[o];
+        const float g = I.lam[o];
+        const float div = ADD<X>(vxx, vyy);
+        const float gdiv = MUL<X>(g, div);
+        const double f2 = 2.0 * (double)f;
+        I.sxy[o] = ADD<X>(I.sxy[o], MUL<X>(fipjp, ADD<X>(vyx, vxy)));
+        I.sxx[o] = F(DADD((double)I.sxx[o], DADD((double)gdiv, DMUL(f2, (double)vxx))));
+        I.syy[o] = F(DADD((double)I.syy[o], DADD((double)gdiv, DMUL(f2, (double)vyy))));
+        D.shift();
+    }
+}
+
+// ===========================================================================
+// Viscoelastic stress update: update_s_visc_PML_PSV.c (case 8 = :391-511).
+// fipjp, f, g, dip, d, e are regenerated per cell from the six relaxed-modulus
+// factors exactly as prepare_update_s_visc_PSV.c:52-62 forms them.
+// ===========================================================================
+template <int R, int L, bool X>
+__global__ void __launch_bounds__(256) k_update_s_vi(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+{
+    const int nt = __ldg(ntb) + off;
+    const Inst &I = insts[blockIdx.y];
+    if (nt > I.nt) return;
+    TileLoc t;
+    if (!tile_of(I, t)) return;
+    const long long P = I.pitch;
+    const int i = t.i;
+    float hc[R + 1];
+#pragma unroll
+    for (int m = 1; m <= R; m++) hc[m] = I.hc[m];
+    const float dhi = I.dhi_vi, DT = I.DT, dthalbe = I.dthalbe;
+    const float fL = (float)L;
+    float eta[L], bip[L], cip[L];
+#pragma unroll
+    for (int l = 0; l < L; l++) {
+        eta[l] = I.eta[l];
+        bip[l] = I.bip[l];
+        cip[l] = I.cip[l];
+    }
+    VDeriv<R, X> D;
+    D.prime(I, i, t.j0);
+    for (int j = t.j0; j <= t.j1; j++) {
+        D.load_row(I, i, j);
+        float vxx, vyx, vxy, vyy;
+        D.compute(I, hc, i, j, dhi, vxx, vyx, vxy, vyy);
+        const long long o = (long long)j * P + i;
+        const float muipjp = I.c_muipjp[o], tsij = I.c_tausipjp[o];
+        const float mu = I.c_mu[o], taus = I.c_taus[o], pi = I.c_pi[o], taup = I.c_taup[o];
+        const float fipjp = F(DMUL((double)__fmul_rn(muipjp, DT), DADD(1.0, (double)__fmul_rn(fL, tsij))));
+        const float f = F(DMUL((double)__fmul_rn(mu, DT), DADD(1.0, (double)__fmul_rn(fL, taus))));
+        const float g = F(DMUL((double)__fmul_rn(pi, DT), DADD(1.0, (double)__fmul_rn(fL, taup))));
+        float sumr = 0.0f, sump = 0.0f, sumq = 0.0f;
+        float rr[L], pp[L], qq[L];
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            rr[l] = I.r[o + l * I.plane];
+            pp[l] = I.p[o + l * I.plane];
+            qq[l] = I.q[o + l * I.plane];
+            sumr = ADD<X>(sumr, rr[l]);
+            sump = ADD<X>(sump, pp[l]);
+            sumq = ADD<X>(sumq, qq[l]);
+        }
+        const float sh = ADD<X>(vxy, vyx);
+        const float dv = ADD<X>(vxx, vyy);
+        const float gdv = MUL<X>(g, dv);
+        const double f2 = 2.0 * (double)f;
+        float sxy = ADD<X>(I.sxy[o], ADD<X>(MUL<X>(fipjp, sh), MUL<X>(dthalbe, sumr)));
+        float sxx = F(DADD((double)I.sxx[o], DADD(DSUB((double)gdv, DMUL(f2, (double)vyy)), (double)MUL<X>(dthalbe, sump))));
+        float syy = F(DADD((double)I.syy[o], DADD(DSUB((double)gdv, DMUL(f2, (double)vxx)), (double)MUL<X>(dthalbe, sumq))));
+        sumr = sump = sumq = 0.0f;
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            const float dip = MUL<X>(MUL<X>(muipjp, eta[l]), tsij);
+            const float dd = MUL<X>(MUL<X>(mu, eta[l]), taus);
+            const float ee = MUL<X>(MUL<X>(pi, eta[l]), taup);
+            const float r = MUL<X>(bip[l], SUB<X>(MUL<X>(rr[l], cip[l]), MUL<X>(dip, sh)));
+            const double d2 = 2.0 * (double)dd;
+            const float pv = F(DMUL((double)bip[l], DADD((double)SUB<X>(MUL<X>(pp[l], cip[l]), MUL<X>(ee, dv)), DMUL(d2, (double)vyy))));
+            const float qv = F(DMUL((double)bip[l], DADD((double)SUB<X>(MUL<X>(qq[l], cip[l]), MUL<X>(ee, dv)), DMUL(d2, (double)vxx))));
+            I.r[o + l * I.plane] = r;
+            I.p[o + l * I.plane] = pv;
+            I.q[o + l * I.plane] = qv;
+            sumr = ADD<X>(sumr, r);
+            sump = ADD<X>(sump, pv);
+            sumq = ADD<X>(sumq, qv);
+        }
+        I.sxy[o] = ADD<X>(sxy, MUL<X>(dthalbe, sumr));
+        I.sxx[o] = ADD<X>(sxx, MUL<X>(dthalbe, sump));
+        I.syy[o] = ADD<X>(syy, MUL<X>(dthalbe, sumq));
+        D.shift();
+    }
+}
+
+// ===========================================================================
+// Explosive source psource.c:23-39 (mode 0/2 when QUELLTYP == 1), adjoint
+// pressure source psource.c:41-53 (mode 1, QUELLTYPB >= 4) and the moment
+// tensor source msource.c:27-41 (QUELLTYP == 5, forward modes).
+// ===========================================================================
+__global__ void k_inject_s(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+{
+    const int nt = __ldg(ntb) + off;
+    const Inst &I = insts[blockIdx.y];
+    if (nt > I.nt) return;
+    const long long P = I.pitch;
+    if (I.mode == 1) {
+        if (I.quelltypb < 4) return;
+        for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < I.ntr; l += gridDim.x * blockDim.x) {
+            const long long o = (long long)I.rec_j[l] * P + I.rec_i[l];
+            const float s = I.res_p[(long long)l * I.nt + (nt - 1)];
+            I.sxx[o] = __fadd_rn(I.sxx[o], s);
+            I.syy[o] = __fadd_rn(I.syy[o], s);
+        }
+        return;
+    }
+    const int NT = I.nt;
+    const float DT = I.DT;
+    if (I.quelltyp_last == 1) {
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < I.nsrc_cells; c += gridDim.x * blockDim.x) {
+            const long long o = (long long)I.src_cell_j[c] * P + I.src_cell_i[c];
+            float sxx = I.sxx[o], syy = I.syy[o];
+            const int s0 = I.src_cell_start[c], ns = I.src_cell_count[c];
+            for (int k = 0; k < ns; k++) {
+                const float *sg = I.signals + (long long)I.src_perm[s0 + k] * NT;   // sg[n-1] = signals[l][n]
+                float amp = 0.0f;
+                if (nt == 1) amp = __fdiv_rn(sg[1], DT);
+                if (nt > 1 && nt < NT) amp = __fdiv_rn(__fsub_rn(sg[nt], sg[nt - 2]), DT);
+                if (nt == NT) amp = __fdiv_rn(-sg[nt - 2], DT);
+                sxx = __fadd_rn(sxx, amp);
+                syy = __fadd_rn(syy, amp);
+            }
+            I.sxx[o] = sxx;
+            I.syy[o] = syy;
+        }
+    } else if (I.quelltyp_last == 5) {
+        // neighbouring moment-tensor sources touch overlapping cells: one thread, list order
+        if (blockIdx.x != 0 || threadIdx.x != 0) return;
+        for (int cidx = 0; cidx < I.nsrc_cells; cidx++) {
+            const int s0 = I.src_cell_start[cidx], ns = I.src_cell_count[cidx];
+            for (int k = 0; k < ns; k++) {
+                const int l = I.src_perm[s0 + k];
+                const int si = I.src_cell_i[cidx], sj = I.src_cell_j[cidx];
+                const float *sg = I.signals + (long long)l * NT;
+                float amp = 0.0f;
+                if (nt == 1) amp = __fdiv_rn(sg[1], DT);
+                if (nt > 1 && nt < NT) amp = __fdiv_rn(__fsub_rn(sg[nt], sg[nt - 2]), DT);
+                if (nt == NT) amp = __fdiv_rn(-sg[nt - 2], DT);
+                const long long o = (long long)sj * P + si;
+                I.sxx[o] = __fadd_rn(I.sxx[o], __fmul_rn(amp, 0.0f));
+                I.syy[o] = __fadd_rn(I.syy[o], __fmul_rn(amp, 0.0f));
+                const double a4 = DMUL(DMUL(0.25, (double)amp), 1.0);
+                const long long o2[4] = {o, o - 1, o - P, o - P - 1};
+                for (int z = 0; z < 4; z++) I.sxy[o2[z]] = F(DADD((double)I.sxy[o2[z]], a4));
+            }
+        }
+    }
+}
+
+// ===========================================================================
+// Free surface at row j = 1 (image method), surface_elastic_PML_PSV.c:29-103.
+// ===========================================================================
+template <int R, bool X>
+__global__ void k_surface_el(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+{
+    const int nt = __ldg(ntb) + off;
+    const Inst &I = insts[blockIdx.y];
+    if (nt > I.nt || !I.free_surf) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (i > I.nx) return;
+    const long long P = I.pitch;
+    const int j = 1;
+    const long long o = (long long)j * P + i;
+    I.syy[o] = 0.0f;
+    float vxx = 0.0f, vyy = 0.0f;
+#pragma unroll
+    for (int m = 1; m <= R; m++) {
+        I.syy[o - m * P] = -I.syy[o + m * P];
+        I.sxy[o - m * P] = -I.sxy[o + (m - 1) * P];
+        vxx = ADD<X>(vxx, MUL<X>(I.hc[m], SUB<X>(I.vx[o + m - 1], I.vx[o - m])));
+        vyy = ADD<X>(vyy, MUL<X>(I.hc[m], SUB<X>(I.vy[o + (m - 1) * P], I.vy[o - m * P])));
+    }
+    vxx = MUL<X>(vxx, I.dh1);
+    vyy = MUL<X>(vyy, I.dh1);
+    const int fw = I.fw, nx = I.nx;
+    if (fw > 0) {
+        if (i <= fw) {
+            const int h = i - 1;
+            float *ps = I.psi_vxxs + (long long)(j - 1) * 2 * fw + h;
+            float v = ADD<X>(MUL<X>(I.b_x[h], *ps), MUL<X>(I.a_x[h], vxx));
+            *ps = v;
+            vxx = ADD<X>(DIV<X>(vxx, I.K_x[h]), v);
+        }
+        if (i >= nx - fw + 1) {
+            const int h = i - nx + 2 * fw - 1;
+            float *ps = I.psi_vxxs + (long long)(j - 1) * 2 * fw + h;
+            float v = ADD<X>(MUL<X>(I.b_x[h], *ps), MUL<X>(I.a_x[h], vxx));
+            *ps = v;
+            vxx = ADD<X>(DIV<X>(vxx, I.K_x[h]), v);
+        }
+    }
+    const float g = I.lam[o];
+    const float fjm = MUL<X>(I.mu[o], 2.0f);   // rho*u*u*2.0 (exact doubling)
+    const float t1 = MUL<X>(DIV<X>(MUL<X>(g, g), ADD<X>(g, fjm)), vxx);
+    const float t2 = MUL<X>(g, vyy);
+    I.sxx[o] = ADD<X>(I.sxx[o], MUL<X>(-I.DT, ADD<X>(t1, t2)));
+}
+
+// ===========================================================================
+// Viscoelastic free surface, surface_visc_PML_PSV.c:60-170 (relaxed moduli
+// from ws = 2 pi / TS, per-column constants precomputed on the host).
+// ===========================================================================
+template <int R, int L, bool X>
+__global__ void k_surface_vi(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+{
+    const int nt = __ldg(ntb) + off;
+    const Inst &I = insts[blockIdx.y];
+    if (nt > I.nt || !I.free_surf) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (i > I.nx) return;
+    const long long P = I.pitch;
+    const int j = 1;
+    const long long o = (long long)j * P + i;
+    I.syy[o] = 0.0f;
+#pragma unroll
+    for (int l = 0; l < L; l++) I.q[o + l * I.plane] = 0.0f;
+    float vxx = 0.0f, vyy = 0.0f;
+#pragma unroll
+    for (int m = 1; m <= R; m++) {
+        I.syy[o - m * P] = -I.syy[o + m * P];
+        I.sxy[o - m * P] = -I.sxy[o + (m - 1) * P];
+        vxx = ADD<X>(vxx, MUL<X>(I.hc[m], SUB<X>(I.vx[o + m - 1], I.vx[o - m])));
+        vyy = ADD<X>(vyy, MUL<X>(I.hc[m], SUB<X>(I.vy[o + (m - 1) * P], I.vy[o - m * P])));
+    }
+    vxx = MUL<X>(vxx, I.dh1);
+    vyy = MUL<X>(vyy, I.dh1);
+    const int fw = I.fw, nx = I.nx;
+    if (fw > 0) {
+        if (i <= fw) {
+            const int h = i - 1;
+            float *ps = I.psi_vxxs + (long long)(j - 1) * 2 * fw + h;
+            float v = ADD<X>(MUL<X>(I.b_x[h], *ps), MUL<X>(I.a_x[h], vxx));
+            *ps = v;
+            vxx = ADD<X>(DIV<X>(vxx, I.K_x[h]), v);
+        }
+        if (i >= nx - fw + 1) {
+            const int h = i - nx + 2 * fw - 1;
+            float *ps = I.psi_vxxs + (long long)(j - 1) * 2 * fw + h;
+            float v = ADD<X>(MUL<X>(I.b_x[h], *ps), MUL<X>(I.a_x[h], vxx));
+            *ps = v;
+            vxx = ADD<X>(DIV<X>(vxx, I.K_x[h]), v);
+        }
+    }
+    const float mu = I.s_mu[i - 1], pi = I.s_pi[i - 1], taus = I.s_taus[i - 1], taup = I.s_taup[i - 1];
+    const float DT = I.DT, dthalbe = I.dthalbe;
+    const float fL = (float)L;
+    float sump = 0.0f;
+#pragma unroll
+    for (int l = 0; l < L; l++) sump = ADD<X>(sump, I.p[o + l * I.plane]);
+    const float fjm = F(DMUL(DMUL((double)mu, 2.0), DADD(1.0, (double)MUL<X>(fL, taus))));
+    const float g = F(DMUL((double)pi, DADD(1.0, (double)MUL<X>(fL, taup))));
+    const float gf = SUB<X>(g, fjm);
+    const float DTgf = MUL<X>(DT, gf);
+    float a = -DIV<X>(MUL<X>(MUL<X>(DTgf, gf), vxx), g);
+    a = SUB<X>(a, MUL<X>(DTgf, vyy));
+    a = SUB<X>(a, MUL<X>(dthalbe, sump));
+    float sxx = ADD<X>(I.sxx[o], a);
+    sump = 0.0f;
+    const float djm = F(DMUL(DMUL(2.0, (double)mu), (double)taus));
+    const float e = MUL<X>(pi, taup);
+    const float de = SUB<X>(djm, e);
+    const double fg1 = DSUB((double)DIV<X>(fjm, g), 1.0);
+#pragma unroll
+    for (int l = 0; l < L; l++) {
+        const float bjm = I.s_bjm[l];
+        const double inner = DSUB(DMUL(DMUL((double)de, fg1), (double)vxx), (double)MUL<X>(de, vyy));
+        const float pv = F(DADD((double)I.p[o + l * I.plane], DMUL((double)bjm, inner)));
+        I.p[o + l * I.plane] = pv;
+        sump = ADD<X>(sump, pv);
+    }
+    I.sxx[o] = ADD<X>(sxx, MUL<X>(dthalbe, sump));
+}
+
+// ===========================================================================
+// Receivers, seismo_ssg.c:24-105 (SEISMO 1..4), sample nt of every trace,
+// plus the psv.c:99 NaN probe on vy[NY/2][NX/2].
+// sec layout: [comp][nt][ntr] (comp 0 vx, 1 vy, 2 p, 3 curl, 4 div).
+// ===========================================================================
+template <int R>
+__global__ void k_seismo(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+{
+    const int nt = __ldg(ntb) + off;
+    const Inst &I = insts[blockIdx.y];
+    if (nt > I.nt) return;
+    const long long P = I.pitch;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        float v = I.vy[(long long)(I.ny / 2) * P + I.nx / 2];
+        if (isnan(v)) atomicOr(I.flag, 1);
+    }
+    if (I.mode == 1 || !I.seismo) return;
+    const long long slab = (long long)I.nt * I.ntr;
+    for (int itr = blockIdx.x * blockDim.x + threadIdx.x; itr < I.ntr; itr += gridDim.x * blockDim.x) {
+        const int i = I.rec_i[itr], j = I.rec_j[itr];
+        const long long o = (long long)j * P + i;
+        const long long s = (long long)(nt - 1) * I.ntr + itr;
+        const int S = I.seismo;
+        if (S == 1 || S == 4) {
+            I.sec[0 * slab + s] = I.vx[o];
+            I.sec[1 * slab + s] = I.vy[o];
+        }
+        if (S == 2 || S == 4) I.sec[2 * slab + s] = __fsub_rn(-I.sxx[o], I.syy[o]);
+        if (S == 3 || S == 4) {
+            float vxx = 0.0f, vyy = 0.0f, vyx = 0.0f, vxy = 0.0f;
+            for (int m = 1; m <= R; m++) {
+                const float h = I.hc[m];
+                vxx = __fadd_rn(vxx, __fmul_rn(h, __fsub_rn(I.vx[o + m - 1], I.vx[o - m])));
+                vyy = __fadd_rn(vyy, __fmul_rn(h, __fsub_rn(I.vy[o + (m - 1) * P], I.vy[o - m * P])));
+                vyx = __fadd_rn(vyx, __fmul_rn(h, __fsub_rn(I.vy[o + m], I.vy[o - m + 1])));
+                vxy = __fadd_rn(vxy, __fmul_rn(h, __fsub_rn(I.vx[o + m * P], I.vx[o - (m - 1) * P])));
+            }
+            const float dhi = I.dhi_el;
+            vxx = __fmul_rn(vxx, dhi);
+            vyy = __fmul_rn(vyy, dhi);
+            vyx = __fmul_rn(vyx, dhi);
+            vxy = __fmul_rn(vxy, dhi);
+            const float u = I.vs[o], pi = I.vp[o], rho = I.rho[o];
+            const float muss = __fmul_rn(__fmul_rn(u, u), rho);
+            const float lamss = __fmul_rn(__fmul_rn(pi, pi), rho);
+            I.sec[4 * slab + s] = F(DMUL((double)__fadd_rn(vxx, vyy), sqrt((double)lamss)));
+            I.sec[3 * slab + s] = F(DMUL((double)__fsub_rn(vxy, vyx), sqrt((double)muss)));
+        }
+    }
+}
+
+// ===========================================================================
+// Snapshot encoding.  Snapshot k holds the five fields of psv.c:246-298
+// (vxp1, vyp1, sxx, syy, sxy) of forward step 1 + k*DTINV.  Each field of
+// each tile (blockDim.x x zch cells) carries its own power-of-two scale so
+// FP16 keeps ~11 significant bits over the whole dynamic range.
+// ===========================================================================
+__device__ __forceinline__ float warp_max(float v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float block_max(float v, float *red)
+{
+    v = warp_max(v);
+    const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if ((threadIdx.x & 31) == 0) red[w] = v;
+    __syncthreads();
+    float m = 0.0f;
+    for (int k = 0; k < nw; k++) m = fmaxf(m, red[k]);
+    __syncthreads();
+    return m;
+}
+
+// scale s = 2^e with e chosen so max|x| / s lies in [2^14, 2^15)
+__device__ __forceinline__ float pow2_scale(float amax)
+{
+    if (!(amax > 0.0f) || isinf(amax)) return 1.0f;
+    int e;
+    frexpf(amax, &e);   // amax = f * 2^e, f in [0.5, 1)
+    return ldexpf(1.0f, e - 15);
+}
+
+__global__ void k_snap_store(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+{
+    const int nt = __ldg(ntb) + off;
+    const Inst &I = insts[blockIdx.y];
+    if (nt > I.nt || I.mode != 0 || !I.store || ((nt - 1) % I.dtinv) != 0) return;
+    const int k = (nt - 1) / I.dtinv;
+    if (k >= I.nsnap) return;
+    const int b = blockIdx.x;
+    if (b >= I.tiles) return;
+    __shared__ float red[32];
+    const int tx = b % I.tiles_x, tz = b / I.tiles_x;
+    const int i = tx * blockDim.x + threadIdx.x + 1;
+    const int j0 = tz * I.zch + 1;
+    const int nrow = min(I.zch, I.ny - j0 + 1);
+    const bool in = i <= I.nx;
+    const long long P = I.pitch;
+    const long long tile_cells = (long long)blockDim.x * I.zch;
+    const float *src[5] = {I.vxp1, I.vyp1, I.sxx, I.syy, I.sxy};
+    if (I.eprecond == 1 || I.eprecond == 3) {
+        for (int r = 0; r < nrow && in; r++) {
+            const long long o = (long long)(j0 + r) * P + i;
+            const long long w = (long long)(j0 + r - 1) * I.nx + (i - 1);
+            I.Ws[w] = __fadd_rn(I.Ws[w], __fadd_rn(__fmul_rn(I.vx[o], I.vx[o]), __fmul_rn(I.vy[o], I.vy[o])));
+        }
+    }
+    for (int f = 0; f < 5; f++) {
+        const long long slot = ((long long)k * 5 + f) * I.tiles + b;
+        const long long base = slot * tile_cells;
+        if (I.snap_prec == DN_SNAP_F32) {
+            float *dst = (float *)I.snap + base;
+            for (int r = 0; r < nrow; r++)
+                if (in) dst[(long long)r * blockDim.x + threadIdx.x] = src[f][(long long)(j0 + r) * P + i];
+            continue;
+        }
+        float amax = 0.0f;
+        for (int r = 0; r < nrow && in; r++) amax = fmaxf(amax, fabsf(src[f][(long long)(j0 + r) * P + i]));
+        amax = block_max(amax, red);
+        const float s = pow2_scale(amax);
+        const float inv = 1.0f / s;   // exact: power of two
+        if (threadIdx.x == 0) I.snap_scale[slot] = s;
+        if (I.snap_prec == DN_SNAP_F16) {
+            __half *dst = (__half *)I.snap + base;
+            for (int r = 0; r < nrow; r++)
+                if (in) dst[(long long)r * blockDim.x + threadIdx.x] = __float2half_rn(src[f][(long long)(j0 + r) * P + i] * inv);
+        } else {
+            __nv_bfloat16 *dst = (__nv_bfloat16 *)I.snap + base;
+            for (int r = 0; r < nrow; r++)
+                if (in) dst[(long long)r * blockDim.x + threadIdx.x] = __float2bfloat16_rn(src[f][(long long)(j0 + r) * P + i] * inv);
+        }
+    }
+}
+
+__device__ __forceinline__ float snap_load(const Inst &I, long long slot, long long idx)
+{
+    const long long tile_cells = (long long)blockDim.x * I.zch;
+    const long long e = slot * tile_cells + idx;
+    if (I.snap_prec == DN_SNAP_F32) return ((const float *)I.snap)[e];
+    const float s = I.snap_scale[slot];
+    if (I.snap_prec == DN_SNAP_F16) return __half2float(((const __half *)I.snap)[e]) * s;
+    return __bfloat162float(((const __nv_bfloat16 *)I.snap)[e]) * s;
+}
+
+// ===========================================================================
+// Adjoint cross-correlation, psv.c:313-387 (GRAD_FORM 1, INVMAT1 1), at the
+// adjoint steps whose mirrored forward step NT-nt+1 stored a snapshot.
+// ===========================================================================
+__global__ void k_correlate(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+{
+    const int nt = __ldg(ntb) + off;
+    const Inst &I = insts[blockIdx.y];
+    if (nt > I.nt || I.mode != 1) return;
+    const int nf = I.nt - nt + 1;   // mirrored forward step
+    if (((nf - 1) % I.dtinv) != 0) return;
+    const int k = (nf - 1) / I.dtinv;
+    if (k >= I.nsnap) return;
+    const int b = blockIdx.x;
+    if (b >= I.tiles) return;
+    const int tx = b % I.tiles_x, tz = b / I.tiles_x;
+    const int i = tx * blockDim.x + threadIdx.x + 1;
+    if (i > I.nx) return;
+    const int j0 = tz * I.zch + 1;
+    const int nrow = min(I.zch, I.ny - j0 + 1);
+    const long long P = I.pitch;
+    for (int r = 0; r < nrow; r++) {
+        const int j = j0 + r;
+        const long long o = (long long)j * P + i;
+        const long long idx = (long long)r * blockDim.x + threadIdx.x;
+        const long long s0 = ((long long)k * 5) * I.tiles + b;
+        const float frx = snap_load(I, s0 + 0 * (long long)I.tiles, idx);
+        const float fry = snap_load(I, s0 + 1 * (long long)I.tiles, idx);
+        const float fx = snap_load(I, s0 + 2 * (long long)I.tiles, idx);
+        const float fy = snap_load(I, s0 + 3 * (long long)I.tiles, idx);
+        const float fu = snap_load(I, s0 + 4 * (long long)I.tiles, idx);
+        const float vxp1 = I.vxp1[o], vyp1 = I.vyp1[o];
+        const float sxx = I.sxx[o], syy = I.syy[o], sxy = I.sxy[o];
+        const float trho = __fadd_rn(__fmul_rn(vxp1, frx), __fmul_rn(vyp1, fry));
+        const float tlam = __fmul_rn(__fadd_rn(fx, fy), __fadd_rn(sxx, syy));
+        const float muss = I.gmuss[o], lamss = I.glamss[o];
+        double tmu = 0.0;
+        const bool mpos = muss > 0.0f;
+        if (mpos) {
+            const double mm = (double)__fmul_rn(muss, muss);
+            const float lm = __fadd_rn(lamss, muss);
+            const double t1 = DMUL(DDIV(1.0, mm), (double)__fmul_rn(fu, sxy));
+            const double t2 = DDIV(DMUL(0.25, (double)tlam), (double)__fmul_rn(lm, lm));
+            const double t3 = DDIV(DMUL(0.25, (double)__fmul_rn(__fsub_rn(fx, fy), __fsub_rn(sxx, syy))), mm);
+            tmu = DADD(DADD(t1, t2), t3);
+        }
+        const long long w = (long long)(j - 1) * I.nx + (i - 1);
+        if (I.acc64) {
+            double *wc = (double *)I.wc, *wcu = (double *)I.wcu, *wcr = (double *)I.wcrho;
+            wcr[w] = DADD(wcr[w], (double)trho);
+            wc[w] = DADD(wc[w], (double)tlam);
+            if (mpos) wcu[w] = DADD(wcu[w], tmu);
+        } else {
+            float *wc = (float *)I.wc, *wcu = (float *)I.wcu, *wcr = (float *)I.wcrho;
+            wcr[w] = __fadd_rn(wcr[w], trho);
+            wc[w] = __fadd_rn(wc[w], tlam);
+            if (mpos) wcu[w] = F(DADD((double)wcu[w], tmu));
+        }
+        if (I.eprecond == 1)
+            I.Wr[w] = __fadd_rn(I.Wr[w], __fadd_rn(__fmul_rn(I.vx[o], I.vx[o]), __fmul_rn(I.vy[o], I.vy[o])));
+    }
+}
+
+}   // namespace dn

@@ -1,0 +1,167 @@
+"""ctypes binding of libdenise_b200.so (the C ABI in include/denise_b200.h).
+
+The shared library is built in-tree by ``denise-black-edition_b200/build.py``.
+Importing this module loads it; if it is missing the import fails loudly -
+there is no CPU fallback for the propagator.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(_HERE)
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libdenise_b200.so")
+
+DN_MAX_L = 5
+
+DN_OK = 0
+DN_EINVAL = -1
+DN_ENOMEM = -2
+DN_EUNSTABLE = -3
+DN_ETIMEDOUT = -4
+DN_EDEVICE = -5
+DN_ENOTSUP = -6
+DN_EIO = -7
+DN_ESTATE = -8
+
+ERROR_NAMES = {
+    DN_EINVAL: "DN_EINVAL", DN_ENOMEM: "DN_ENOMEM", DN_EUNSTABLE: "DN_EUNSTABLE",
+    DN_ETIMEDOUT: "DN_ETIMEDOUT", DN_EDEVICE: "DN_EDEVICE", DN_ENOTSUP: "DN_ENOTSUP",
+    DN_EIO: "DN_EIO", DN_ESTATE: "DN_ESTATE",
+}
+
+MODE_FORWARD, MODE_ADJOINT, MODE_OBJECTIVE = 0, 1, 2
+SNAP_F32, SNAP_F16, SNAP_BF16 = 0, 1, 2
+ACC_F32, ACC_F64 = 0, 1
+ARITH_EXACT, ARITH_FMA = 0, 1
+SEC_VX, SEC_VY, SEC_P, SEC_CURL, SEC_DIV = 0, 1, 2, 3, 4
+
+
+class DeniseError(RuntimeError):
+    """A DN_E* status returned by the library; ``code`` holds the value."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("dh", ctypes.c_float), ("dt", ctypes.c_float),
+        ("nt", ctypes.c_int), ("fdorder", ctypes.c_int), ("maxrelerror", ctypes.c_int),
+        ("free_surf", ctypes.c_int), ("fw", ctypes.c_int),
+        ("damping", ctypes.c_float), ("fpml", ctypes.c_float),
+        ("npower", ctypes.c_float), ("k_max_pml", ctypes.c_float),
+        ("boundary", ctypes.c_int), ("L", ctypes.c_int),
+        ("fl", ctypes.c_float * DN_MAX_L), ("ts", ctypes.c_float),
+        ("invmat1", ctypes.c_int), ("grad_form", ctypes.c_int), ("quelltypb", ctypes.c_int),
+        ("seismo", ctypes.c_int), ("dtinv", ctypes.c_int), ("eprecond", ctypes.c_int),
+        ("store_snapshots", ctypes.c_int), ("snap_precision", ctypes.c_int),
+        ("grad_accum", ctypes.c_int), ("arith", ctypes.c_int), ("honor_q", ctypes.c_int),
+    ]
+
+
+class Acq(ctypes.Structure):
+    _fields_ = [
+        ("nsrc", ctypes.c_int),
+        ("src_i", ctypes.POINTER(ctypes.c_int)), ("src_j", ctypes.POINTER(ctypes.c_int)),
+        ("src_type", ctypes.POINTER(ctypes.c_int)), ("src_azi", ctypes.POINTER(ctypes.c_float)),
+        ("signals", ctypes.POINTER(ctypes.c_float)),
+        ("ntr", ctypes.c_int),
+        ("rec_i", ctypes.POINTER(ctypes.c_int)), ("rec_j", ctypes.POINTER(ctypes.c_int)),
+    ]
+
+
+class Pml(ctypes.Structure):
+    _fields_ = [(n, ctypes.POINTER(ctypes.c_float)) for n in (
+        "d_x", "K_x", "alpha_prime_x", "a_x", "b_x",
+        "d_x_half", "K_x_half", "alpha_prime_x_half", "a_x_half", "b_x_half",
+        "d_y", "K_y", "alpha_prime_y", "a_y", "b_y",
+        "d_y_half", "K_y_half", "alpha_prime_y_half", "a_y_half", "b_y_half")]
+
+
+PML_NAMES = [f[0] for f in Pml._fields_]
+
+# every function the header declares, with its argument types
+_P = ctypes.POINTER
+_c_int_p = _P(ctypes.c_int)
+_c_float_p = _P(ctypes.c_float)
+_c_double_p = _P(ctypes.c_double)
+_vp = ctypes.c_void_p
+SIGNATURES = {
+    "dn_last_error": (ctypes.c_char_p, []),
+    "dn_version": (ctypes.c_int, [_c_int_p, _c_int_p]),
+    "dn_device_count": (ctypes.c_int, [_c_int_p]),
+    "dn_holbergcoeff": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_float_p]),
+    "dn_pml_profiles": (ctypes.c_int, [_P(Params), _P(Pml)]),
+    "dn_cfl_check": (ctypes.c_int, [_P(Params), ctypes.c_float, _c_double_p]),
+    "dn_average_materials": (ctypes.c_int, [_P(Params), _c_float_p, _c_float_p, _c_float_p,
+                                            _c_float_p, _c_float_p, _c_float_p]),
+    "dn_prepare_visc": (ctypes.c_int, [_P(Params)] + [_c_float_p] * 16),
+    "dn_wavelet": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                  ctypes.c_float, ctypes.c_float, ctypes.c_int, _c_float_p]),
+    "dn_model_create": (ctypes.c_int, [_P(Params), _c_float_p, _c_float_p, _c_float_p,
+                                       _c_float_p, _c_float_p, ctypes.c_int, _P(_vp)]),
+    "dn_model_destroy": (ctypes.c_int, [_vp]),
+    "dn_model_params": (ctypes.c_int, [_vp, _P(Params)]),
+    "dn_model_footprint": (ctypes.c_int, [_P(Params), _P(ctypes.c_size_t)]),
+    "dn_shot_footprint": (ctypes.c_int, [_P(Params), ctypes.c_int, ctypes.c_int, _P(ctypes.c_size_t)]),
+    "dn_shot_create": (ctypes.c_int, [_vp, _P(Acq), _P(_vp)]),
+    "dn_shot_destroy": (ctypes.c_int, [_vp]),
+    "dn_run": (ctypes.c_int, [_P(_vp), ctypes.c_int, ctypes.c_int]),
+    "dn_run_plain": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "dn_shot_get_sections": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p]),
+    "dn_shot_set_residuals": (ctypes.c_int, [_vp, _c_float_p, _c_float_p, _c_float_p]),
+    "dn_shot_accumulate_gradient": (ctypes.c_int, [_vp]),
+    "dn_model_get_gradient": (ctypes.c_int, [_vp, _c_float_p, _c_float_p, _c_float_p]),
+    "dn_model_zero_gradient": (ctypes.c_int, [_vp]),
+    "dn_shot_get_field": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p]),
+    "dn_run_steps": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "dn_shot_get_snapshot": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_float_p]),
+    "dn_last_run_stats": (ctypes.c_int, [_c_double_p, _P(ctypes.c_longlong)]),
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python denise-black-edition_b200/build.py` "
+            "(the propagator has no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(code):
+    if code != DN_OK:
+        raise DeniseError(code, lib.dn_last_error().decode(errors="replace"))
+    return code
+
+
+def fptr(a):
+    """float32 C-contiguous array -> float*; None -> NULL."""
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_c_float_p)
+
+
+def iptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_c_int_p)
+
+
+def device_count():
+    n = ctypes.c_int(0)
+    lib.dn_device_count(ctypes.byref(n))
+    return n.value

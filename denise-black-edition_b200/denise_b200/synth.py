@@ -1,0 +1,152 @@
+"""Seeded synthetic inputs of the benchmark workloads.
+
+No public dataset is named for this path; the reference's Marmousi-II inputs
+are not available.  Every model here is drawn from one seeded family:
+
+* vp(z) = 1800 + 2700 z / z_max, plus 6 layer boundaries at depths uniform in
+  (0, z_max) that each add a jump uniform in (-300, 300) m/s below them, plus
+  Gaussian-smoothed (sigma 10 cells) N(0, 1) noise normalised to max |.| = 1
+  and scaled by 0.05 vp;
+* vs = max(vp / 1.73, 1000), rho = 310 vp^0.25 (Gardner);
+* viscoelastic runs add Qp ~ U(60, 120), Qs ~ U(30, 60) per model, times
+  (1 + 0.1 smoothed noise).
+
+Arrays have the reference's file order, shape (nx, ny).
+"""
+import math
+
+import numpy as np
+
+from .api import PsvParams, wavelet
+
+
+def _smooth(noise, sigma):
+    from scipy.ndimage import gaussian_filter
+
+    return gaussian_filter(noise, sigma=sigma, mode="nearest")
+
+
+def base_model(nx, ny, dh, seed, smooth_sigma=10.0):
+    rng = np.random.default_rng(seed)
+    z = np.arange(ny, dtype=np.float64) * dh
+    zmax = max(z[-1], dh)
+    vp1 = 1800.0 + 2700.0 * z / zmax
+    depths = rng.uniform(0.0, zmax, 6)
+    jumps = rng.uniform(-300.0, 300.0, 6)
+    for d, jmp in zip(depths, jumps):
+        vp1 = vp1 + np.where(z >= d, jmp, 0.0)
+    vp = np.broadcast_to(vp1[None, :], (nx, ny)).copy()
+    pert = _smooth(rng.standard_normal((nx, ny)), smooth_sigma)
+    pert /= max(np.abs(pert).max(), 1e-30)
+    vp = vp * (1.0 + 0.05 * pert)
+    vs = np.maximum(vp / 1.73, 1000.0)
+    rho = 310.0 * vp ** 0.25
+    return vp.astype(np.float32), vs.astype(np.float32), rho.astype(np.float32)
+
+
+def q_model(nx, ny, seed, smooth_sigma=10.0):
+    rng = np.random.default_rng(seed + 7919)
+    qp0 = rng.uniform(60.0, 120.0)
+    qs0 = rng.uniform(30.0, 60.0)
+    n = _smooth(rng.standard_normal((nx, ny)), smooth_sigma)
+    n /= max(np.abs(n).max(), 1e-30)
+    return (qp0 * (1 + 0.1 * n)).astype(np.float32), (qs0 * (1 + 0.1 * n)).astype(np.float32)
+
+
+def smoothed(a, sigma):
+    return _smooth(np.asarray(a, np.float64), sigma).astype(np.float32)
+
+
+def add_ellipse(vp, vs, rho, dh, seed, v=5500.0):
+    rng = np.random.default_rng(seed + 104729)
+    nx, ny = vp.shape
+    cx, cz = rng.uniform(0.3, 0.7) * nx, rng.uniform(0.4, 0.7) * ny
+    ax, az = rng.uniform(0.05, 0.12) * nx, rng.uniform(0.05, 0.12) * ny
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    m = ((ii - cx) / ax) ** 2 + ((jj - cz) / az) ** 2 <= 1.0
+    vp = vp.copy()
+    vp[m] = v
+    return vp, np.maximum(vp / 1.73, 1000.0).astype(np.float32), (310.0 * vp ** 0.25).astype(np.float32)
+
+
+def iround(x):
+    """fd.h:17: (int)floor(x + 0.5)."""
+    return int(math.floor(x + 0.5))
+
+
+def grid_index(x_m, dh):
+    """Grid index of a source/receiver coordinate (sources.c, splitsrc.c:27, receiver.c:55)."""
+    return iround(np.float32(x_m) / np.float32(dh))
+
+
+def receivers_line(x0, x1, n, z, dh):
+    xs = np.linspace(x0, x1, n)
+    ri = np.array([grid_index(x, dh) for x in xs], np.int32)
+    rj = np.full(n, grid_index(z, dh), np.int32)
+    # receiver.c:63-83 removes receivers sharing a grid point
+    keep, seen = [], set()
+    for k in range(n):
+        key = (int(ri[k]), int(rj[k]))
+        if key not in seen:
+            seen.add(key)
+            keep.append(k)
+    return ri[keep], rj[keep]
+
+
+def ricker_source(p: PsvParams, fc, amp=1.0, tshift=0.0):
+    return wavelet(1, p.nt, p.dt, tshift, fc, amp)
+
+
+# ---------------------------------------------------------------------------
+# the benchmark configurations
+# ---------------------------------------------------------------------------
+def c0_params(**kw):
+    """Plain elastic forward: 600 x 300, DH 5 m, DT 0.4 ms, NT 5000, FDORDER 8, FW 20, free surface."""
+    base = dict(nx=600, ny=300, dh=5.0, dt=4e-4, nt=5000, fdorder=8, maxrelerror=1, free_surf=1, fw=20,
+                damping=1500.0, fpml=10.0, npower=4.0, k_max_pml=1.0, ts=0.1)
+    base.update(kw)
+    return PsvParams(**base)
+
+
+def c0_case(seed=0, **kw):
+    p = c0_params(**kw)
+    vp, vs, rho = base_model(p.nx, p.ny, p.dh, seed)
+    sig = ricker_source(p, 10.0)[None, :]
+    si = np.array([grid_index(1500.0 * p.nx / 600.0, p.dh)], np.int32)
+    sj = np.array([max(grid_index(10.0, p.dh), 1)], np.int32)
+    ri, rj = receivers_line(100.0 * p.nx / 600.0, 2900.0 * p.nx / 600.0, 120, 20.0, p.dh)
+    return p, (vp, vs, rho), (si, sj, sig), (ri, rj)
+
+
+C1_FL = (2.0, 8.0, 25.0)   # relaxation frequencies for L = 3 (not given by the workload; chosen here)
+
+
+def c1_params(**kw):
+    """Batched viscoelastic: 2000 x 600, DH 5, DT 0.4 ms, NT 6000, FDORDER 8, L 3."""
+    base = dict(nx=2000, ny=600, dh=5.0, dt=4e-4, nt=6000, fdorder=8, maxrelerror=1, free_surf=1, fw=20,
+                damping=1500.0, fpml=10.0, npower=4.0, k_max_pml=1.0, L=3, fl=C1_FL, ts=1.0 / 8.0)
+    base.update(kw)
+    return PsvParams(**base)
+
+
+def c1_shot(p: PsvParams, k, nshots=64, seed=None):
+    """Shot k of the batched workload: its own model (seed k+1), source k of nshots."""
+    seed = k + 1 if seed is None else seed
+    vp, vs, rho = base_model(p.nx, p.ny, p.dh, seed)
+    qp, qs = q_model(p.nx, p.ny, seed)
+    xmax = (p.nx - 1) * p.dh
+    xs = 200.0 + (xmax - 400.0) * k / max(nshots - 1, 1)
+    si = np.array([grid_index(xs, p.dh)], np.int32)
+    sj = np.array([max(grid_index(10.0, p.dh), 1)], np.int32)
+    sig = ricker_source(p, 8.0)[None, :]
+    ri, rj = receivers_line(100.0, xmax - 100.0, 400, 20.0, p.dh)
+    return (vp, vs, rho, qp, qs), (si, sj, sig), (ri, rj)
+
+
+def c2_params(**kw):
+    """FWI gradient: 1700 x 500, DH 10, DT 1 ms, NT 4000, FDORDER 8, DTINV 2."""
+    base = dict(nx=1700, ny=500, dh=10.0, dt=1e-3, nt=4000, fdorder=8, maxrelerror=1, free_surf=1, fw=20,
+                damping=1500.0, fpml=10.0, npower=4.0, k_max_pml=1.0, ts=1.0 / 8.0, dtinv=2, quelltypb=1,
+                store_snapshots=1)
+    base.update(kw)
+    return PsvParams(**base)

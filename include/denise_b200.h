@@ -1,0 +1,229 @@
+/*
+ * denise_b200.h - C ABI of the B200 P-SV propagator and FWI adjoint gradient.
+ *
+ * This library replaces the reference's single-shot time loop
+ *   psv()                     src/PSV/psv.c:17            (modes 0/1/2)
+ * and everything it calls per time step:
+ *   update_v_PML_PSV          include/fd.h:324            (velocity + CPML + force/adjoint sources)
+ *   update_s_elastic_PML_PSV  include/fd.h:309            (elastic stress + CPML)
+ *   update_s_visc_PML_PSV     include/fd.h:316            (viscoelastic stress + memory variables)
+ *   surface_elastic_PML_PSV   include/fd.h:297, surface_visc_PML_PSV include/fd.h:300
+ *   psource / msource         include/fd.h:858 / :827
+ *   seismo_ssg                include/fd.h:904
+ *   eprecond                  include/fd.h:779
+ *   zero_denise_*_PSV         include/fd.h:331 / :335
+ *   the forward-snapshot store and adjoint cross-correlation inlined at src/PSV/psv.c:240-387,
+ *   the per-shot gradient assembly ass_gradPSV (src/PSV/ass_gradPSV.c:10),
+ * together with the MPI halo exchange (exchange_v/s_PSV), which disappears because
+ * the whole grid of a shot lives on one GPU.
+ *
+ * Set-up numerics that the reference computes on the host (PML_pro, holbergcoeff,
+ * av_mue/av_rho/av_tau with the single-rank periodic material wrap of matcopy_*,
+ * prepare_update_s_visc_PSV) are exported too; they are computed in host C with
+ * the reference's float/double promotion rules and are bit-identical to it.
+ *
+ * Conventions
+ *  - Grid indices are the reference's: i = 1..nx (x, contiguous in its files),
+ *    j = 1..ny (depth).  A source/receiver at (i, j) is the reference's
+ *    srcpos_loc[1..2] / recpos_loc[1..2].
+ *  - Model, gradient and snapshot arrays cross the ABI in the reference's FILE
+ *    order (readmod_elastic_PSV.c:72-85, extract_LBFGS_PSV.c:84-200): x-major,
+ *    z contiguous, a[(i-1)*ny + (j-1)].
+ *  - Seismic sections are [ntr][nt] row-major, sample k = time step k+1
+ *    (the reference's section[itr][nt], seismo_ssg.c:24).
+ *  - Every entry point returns an int status (DN_OK or a negative DN_E* code).
+ *    Nothing in the library exits or aborts; the host driver maps errors to the
+ *    reference's err() behaviour.
+ *  - Objects are not thread-safe; use one model/shot set per host thread.
+ */
+#ifndef DENISE_B200_H
+#define DENISE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DN_VERSION_MAJOR 0
+#define DN_VERSION_MINOR 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define DN_OK 0
+#define DN_EINVAL (-1)     /* bad parameter: FDORDER, MAXRELERROR, sizes, CFL ... */
+#define DN_ENOMEM (-2)     /* device or host allocation failed */
+#define DN_EUNSTABLE (-3)  /* NaN in the wavefield (psv.c:99-103 "Simulation is unstable") */
+#define DN_ETIMEDOUT (-4)  /* a bounded device/host wait ran out */
+#define DN_EDEVICE (-5)    /* CUDA error; see dn_last_error() */
+#define DN_ENOTSUP (-6)    /* option the propagator does not implement */
+#define DN_EIO (-7)        /* file could not be read / written */
+#define DN_ESTATE (-8)     /* call out of order (e.g. adjoint before a stored forward) */
+
+/* ---- enums ------------------------------------------------------------- */
+#define DN_MAX_L 5           /* max relaxation mechanisms */
+
+#define DN_MODE_FORWARD 0    /* psv() mode 0: forward, stores snapshots if params.store_snapshots */
+#define DN_MODE_ADJOINT 1    /* psv() mode 1: back-propagation + cross-correlation */
+#define DN_MODE_OBJECTIVE 2  /* psv() mode 2: forward for the objective only */
+
+#define DN_SNAP_F32 0        /* snapshot storage precision */
+#define DN_SNAP_F16 1        /* IEEE half with a per-snapshot, per-field power-of-two scale */
+#define DN_SNAP_BF16 2       /* bfloat16 with the same scaling */
+
+#define DN_ACC_F32 0         /* gradient accumulation in float, in the reference's order */
+#define DN_ACC_F64 1         /* gradient accumulation in double */
+
+#define DN_ARITH_EXACT 0     /* FP32 with the reference's operation order and double promotions */
+#define DN_ARITH_FMA 1       /* FP32 with fused multiply-add contraction (faster, not bit-exact) */
+
+/* section components (seismo_ssg.c SEISMO cases) */
+#define DN_SEC_VX 0
+#define DN_SEC_VY 1
+#define DN_SEC_P 2
+#define DN_SEC_CURL 3
+#define DN_SEC_DIV 4
+
+/* gradient components */
+#define DN_GRAD_VP 0
+#define DN_GRAD_VS 1
+#define DN_GRAD_RHO 2
+
+/* ---- parameters (the subset of read_par.c globals the path reads) ---------- */
+typedef struct dn_params {
+    int nx, ny;              /* NX, NY                               read_par.c case 7, 8 */
+    float dh;                /* DH                                   case 9 */
+    float dt;                /* DT                                   case 11 */
+    int nt;                  /* NT = iround(TIME/DT)                 FD_PSV.c:68 */
+    int fdorder;             /* FDORDER 2,4,...,12                   case 5 */
+    int maxrelerror;         /* MAXRELERROR 0..4                     case 6 */
+    int free_surf;           /* FREE_SURF                            case 28 */
+    int fw;                  /* FW (CPML width in points)            case 29 */
+    float damping;           /* DAMPING                              case 30 */
+    float fpml;              /* FPML                                 case 31 */
+    float npower;            /* npower                               case 32 */
+    float k_max_pml;         /* k_max_PML                            case 33 */
+    int boundary;            /* BOUNDARY (only 0 supported)          case 34 */
+    int L;                   /* relaxation mechanisms, 0 = elastic   case 25 */
+    float fl[DN_MAX_L];      /* FL[1..L]                             case 26 */
+    float ts;                /* TS = 1/max source fc (sources.c:90); used by the visco free surface */
+    int invmat1;             /* INVMAT1 (1 = vp,vs,rho)              case 66 */
+    int grad_form;           /* GRAD_FORM (1)                        case 67 */
+    int quelltypb;           /* QUELLTYPB adjoint source type        case 68 */
+    int seismo;              /* SEISMO 0..4                          case 44 */
+    int dtinv;               /* DTINV snapshot interval              case 95 */
+    int eprecond;            /* EPRECOND (0,1,3)                     workflow file */
+    int store_snapshots;     /* store forward snapshots in mode 0 (MODE>0 in the reference) */
+    int snap_precision;      /* DN_SNAP_* */
+    int grad_accum;          /* DN_ACC_* */
+    int arith;               /* DN_ARITH_* */
+    int honor_q;             /* 0: Q forced to 30 as readmod_visc_PSV.c:106-107; 1: use the qp/qs arrays */
+} dn_params;
+
+/* One shot's acquisition: sources (psource/update_v injection points) and
+ * receivers (seismo_ssg).  All pointers are host memory; copied at create. */
+typedef struct dn_acq {
+    int nsrc;
+    const int *src_i, *src_j;      /* grid indices of the sources, 1-based (splitsrc.c:27-28) */
+    const int *src_type;           /* QUELLTYP per source (srcpos[8]) 1 explosive, 2/3 force, 4 rotated, 5 moment */
+    const float *src_azi;          /* azimuth in degrees (srcpos[7]), may be NULL */
+    const float *signals;          /* [nsrc][nt] source time functions (wavelet.c) */
+    int ntr;
+    const int *rec_i, *rec_j;      /* receiver grid indices, 1-based (receiver.c:55-57) */
+} dn_acq;
+
+/* CPML profile vectors, each [2*fw], index h-1 for the reference's h = 1..2*FW
+ * (left/top frame in 1..FW, right/bottom in FW+1..2*FW; PML_pro.c:65-407). */
+typedef struct dn_pml {
+    float *d_x, *K_x, *alpha_prime_x, *a_x, *b_x;
+    float *d_x_half, *K_x_half, *alpha_prime_x_half, *a_x_half, *b_x_half;
+    float *d_y, *K_y, *alpha_prime_y, *a_y, *b_y;
+    float *d_y_half, *K_y_half, *alpha_prime_y_half, *a_y_half, *b_y_half;
+} dn_pml;
+
+typedef struct dn_model dn_model;   /* device-resident material coefficients for one grid */
+typedef struct dn_shot dn_shot;     /* device-resident wavefield state of one shot */
+
+/* ---- library ------------------------------------------------------------ */
+const char *dn_last_error(void);      /* thread-local text of the last failure */
+int dn_version(int *major, int *minor);
+int dn_device_count(int *count);
+
+/* ---- host set-up numerics (bit-identical to the reference) ----------------- */
+/* holbergcoeff(): src/holbergcoeff.c:19-90; hc[0..6] */
+int dn_holbergcoeff(int fdorder, int maxrelerror, float hc[7]);
+/* PML_pro(): src/PML_pro.c:65-407; every dn_pml vector must hold 2*fw floats */
+int dn_pml_profiles(const dn_params *p, dn_pml *out);
+/* CFL limit of checkfd_ssg_elastic(): src/checkfd_ssg_elastic.c:89,126 */
+int dn_cfl_check(const dn_params *p, float vp_max, double *dtstab);
+/* matcopy_elastic_PSV (single-rank periodic wrap) + av_mue + av_rho:
+ * src/PSV/matcopy_elastic_PSV.c, src/av_mue.c:4-51, src/av_rho.c:5-28.
+ * Inputs and outputs in file order [nx*ny]. */
+int dn_average_materials(const dn_params *p, const float *vp, const float *vs, const float *rho,
+                         float *uipjp, float *rip, float *rjp);
+/* readmod_visc_PSV tau/eta (src/PSV/readmod_visc_PSV.c:31-120), matcopy_PSV wrap, av_tau
+ * (src/av_tau.c:5-15) and prepare_update_s_visc_PSV (src/PSV/prepare_update_s_visc_PSV.c:9-94).
+ * Outputs: fipjp, f, g [nx*ny] and dip, d, e [L][nx*ny] (file order per l), bip, bjm, cip, cjm,
+ * eta [L]. */
+int dn_prepare_visc(const dn_params *p, const float *vp, const float *vs, const float *rho,
+                    const float *qp, const float *qs, float *fipjp, float *f, float *g,
+                    float *dip, float *d, float *e, float *bip, float *bjm, float *cip, float *cjm,
+                    float *eta);
+/* Ricker / fumue / sin^3 / Gaussian-derivative / spike wavelets of wavelet.c:12-120
+ * (QUELLART 1,2,4,5,6) for one source, with N_ORDER time integrations.  out[nt]. */
+int dn_wavelet(int quellart, int nt, float dt, float tshift, float fc, float amp, int n_order, float *out);
+
+/* ---- models and shots (device) -------------------------------------------- */
+/* Builds every derived coefficient on the host (the functions above) and uploads
+ * it to `device`.  vp, vs, rho (and qp, qs when p->L > 0) are in file order. */
+int dn_model_create(const dn_params *p, const float *vp, const float *vs, const float *rho,
+                    const float *qp, const float *qs, int device, dn_model **out);
+int dn_model_destroy(dn_model *m);
+int dn_model_params(const dn_model *m, dn_params *out);
+/* Bytes of device memory a model / a shot of this acquisition will hold. */
+int dn_model_footprint(const dn_params *p, size_t *bytes);
+int dn_shot_footprint(const dn_params *p, int ntr, int store_snapshots, size_t *bytes);
+
+int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out);
+int dn_shot_destroy(dn_shot *s);
+
+/* Runs the whole time loop (nt = 1..NT) of psv() for n shots at once in one
+ * batched launch per half-step (shots may belong to different models and grid
+ * sizes; they must share FDORDER and elastic/visco).  mode: DN_MODE_*.
+ * Mode 0 stores snapshots iff the model's params.store_snapshots.  Mode 1
+ * needs dn_shot_set_residuals() and a previous stored mode-0 run of the shot.
+ * Returns DN_EUNSTABLE if a NaN appeared (checked at the psv.c:99 cell). */
+int dn_run(dn_shot *const *shots, int n, int mode);
+/* Plain path: one shot, one kernel launch per operation, no batching/graphs. */
+int dn_run_plain(dn_shot *s, int mode);
+
+/* Sections recorded in the last forward run; comp = DN_SEC_*; out [ntr][nt]. */
+int dn_shot_get_sections(const dn_shot *s, int comp, float *out);
+/* Adjoint sources for mode 1: residuals [ntr][nt] as calc_res() leaves them
+ * (time-reversed, src/calc_res.c:432-445).  NULL = component not used. */
+int dn_shot_set_residuals(dn_shot *s, const float *vxdiff, const float *vydiff, const float *pdiff);
+/* ass_gradPSV (src/PSV/ass_gradPSV.c:10-152) of this shot's correlation, then
+ * added to the model's stacked gradient (grad_obj_psv.c:253-261). */
+int dn_shot_accumulate_gradient(dn_shot *s);
+/* The model's stacked gradients (waveconv, waveconv_u, waveconv_rho) in file order. */
+int dn_model_get_gradient(const dn_model *m, float *g_vp, float *g_vs, float *g_rho);
+int dn_model_zero_gradient(dn_model *m);
+
+/* Unit-level access for parity tests: full-grid interior copies in file order.
+ * field ids: 0 vx, 1 vy, 2 sxx, 3 syy, 4 sxy, 5 vxp1, 6 vyp1,
+ *            7 waveconv_shot, 8 waveconv_u_shot, 9 waveconv_rho_shot, 10 Ws, 11 Wr */
+int dn_shot_get_field(const dn_shot *s, int field, float *out);
+/* Runs only time steps [nt0, nt1] of `mode` on one shot (nt0 == 1 zeroes the state). */
+int dn_run_steps(dn_shot *s, int mode, int nt0, int nt1);
+/* Decoded forward snapshot k (0-based) of one stored field (0 rho_x, 1 rho_y, 2 x, 3 y, 4 u). */
+int dn_shot_get_snapshot(const dn_shot *s, int k, int field, float *out);
+
+/* Device time of the last dn_run / dn_run_plain in milliseconds (CUDA events
+ * around the time loop only) and the number of kernel launches it issued. */
+int dn_last_run_stats(double *device_ms, long long *launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,329 @@
+/*
+ * ORACLE / TEST INFRASTRUCTURE - never part of the product.
+ *
+ * Drives the reference DENISE P-SV code (compiled unmodified from its own
+ * sources, see oracle/Makefile) for a single shot on a single rank, through
+ * flat arrays that ctypes can pass.  The call sequence mirrors the reference's
+ * drivers:
+ *   set-up:   FD_PSV.c:68-250 (initproc, alloc_*, PML_pro, holbergcoeff,
+ *             readmod_*_PSV, matcopy_*, av_mue, av_rho, av_tau,
+ *             prepare_update_s_visc_PSV)
+ *   one shot: grad_obj_psv.c:61-215 (init_grad, psv mode 0, residuals
+ *             supplied by the caller, srcpos_loc_back from the receivers,
+ *             psv mode 1, ass_gradPSV)
+ * Arrays cross this interface in file order (x-major, z contiguous).
+ */
+#include "fd.h"
+
+/* globals defined by the reference (include/globvar.h) */
+extern int NX, NY, NXG, NYG, NT, FDORDER, MAXRELERROR, FREE_SURF, FW, BOUNDARY, L, QUELLTYPB, DTINV, SEISMO, NDT;
+extern int EPRECOND, MODE, GRAD_FORM, INVMAT1, INV_STF, MYID, MYID_SHOT, NPROCX, NPROCY, NPROC, NP, NCOLORS, COLOR;
+extern int IDX, IDY, IDXI, IDYI, NTDTINV, NXNYI, SNAP, READMOD, WRITEMOD, PHYSICS, QUELLTYP, LOG;
+extern int INV_VP_ITER, INV_VS_ITER, INV_RHO_ITER, RUN_MULTIPLE_SHOTS, QUELLART, N_ORDER, LNORM, TIMEWIN, TRKILL;
+extern int OFFSET_MUTE, TIMELAPSE, TIME_FILT, COMP_WEIGHT, POS[3];
+extern float DH, DT, DAMPING, FPML, npower, k_max_PML, TS, *FL, TSNAP1, TSNAP2, TSNAPINC, TIME;
+extern char MFILE[STRING_SIZE];
+extern FILE *FP;
+
+static struct wavePSV W;
+static struct wavePSV_PML WP;
+static struct matPSV M;
+static struct fwiPSV FWI;
+static struct mpiPSV MP;
+static struct seisPSV S;
+static struct seisPSVfwi SF;
+static struct acq A;
+static float *hc = NULL;
+static float **Ws = NULL, **Wr = NULL, **We = NULL;
+static int *DTINV_help = NULL;
+static int g_ready = 0, g_ntr = 0, g_nsrc = 0;
+static MPI_Request *req_send, *req_rec;
+
+/* ip: nx ny nt fdorder maxrelerror free_surf fw L quelltypb dtinv seismo eprecond mode
+ * fp: dh dt damping fpml npower k_max_pml ts fl[0..4] */
+int refh_setup(const int *ip, const float *fp, const char *mfile)
+{
+    FP = stderr;
+    NX = NXG = ip[0];
+    NY = NYG = ip[1];
+    NT = ip[2];
+    FDORDER = ip[3];
+    MAXRELERROR = ip[4];
+    FREE_SURF = ip[5];
+    FW = ip[6];
+    L = ip[7];
+    QUELLTYPB = ip[8];
+    DTINV = ip[9] > 0 ? ip[9] : 1;
+    SEISMO = ip[10];
+    EPRECOND = ip[11];
+    MODE = ip[12];
+    DH = fp[0];
+    DT = fp[1];
+    DAMPING = fp[2];
+    FPML = fp[3];
+    npower = fp[4];
+    k_max_PML = fp[5];
+    TS = fp[6];
+    TIME = NT * DT;
+    FL = vector(1, L > 0 ? L : 1);
+    for (int l = 1; l <= L; l++) FL[l] = fp[6 + l];
+    BOUNDARY = 0;
+    NDT = 1;
+    GRAD_FORM = 1;
+    INVMAT1 = 1;
+    INV_STF = 0;
+    MYID = MYID_SHOT = 0;
+    NPROCX = NPROCY = 1;
+    NPROC = NP = 1;
+    NCOLORS = 1;
+    COLOR = 0;
+    IDX = IDY = IDXI = IDYI = 1;
+    SNAP = 0;
+    READMOD = 1;
+    WRITEMOD = 0;
+    PHYSICS = 1;
+    LOG = 0;
+    INV_VP_ITER = INV_VS_ITER = INV_RHO_ITER = 0;
+    N_ORDER = 0;
+    LNORM = 2;
+    TIMEWIN = TRKILL = OFFSET_MUTE = TIMELAPSE = TIME_FILT = 0;
+    strncpy(MFILE, mfile, STRING_SIZE - 1);
+
+    initproc();
+    NTDTINV = ceil((float)NT / (float)DTINV);   /* FD_PSV.c:82 */
+    NXNYI = (NX / IDXI) * (NY / IDYI);
+    req_send = (MPI_Request *)malloc(REQUEST_COUNT * sizeof(MPI_Request));
+    req_rec = (MPI_Request *)malloc(REQUEST_COUNT * sizeof(MPI_Request));
+
+    alloc_PSV(&W, &WP);
+    if (FW > 0)
+        PML_pro(WP.d_x, WP.K_x, WP.alpha_prime_x, WP.a_x, WP.b_x, WP.d_x_half, WP.K_x_half, WP.alpha_prime_x_half,
+                WP.a_x_half, WP.b_x_half, WP.d_y, WP.K_y, WP.alpha_prime_y, WP.a_y, WP.b_y, WP.d_y_half, WP.K_y_half,
+                WP.alpha_prime_y_half, WP.a_y_half, WP.b_y_half);
+    alloc_matPSV(&M);
+    alloc_mpiPSV(&MP);
+    if (MODE > 0) alloc_fwiPSV(&FWI);
+    hc = holbergcoeff();
+    if (L) readmod_visc_PSV(M.prho, M.ppi, M.pu, M.ptaus, M.ptaup, M.peta);
+    else readmod_elastic_PSV(M.prho, M.ppi, M.pu);
+    if (L) matcopy_PSV(M.prho, M.ppi, M.pu, M.ptaus, M.ptaup);
+    else matcopy_elastic_PSV(M.prho, M.ppi, M.pu);
+    av_mue(M.pu, M.puipjp, M.prho);
+    av_rho(M.prho, M.prip, M.prjp);
+    if (L) av_tau(M.ptaus, M.ptausipjp);
+    if (L)
+        prepare_update_s_visc_PSV(M.etajm, M.etaip, M.peta, M.fipjp, M.pu, M.puipjp, M.ppi, M.prho, M.ptaus, M.ptaup,
+                                  M.ptausipjp, M.f, M.g, M.bip, M.bjm, M.cip, M.cjm, M.dip, M.d, M.e);
+    Ws = matrix(1, NY, 1, NX);
+    Wr = matrix(1, NY, 1, NX);
+    We = matrix(1, NY, 1, NX);
+    DTINV_help = ivector(1, NT);
+    g_ready = 1;
+    return 0;
+}
+
+int refh_get_hc(float *out)
+{
+    for (int k = 0; k <= 6; k++) out[k] = hc[k];
+    return 0;
+}
+
+/* 20 vectors of 2*FW in dn_pml order: d K alpha a b for x, x_half, y, y_half */
+int refh_get_pml(float *out)
+{
+    float *v[20] = {WP.d_x, WP.K_x, WP.alpha_prime_x, WP.a_x, WP.b_x, WP.d_x_half, WP.K_x_half,
+                    WP.alpha_prime_x_half, WP.a_x_half, WP.b_x_half, WP.d_y, WP.K_y, WP.alpha_prime_y, WP.a_y,
+                    WP.b_y, WP.d_y_half, WP.K_y_half, WP.alpha_prime_y_half, WP.a_y_half, WP.b_y_half};
+    for (int k = 0; k < 20; k++)
+        for (int h = 1; h <= 2 * FW; h++) out[k * 2 * FW + h - 1] = v[k][h];
+    return 0;
+}
+
+static void to_file(float **a, float *out)
+{
+    for (int i = 1; i <= NX; i++)
+        for (int j = 1; j <= NY; j++) out[(size_t)(i - 1) * NY + (j - 1)] = a[j][i];
+}
+
+/* which: 0 rip 1 rjp 2 uipjp 3 fipjp 4 f 5 g 6 tausipjp 7 taus 8 taup,
+ *        100+l dip[l] 200+l d[l] 300+l e[l] (l = 1..L) */
+int refh_get_mat(int which, float *out)
+{
+    if (which == 0) to_file(M.prip, out);
+    else if (which == 1) to_file(M.prjp, out);
+    else if (which == 2) to_file(M.puipjp, out);
+    else if (which >= 3 && which <= 8 && L) {
+        float **a[6] = {M.fipjp, M.f, M.g, M.ptausipjp, M.ptaus, M.ptaup};
+        to_file(a[which - 3], out);
+    } else if (which > 100 && L) {
+        float ***t = which < 200 ? M.dip : (which < 300 ? M.d : M.e);
+        int l = which % 100;
+        for (int i = 1; i <= NX; i++)
+            for (int j = 1; j <= NY; j++) out[(size_t)(i - 1) * NY + (j - 1)] = t[j][i][l];
+    } else return -1;
+    return 0;
+}
+
+/* bip bjm cip cjm eta [L each] */
+int refh_get_visc_vectors(float *out)
+{
+    for (int l = 1; l <= L; l++) {
+        out[0 * L + l - 1] = M.bip[l];
+        out[1 * L + l - 1] = M.bjm[l];
+        out[2 * L + l - 1] = M.cip[l];
+        out[3 * L + l - 1] = M.cjm[l];
+        out[4 * L + l - 1] = M.peta[l];
+    }
+    return 0;
+}
+
+/* srcpos: 8 rows x nsrc (the reference's srcpos_loc[1..8][l] = i, j, 0, tshift, fc, amp, azimuth, type) */
+int refh_set_acq(int nsrc, const float *srcpos, const float *signals, int ntr, const int *rec_i, const int *rec_j)
+{
+    g_nsrc = nsrc;
+    g_ntr = ntr;
+    A.srcpos_loc = matrix(1, 8, 1, nsrc > 0 ? nsrc : 1);
+    for (int r = 1; r <= 8; r++)
+        for (int l = 1; l <= nsrc; l++) A.srcpos_loc[r][l] = srcpos[(r - 1) * nsrc + (l - 1)];
+    A.signals = fmatrix(1, nsrc > 0 ? nsrc : 1, 1, NT);
+    for (int l = 1; l <= nsrc; l++)
+        for (int t = 1; t <= NT; t++) A.signals[l][t] = signals[(size_t)(l - 1) * NT + (t - 1)];
+    A.recpos_loc = imatrix(1, 3, 1, ntr > 0 ? ntr : 1);
+    for (int l = 1; l <= ntr; l++) {
+        A.recpos_loc[1][l] = rec_i[l - 1];
+        A.recpos_loc[2][l] = rec_j[l - 1];
+        A.recpos_loc[3][l] = l;
+    }
+    alloc_seisPSV(ntr, NT, &S);
+    if (MODE > 0) alloc_seisPSVfwi(ntr, ntr, NT, &SF);
+    QUELLTYP = nsrc > 0 ? (int)A.srcpos_loc[8][1] : 1;   /* FD_PSV.c:298 */
+    return 0;
+}
+
+/* psv() over all NT steps in `mode`; for mode 0 with MODE > 0 the per-shot
+ * accumulators are re-initialised first (grad_obj_psv.c:61-70). */
+int refh_run(int mode)
+{
+    if (mode == 0 && MODE > 0) {
+        init_grad(FWI.waveconv_shot);
+        init_grad(FWI.waveconv_u_shot);
+        init_grad(FWI.waveconv_rho_shot);
+        if (EPRECOND == 1 || EPRECOND == 3) {
+            init_grad(Ws);
+            init_grad(Wr);
+            init_grad(We);
+        }
+    }
+    if (mode == 1) {
+        A.srcpos_loc_back = matrix(1, 6, 1, g_ntr);
+        for (int i = 1; i <= g_ntr; i++) {
+            A.srcpos_loc_back[1][i] = A.recpos_loc[1][i];
+            A.srcpos_loc_back[2][i] = A.recpos_loc[2][i];
+        }
+        psv(&W, &WP, &M, &FWI, &MP, &S, &SF, &A, hc, 1, 1, g_ntr, NT, g_ntr, Ws, Wr, 1, DTINV_help, 1, req_send,
+            req_rec);
+    } else {
+        psv(&W, &WP, &M, &FWI, &MP, &S, &SF, &A, hc, 1, 1, g_nsrc, NT, g_ntr, Ws, Wr, 1, DTINV_help, mode,
+            req_send, req_rec);
+    }
+    return 0;
+}
+
+/* comp 0 vx 1 vy 2 p 3 curl 4 div -> [ntr][nt] */
+int refh_get_sections(int comp, float *out)
+{
+    float **sec = comp == 0 ? S.sectionvx : comp == 1 ? S.sectionvy : comp == 2 ? S.sectionp
+                : comp == 3 ? S.sectioncurl : S.sectiondiv;
+    if (!sec) return -1;
+    for (int r = 1; r <= g_ntr; r++)
+        for (int t = 1; t <= NT; t++) out[(size_t)(r - 1) * NT + (t - 1)] = sec[r][t];
+    return 0;
+}
+
+/* adjoint sources [ntr][nt] (NULL leaves a component untouched) */
+int refh_set_residuals(const float *vx, const float *vy, const float *p)
+{
+    for (int r = 1; r <= g_ntr; r++)
+        for (int t = 1; t <= NT; t++) {
+            size_t k = (size_t)(r - 1) * NT + (t - 1);
+            if (vx && SF.sectionvxdiff) SF.sectionvxdiff[r][t] = vx[k];
+            if (vy && SF.sectionvydiff) SF.sectionvydiff[r][t] = vy[k];
+            if (p && SF.sectionpdiff) SF.sectionpdiff[r][t] = p[k];
+        }
+    return 0;
+}
+
+/* The reference's L2 residual (calc_res.c, LNORM 2): data/syn [ntr][nt] in,
+ * time-reversed residual [ntr][nt] out, returns 0.5 sum r^2 (test shot). */
+double refh_calc_res(const float *data, const float *syn, float *diff)
+{
+    float **d = matrix(1, g_ntr, 1, NT), **s = matrix(1, g_ntr, 1, NT);
+    float **df = matrix(1, g_ntr, 1, NT), **dfo = matrix(1, g_ntr, 1, NT);
+    int **recpos = imatrix(1, 3, 1, g_ntr);
+    float **srcpos = matrix(1, 8, 1, 1);
+    for (int r = 1; r <= g_ntr; r++) {
+        recpos[1][r] = A.recpos_loc[1][r];
+        recpos[2][r] = A.recpos_loc[2][r];
+        recpos[3][r] = r;
+        for (int t = 1; t <= NT; t++) {
+            d[r][t] = data[(size_t)(r - 1) * NT + (t - 1)];
+            s[r][t] = syn[(size_t)(r - 1) * NT + (t - 1)];
+        }
+    }
+    COMP_WEIGHT = 0;
+    double l2 = calc_res(d, s, df, dfo, g_ntr, NT, 2, 0.0, 0, 1, 1, g_ntr, recpos, A.recpos_loc, srcpos, 1, 1, 1);
+    for (int r = 1; r <= g_ntr; r++)
+        for (int t = 1; t <= NT; t++) diff[(size_t)(r - 1) * NT + (t - 1)] = df[r][t];
+    free_matrix(d, 1, g_ntr, 1, NT);
+    free_matrix(s, 1, g_ntr, 1, NT);
+    free_matrix(df, 1, g_ntr, 1, NT);
+    free_matrix(dfo, 1, g_ntr, 1, NT);
+    free_imatrix(recpos, 1, 3, 1, g_ntr);
+    free_matrix(srcpos, 1, 8, 1, 1);
+    return l2;
+}
+
+/* field ids match dn_shot_get_field: 0 vx 1 vy 2 sxx 3 syy 4 sxy 5 vxp1 6 vyp1
+ * 7 waveconv_shot 8 waveconv_u_shot 9 waveconv_rho_shot 10 Ws 11 Wr */
+int refh_get_field(int field, float *out)
+{
+    float **a = NULL;
+    switch (field) {
+    case 0: a = W.pvx; break;
+    case 1: a = W.pvy; break;
+    case 2: a = W.psxx; break;
+    case 3: a = W.psyy; break;
+    case 4: a = W.psxy; break;
+    case 5: a = W.pvxp1; break;
+    case 6: a = W.pvyp1; break;
+    case 7: a = FWI.waveconv_shot; break;
+    case 8: a = FWI.waveconv_u_shot; break;
+    case 9: a = FWI.waveconv_rho_shot; break;
+    case 10: a = Ws; break;
+    case 11: a = Wr; break;
+    default: return -1;
+    }
+    if (!a) return -1;
+    to_file(a, out);
+    return 0;
+}
+
+/* snapshot k (0-based) of field f (0 rho_x 1 rho_y 2 x 3 y 4 u), file order */
+int refh_get_snapshot(int k, int f, float *out)
+{
+    float *v = f == 0 ? FWI.forward_prop_rho_x : f == 1 ? FWI.forward_prop_rho_y : f == 2 ? FWI.forward_prop_x
+             : f == 3 ? FWI.forward_prop_y : FWI.forward_prop_u;
+    for (size_t c = 0; c < (size_t)NXNYI; c++) out[c] = v[(size_t)k * NXNYI + c + 1];
+    return 0;
+}
+
+/* ass_gradPSV of the current shot followed by the stacking of grad_obj_psv.c:253-261
+ * into zeroed stacks; returns vp, vs, rho gradients in file order */
+int refh_ass_grad(float *gvp, float *gvs, float *grho)
+{
+    ass_gradPSV(&FWI, &M, 1);
+    to_file(FWI.waveconv_shot, gvp);
+    to_file(FWI.waveconv_u_shot, gvs);
+    to_file(FWI.waveconv_rho_shot, grho);
+    return 0;
+}
