@@ -1,0 +1,352 @@
+"""Benchmark of the B200 P-SV propagator on the batched viscoelastic workload.
+
+Workload (one "step"): 64 viscoelastic shots (L = 3, FDORDER 8, CPML 20,
+free surface), each on its own 2000 x 600 model (DH 5 m) with 400 receivers,
+run through the whole time loop of NT = 6000 steps (DT 0.4 ms) as one batched,
+graph-replayed launch per operation.  Metric: Mcell-updates/s = shots x NX x
+NZ x NT / time.  Inputs (~15 GB resident) are larger than L2, so no flush is
+needed between timed steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank runs its own 64-shot batch (shots are independent:
+weak scaling, no collective on the data path); rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "denise-black-edition_b200")
+for _p in (PKG, os.path.join(ROOT, "tests")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Elastic Mcell-updates/s, HBM % peak; batched shots/s vs plain; p50/p99 latency"
+UNIT = "Mcell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--shots", type=int, default=64)
+    ap.add_argument("--nt", type=int, default=6000)
+    ap.add_argument("--nx", type=int, default=2000)
+    ap.add_argument("--ny", type=int, default=600)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--plain-shots", type=int, default=4)
+    ap.add_argument("--cpu-sample-nt", type=int, default=60)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path (oracle/_ref: the reference's own code, or the C port)
+# ---------------------------------------------------------------------------
+def _cpu_worker(args):
+    """One process: one shot of the workload for `nt_sample` steps on the reference's code."""
+    kind, k, nx, ny, nt_sample, seed = args
+    import oracles as O
+    from denise_b200 import synth
+
+    p = synth.c1_params(nx=nx, ny=ny, nt=nt_sample)
+    model, src, rec = synth.c1_shot(p, k, seed=seed)
+    src = src + (np.ones(1, np.int32), np.zeros(1, np.float32))
+    if kind == "reference":
+        r = O.Reference(p, model, src, rec, mode_global=0)
+        t0 = time.perf_counter()
+        r.run(0)
+        return time.perf_counter() - t0
+    r = O.Restatement(p, model, src, rec, "f")
+    t0 = time.perf_counter()
+    r.forward(store=False)
+    return time.perf_counter() - t0
+
+
+def cpu_sample(nx, ny, nt_sample, nproc=None):
+    """Runs nproc concurrent single-rank shots on the host cores; returns (Mcell/s, cores, kind, secs)."""
+    import multiprocessing as mp
+
+    import oracles as O
+
+    kind = "reference" if O.reference_available() else "port"
+    nproc = nproc or min(os.cpu_count() or 1, 64)
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(nproc) as pool:
+        times = pool.map(_cpu_worker, [(kind, k, nx, ny, nt_sample, 1000 + k) for k in range(nproc)])
+    wall = time.perf_counter() - t0
+    cells = nproc * nx * ny * nt_sample
+    rate = cells / max(times) / 1e6
+    return rate, nproc, kind, max(times), wall
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def build_inputs(p, nshots, shot_offset):
+    from denise_b200 import synth
+
+    return [synth.c1_shot(p, k % 64, nshots=64, seed=1 + k + shot_offset) for k in range(nshots)]
+
+
+def create_batch(p, inputs, device):
+    from concurrent.futures import ThreadPoolExecutor
+
+    import denise_b200 as dn
+
+    def mk(inp):
+        model, src, rec = inp
+        m = dn.Model(p, *model, device=device)
+        s = dn.Shot(m, src[0], src[1], src[2], rec[0], rec[1])
+        return m, s
+
+    with ThreadPoolExecutor(max_workers=min(16, len(inputs))) as ex:
+        return list(ex.map(mk, inputs))
+
+
+def run_ours(a, rank, world, local_rank):
+    import denise_b200 as dn
+    from denise_b200 import synth
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        torch.cuda.set_device(local_rank)
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=600))
+        dist = dist_mod
+    device = local_rank
+    p = synth.c1_params(nx=a.nx, ny=a.ny, nt=a.nt)
+    cells_step = a.shots * p.nx * p.ny * p.nt
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        rate, cores, kind, secs, wall = cpu_sample(p.nx, p.ny, a.cpu_sample_nt)
+        cpu = {"value": round(rate, 3), "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": f"{cores} concurrent single-rank shots of the {p.nx}x{p.ny} L=3 FDORDER 8 workload, "
+                         f"{a.cpu_sample_nt} time steps each ({secs:.1f} s)"}
+
+    inputs = build_inputs(p, a.shots, rank * a.shots)
+    pairs = create_batch(p, inputs, device)
+    shots = [s for _, s in pairs]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    import torch
+
+    for _ in range(a.warmup):
+        dn.run(shots)
+    torch.cuda.synchronize(device)
+    barrier()
+    with ClockSampler(device) as clk:
+        t0 = time.perf_counter()
+        dev_ms = 0.0
+        launches = 0
+        for _ in range(a.steps):
+            dn.run(shots)
+            ms, nl = dn.last_run_stats()
+            dev_ms += ms
+            launches += nl
+        torch.cuda.synchronize(device)
+        wall = time.perf_counter() - t0
+    barrier()
+    t_dev = dev_ms / 1e3
+    if dist is not None:
+        tt = torch.tensor([t_dev], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_dev = float(tt.item())
+    value = cells_step * a.steps * world / t_dev / 1e6
+    ms_step = t_dev / a.steps * 1e3
+
+    result = None
+    if rank == 0:
+        # per-kernel times of the same batch (direct launches with events between kernels)
+        prof = dn.api.profile_steps(shots, dn.MODE_FORWARD, nsteps=20)
+        cells = a.shots * p.nx * p.ny
+        peak, peak_kind = measured_peak()
+        s_bytes = (14 + 6 * p.L) * 4 * cells       # stress kernel algorithmic bytes per launch
+        v_bytes = 9 * 4 * cells
+        achieved = s_bytes / (prof["update_s"] * 1e-3) / 1e9
+        step_bytes = (23 + 6 * p.L) * 4 * cells
+        step_ms = sum(prof.values())
+        roof = {"bound": "hbm", "kernel": "k_update_s_vi<4,3,true> (viscoelastic stress update)",
+                "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": s_bytes,
+                "v_kernel_gbs": round(v_bytes / (prof["update_v"] * 1e-3) / 1e9, 1),
+                "whole_step_gbs_direct": round(step_bytes / (step_ms * 1e-3) / 1e9, 1),
+                "kernel_ms": {k: round(v, 4) for k, v in prof.items()}}
+        # plain (one shot at a time, direct launches) on a subset
+        plain_shots = shots[: max(1, min(a.plain_shots, len(shots)))]
+        torch.cuda.synchronize(device)
+        tp = 0.0
+        for s in plain_shots:
+            dn.run_plain(s)
+            tp += dn.last_run_stats()[0] / 1e3
+        plain_sps = len(plain_shots) / tp
+        batched_sps = a.shots * a.steps / t_dev
+        e2e = None
+        if not a.no_e2e:
+            e2e = run_e2e(p, inputs, device, cells_step)
+        result = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms_step, 2), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model family, see denise_b200/synth.py)",
+            "config": {"workload": f"batched viscoelastic forward: {a.shots} shots x {p.nx}x{p.ny} grid, NT={p.nt}, "
+                                   f"L=3, FDORDER 8, FW 20, free surface, 400 receivers/shot",
+                       "shots_per_gpu": a.shots, "nx": p.nx, "nz": p.ny, "nt": p.nt, "fdorder": p.fdorder, "L": p.L,
+                       "arith": "exact (bit-identical to the reference)",
+                       "l2_flush": "inputs larger than L2 (resident state ~15 GB)",
+                       "parallelism": f"shots-dp{world}"},
+            "shots_per_s": {"batched": round(batched_sps, 3), "plain": round(plain_sps, 3),
+                            "speedup": round(batched_sps / plain_sps, 3),
+                            "plain_sample_shots": len(plain_shots)},
+            "roofline": roof,
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "wall_s_timed": round(wall, 3),
+        }
+        if e2e:
+            result["e2e"] = e2e
+        if cpu:
+            result["cpu_baseline"] = cpu
+    for m, s in pairs:
+        s.close()
+        m.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def run_e2e(p, inputs, device, cells_step):
+    """One step through the public API with host buffers: models/shots created from host arrays
+    (host set-up + H2D), the batched run, sections read back (D2H), objects freed."""
+    import denise_b200 as dn
+    import torch
+
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    pairs = create_batch(p, inputs, device)
+    shots = [s for _, s in pairs]
+    dn.run(shots)
+    secs = [(s.sections(dn.SEC_VX), s.sections(dn.SEC_VY)) for s in shots]
+    for m, s in pairs:
+        s.close()
+        m.close()
+    torch.cuda.synchronize(device)
+    t = time.perf_counter() - t0
+    h2d = sum(5 * m[0].size * 4 + src[2].nbytes + 8 * len(rec[0]) + 8 for m, src, rec in inputs)
+    d2h = sum(a.nbytes + b.nbytes for a, b in secs)
+    return {"value": round(cells_step / t / 1e6, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "steps": 1, "seconds": round(t, 3)}
+
+
+def run_reference(a, rank, world):
+    from denise_b200 import synth
+
+    if rank != 0:
+        return None
+    p = synth.c1_params(nx=a.nx, ny=a.ny, nt=a.nt)
+    for _ in range(a.warmup):
+        cpu_sample(p.nx, p.ny, max(2, a.cpu_sample_nt // 6))
+    rates, secs = [], []
+    for _ in range(a.steps):
+        rate, cores, kind, sec, wall = cpu_sample(p.nx, p.ny, a.cpu_sample_nt)
+        rates.append(rate)
+        secs.append(sec)
+    value = float(np.median(rates))
+    ms = float(np.median(secs)) * 1e3
+    sample = (f"{cores} concurrent single-rank shots of the {p.nx}x{p.ny} L=3 FDORDER 8 workload, "
+              f"{a.cpu_sample_nt} time steps each per step")
+    return {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"batched viscoelastic forward: {p.nx}x{p.ny}, L=3, FDORDER 8 (bounded sample)",
+                       "parallelism": "host processes"},
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if a.impl == "reference":
+        res = run_reference(a, rank, world)
+    else:
+        res = run_ours(a, rank, world, local_rank)
+    if rank == 0 and res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -16,7 +16,7 @@
 #include <vector>
 
 #include "dn_internal.h"
-#include "dn_kernels.cuh"
+#include "dn_kernels_tma.cuh"
 
 using namespace dn;
 
@@ -353,6 +353,10 @@ extern "C" int dn_model_create(const dn_params *p, const float *vp, const float 
         dn_model_destroy(m);
         return dn_fail(DN_EDEVICE, "dn_model_create: upload failed");
     }
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        dn_model_destroy(m);
+        return dn_fail(DN_EDEVICE, "dn_model_create: upload did not complete");
+    }
     *out = m;
     return DN_OK;
 }
@@ -456,6 +460,7 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
                            acq->rec_j[l]);
     dn_shot *s = new dn_shot();
     s->m = m;
+    m->nshots++;
     s->p = *p;
     s->nsrc = acq->nsrc;
     s->ntr = acq->ntr;
@@ -497,8 +502,8 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
     std::vector<double> nsin(acq->nsrc), cosv(acq->nsrc);
     for (int l = 0; l < acq->nsrc; l++) {
         float azi_rad = s->src_azi[l] * 3.141592653589793 / 180;   // update_v_PML_PSV.c:743
-        nsin[l] = -sin(azi_rad);
-        cosv[l] = cos(azi_rad);
+        nsin[l] = -sin((double)azi_rad);   // C promotes the float argument to double
+        cosv[l] = cos((double)azi_rad);
     }
 
     const Layout &L = m->lay;
@@ -580,7 +585,10 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
         dn_shot_destroy(s);
         return dn_fail(DN_EDEVICE, "dn_shot_create: upload failed");
     }
-    m->nshots++;
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        dn_shot_destroy(s);
+        return dn_fail(DN_EDEVICE, "dn_shot_create: upload did not complete");
+    }
     *out = s;
     return DN_OK;
 }
@@ -749,17 +757,43 @@ struct LaunchCfg {
     int bx;
     int R, L;
     bool exact;
+    bool tma;   // stencil kernels fed by the bulk-copy row pipeline
     bool any_surf, any_src_s, any_store, any_adj, any_rec;
 };
 
+// marks (optional, profiling only): 9 events recorded around the 8 kernel slots
+// v, inject_v, s, inject_s, surface, seismo, snap, correlate
+#define MARK(k)                                                                                    \
+    do {                                                                                           \
+        if (marks) cudaEventRecord(marks[k], st);                                                  \
+    } while (0)
+
 template <int R, bool X>
-static void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int *ntb, int off, long long &nl)
+static void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int *ntb, int off, long long &nl,
+                          cudaEvent_t *marks)
 {
-    k_update_v<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
+    MARK(0);
+    if (c.tma) k_update_v_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QV>(slot_floats_v()), st>>>(d, ntb, off);
+    else k_update_v<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
+    MARK(1);
     k_inject_v<<<c.src_grid, 128, 0, st>>>(d, ntb, off);
+    MARK(2);
     nl += 2;
     if (c.L == 0) {
-        k_update_s_el<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
+        if (c.tma)
+            k_update_s_el_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QS_EL>(slot_floats_s_el()), st>>>(d, ntb, off);
+        else k_update_s_el<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
+    } else if (c.tma) {
+#define DN_VI_TMA(LL)                                                                                          \
+    k_update_s_vi_tma<R, LL, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QS_VI>(slot_floats_s_vi(LL)), st>>>(d, ntb, off)
+        switch (c.L) {
+        case 1: DN_VI_TMA(1); break;
+        case 2: DN_VI_TMA(2); break;
+        case 3: DN_VI_TMA(3); break;
+        case 4: DN_VI_TMA(4); break;
+        default: DN_VI_TMA(5); break;
+        }
+#undef DN_VI_TMA
     } else {
         switch (c.L) {
         case 1: k_update_s_vi<R, 1, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
@@ -770,10 +804,12 @@ static void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, co
         }
     }
     nl++;
+    MARK(3);
     if (c.any_src_s) {
         k_inject_s<<<c.src_grid, 128, 0, st>>>(d, ntb, off);
         nl++;
     }
+    MARK(4);
     if (c.any_surf) {
         if (c.L == 0) {
             k_surface_el<R, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off);
@@ -788,35 +824,83 @@ static void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, co
         }
         nl++;
     }
+    MARK(5);
     k_seismo<R><<<c.rec_grid, 128, 0, st>>>(d, ntb, off);
     nl++;
+    MARK(6);
     if (c.any_store) {
         k_snap_store<<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
         nl++;
     }
+    MARK(7);
     if (c.any_adj) {
         k_correlate<<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
         nl++;
     }
+    MARK(8);
+}
+
+// opt the pipelined kernels into their dynamic shared memory (needed above 48 KB)
+template <int R, bool X>
+static int set_smem_attrs_R()
+{
+    cudaFuncSetAttribute(k_update_v_tma<R, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)pipe_smem_bytes<QV>(slot_floats_v()));
+    cudaFuncSetAttribute(k_update_s_el_tma<R, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)pipe_smem_bytes<QS_EL>(slot_floats_s_el()));
+    cudaFuncSetAttribute(k_update_s_vi_tma<R, 1, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)pipe_smem_bytes<QS_VI>(slot_floats_s_vi(1)));
+    cudaFuncSetAttribute(k_update_s_vi_tma<R, 2, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)pipe_smem_bytes<QS_VI>(slot_floats_s_vi(2)));
+    cudaFuncSetAttribute(k_update_s_vi_tma<R, 3, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)pipe_smem_bytes<QS_VI>(slot_floats_s_vi(3)));
+    cudaFuncSetAttribute(k_update_s_vi_tma<R, 4, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)pipe_smem_bytes<QS_VI>(slot_floats_s_vi(4)));
+    cudaError_t e = cudaFuncSetAttribute(k_update_s_vi_tma<R, 5, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pipe_smem_bytes<QS_VI>(slot_floats_s_vi(5)));
+    return e == cudaSuccess ? 0 : -1;
 }
 
 template <bool X>
-static void launch_step_X(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int *ntb, int off, long long &nl)
+static int set_smem_attrs_X(int R)
 {
-    switch (c.R) {
-    case 1: launch_step_R<1, X>(c, st, d, ntb, off, nl); break;
-    case 2: launch_step_R<2, X>(c, st, d, ntb, off, nl); break;
-    case 3: launch_step_R<3, X>(c, st, d, ntb, off, nl); break;
-    case 4: launch_step_R<4, X>(c, st, d, ntb, off, nl); break;
-    case 5: launch_step_R<5, X>(c, st, d, ntb, off, nl); break;
-    default: launch_step_R<6, X>(c, st, d, ntb, off, nl); break;
+    switch (R) {
+    case 1: return set_smem_attrs_R<1, X>();
+    case 2: return set_smem_attrs_R<2, X>();
+    case 3: return set_smem_attrs_R<3, X>();
+    case 4: return set_smem_attrs_R<4, X>();
+    case 5: return set_smem_attrs_R<5, X>();
+    default: return set_smem_attrs_R<6, X>();
     }
 }
 
-static void launch_step(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int *ntb, int off, long long &nl)
+static int prepare_launch(const LaunchCfg &c)
 {
-    if (c.exact) launch_step_X<true>(c, st, d, ntb, off, nl);
-    else launch_step_X<false>(c, st, d, ntb, off, nl);
+    if (!c.tma) return DN_OK;
+    int e = c.exact ? set_smem_attrs_X<true>(c.R) : set_smem_attrs_X<false>(c.R);
+    if (e) return dn_fail(DN_EDEVICE, "cudaFuncSetAttribute (dynamic shared memory) failed");
+    return DN_OK;
+}
+
+template <bool X>
+static void launch_step_X(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int *ntb, int off, long long &nl,
+                          cudaEvent_t *marks)
+{
+    switch (c.R) {
+    case 1: launch_step_R<1, X>(c, st, d, ntb, off, nl, marks); break;
+    case 2: launch_step_R<2, X>(c, st, d, ntb, off, nl, marks); break;
+    case 3: launch_step_R<3, X>(c, st, d, ntb, off, nl, marks); break;
+    case 4: launch_step_R<4, X>(c, st, d, ntb, off, nl, marks); break;
+    case 5: launch_step_R<5, X>(c, st, d, ntb, off, nl, marks); break;
+    default: launch_step_R<6, X>(c, st, d, ntb, off, nl, marks); break;
+    }
+}
+
+static void launch_step(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int *ntb, int off, long long &nl,
+                        cudaEvent_t *marks = nullptr)
+{
+    if (c.exact) launch_step_X<true>(c, st, d, ntb, off, nl, marks);
+    else launch_step_X<false>(c, st, d, ntb, off, nl, marks);
 }
 
 __global__ void k_advance(int *ntb, int by) { *ntb += by; }
@@ -868,6 +952,7 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c)
     c.L = p0.L;
     c.exact = p0.arith == DN_ARITH_EXACT;
     c.bx = shots[0]->bx;
+    c.tma = c.bx == TMA_W && !(getenv("DN_KERNEL") && strcmp(getenv("DN_KERNEL"), "reg") == 0);
     c.any_surf = c.any_src_s = c.any_store = c.any_adj = c.any_rec = false;
     int maxtiles = 0, maxsrc = 1, maxnx = 1, maxtr = 1;
     for (int k = 0; k < n; k++) {
@@ -919,6 +1004,7 @@ static int finish_run(dn_shot *const *shots, int n, int mode, cudaStream_t st)
     for (int k = 0; k < n; k++) {
         int f = 0;
         CU(cudaMemcpy(&f, shots[k]->d_flag, 4, cudaMemcpyDeviceToHost));
+        if (f & 2) return dn_fail(DN_ETIMEDOUT, "a pipelined stencil kernel gave up waiting for its row copies (shot %d)", k);
         if (f & 1) bad = k;
         if (mode == 0 && shots[k]->p.store_snapshots) shots[k]->stored = 1;
         if (mode == 1) shots[k]->correlated = 1;
@@ -945,6 +1031,8 @@ extern "C" int dn_run(dn_shot *const *shots, int n, int mode)
     st = dev_state(device, &ds);
     if (st) return st;
     CU(cudaSetDevice(device));
+    st = prepare_launch(c);
+    if (st) return st;
     int maxnt = 0;
     for (int k = 0; k < n; k++) maxnt = std::max(maxnt, shots[k]->p.nt);
 
@@ -970,7 +1058,8 @@ extern "C" int dn_run(dn_shot *const *shots, int n, int mode)
             delete b;
             return dn_fail(DN_ENOMEM, "dn_run: descriptor allocation failed");
         }
-        CU(cudaMemcpy(b->d_insts, b->h_insts.data(), sizeof(Inst) * n, cudaMemcpyHostToDevice));
+        CU(cudaMemcpyAsync(b->d_insts, b->h_insts.data(), sizeof(Inst) * n, cudaMemcpyHostToDevice, ds->stream));
+        CU(cudaStreamSynchronize(ds->stream));
         b->chunk = graph_chunk(maxnt);
         cudaGraph_t g;
         CU(cudaStreamBeginCapture(ds->stream, cudaStreamCaptureModeThreadLocal));
@@ -1025,10 +1114,13 @@ static int run_direct(dn_shot *s, int mode, int nt0, int nt1, bool zero)
     st = dev_state(s->m->device, &ds);
     if (st) return st;
     CU(cudaSetDevice(s->m->device));
+    st = prepare_launch(c);
+    if (st) return st;
     Inst h = make_inst(s, mode);
     Inst *d = nullptr;
     CU(cudaMalloc(&d, sizeof(Inst)));
-    cudaMemcpy(d, &h, sizeof(Inst), cudaMemcpyHostToDevice);
+    CU(cudaMemcpyAsync(d, &h, sizeof(Inst), cudaMemcpyHostToDevice, ds->stream));
+    CU(cudaStreamSynchronize(ds->stream));
     if (zero) {
         st = zero_for_run(s, mode, ds->stream);
         if (st) {
@@ -1283,5 +1375,66 @@ extern "C" int dn_model_zero_gradient(dn_model *m)
     if (!m) return dn_fail(DN_EINVAL, "null model");
     CU(cudaSetDevice(m->device));
     CU(cudaMemset(m->dgrad, 0, 3 * (size_t)m->p.nx * m->p.ny * (m->grad64 ? 8 : 4)));
+    return DN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// per-kernel timing of the batched step (direct launches, CUDA events on the
+// engine stream between the kernels); ms_out[8]: average ms per launch of
+// v, inject_v, s, inject_s, surface, seismo, snap_store, correlate
+// ---------------------------------------------------------------------------
+extern "C" int dn_profile_steps(dn_shot *const *shots, int n, int mode, int nsteps, double *ms_out)
+{
+    LaunchCfg c;
+    int st = check_batch(shots, n, mode, c);
+    if (st) return st;
+    if (nsteps < 1 || !ms_out) return dn_fail(DN_EINVAL, "dn_profile_steps: bad arguments");
+    const int device = shots[0]->m->device;
+    DevState *ds;
+    st = dev_state(device, &ds);
+    if (st) return st;
+    CU(cudaSetDevice(device));
+    st = prepare_launch(c);
+    if (st) return st;
+    std::vector<Inst> h;
+    int maxnt = 0;
+    for (int k = 0; k < n; k++) {
+        h.push_back(make_inst(shots[k], mode));
+        maxnt = std::max(maxnt, shots[k]->p.nt);
+    }
+    nsteps = std::min(nsteps, maxnt);
+    Inst *d = nullptr;
+    CU(cudaMalloc(&d, sizeof(Inst) * n));
+    CU(cudaMemcpyAsync(d, h.data(), sizeof(Inst) * n, cudaMemcpyHostToDevice, ds->stream));
+    for (int k = 0; k < n; k++) {
+        st = zero_for_run(shots[k], mode, ds->stream);
+        if (st) {
+            cudaFree(d);
+            return st;
+        }
+    }
+    cudaEvent_t ev[9];
+    for (int k = 0; k < 9; k++) cudaEventCreate(&ev[k]);
+    double acc[8] = {0};
+    long long nl = 0;
+    for (int t = 1; t <= nsteps; t++) {
+        launch_step(c, ds->stream, d, ds->d_zero, t, nl, ev);
+        cudaEventSynchronize(ev[8]);
+        for (int k = 0; k < 8; k++) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+            acc[k] += ms;
+        }
+    }
+    for (int k = 0; k < 8; k++) ms_out[k] = acc[k] / nsteps;
+    for (int k = 0; k < 9; k++) cudaEventDestroy(ev[k]);
+    cudaError_t e = cudaGetLastError();
+    cudaStreamSynchronize(ds->stream);
+    cudaFree(d);
+    for (int k = 0; k < n; k++) {
+        if (mode == 0) shots[k]->stored = 0;
+        if (mode == 1) shots[k]->correlated = 0;
+    }
+    if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "dn_profile_steps: %s", cudaGetErrorString(e));
     return DN_OK;
 }

@@ -116,54 +116,90 @@ __device__ __forceinline__ bool tile_of(const Inst &I, TileLoc &t)
 // Velocity update: update_v_PML_PSV.c:53-715 (FDORDER 2..12) + CPML on the
 // stress derivatives; mode 0/2: vxp1 = rip (sxx_x + sxy_y) / DH (:451-453),
 // mode 1: vxp1 += DT * vx with the old vx (:455-457).
+// Each thread streams down its column; the loads of row j+1 are issued before
+// row j is computed so two rows of DRAM traffic are in flight per thread.
 // ===========================================================================
 template <int R, bool X>
 __global__ void __launch_bounds__(256) k_update_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = __ldg(ntb) + off;
+    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
     if (nt > I.nt) return;
     TileLoc t;
     if (!tile_of(I, t)) return;
     const long long P = I.pitch;
     const int i = t.i;
-    const float *__restrict__ sxx = I.sxx;
-    const float *__restrict__ syy = I.syy;
-    const float *__restrict__ sxy = I.sxy;
+    const float *__restrict__ sxx = I.sxx + i;
+    const float *__restrict__ syy = I.syy + i;
+    const float *__restrict__ sxy = I.sxy + i;
+    const float *__restrict__ rip = I.rip + i;
+    const float *__restrict__ rjp = I.rjp + i;
+    float *__restrict__ vx = I.vx + i;
+    float *__restrict__ vy = I.vy + i;
+    float *__restrict__ vxp1 = I.vxp1 + i;
+    float *__restrict__ vyp1 = I.vyp1 + i;
     float hc[R + 1];
 #pragma unroll
     for (int m = 1; m <= R; m++) hc[m] = I.hc[m];
     const float DT = I.DT, DH = I.DH;
     const int mode = I.mode;
     const bool snapstep = (mode == 0) && I.store && ((nt - 1) % I.dtinv == 0);
-    const int fw = I.fw, nx = I.nx, ny = I.ny;
+    const int fw = I.fw, nx = I.nx, ny = I.ny, free_surf = I.free_surf;
+    const bool xframe = fw > 0 && (i <= fw || i >= nx - fw + 1);
 
-    // window: wyy[k] = syy[j-R+1+k], wxy[k] = sxy[j-R+k]
+    // z windows: wyy[k] = syy[j-R+1+k], wxy[k] = sxy[j-R+k]
     float wyy[2 * R], wxy[2 * R];
 #pragma unroll
     for (int k = 0; k < 2 * R - 1; k++) {
-        wyy[k] = syy[(long long)(t.j0 - R + 1 + k) * P + i];
-        wxy[k] = sxy[(long long)(t.j0 - R + k) * P + i];
+        wyy[k] = __ldg(syy + (long long)(t.j0 - R + 1 + k) * P);
+        wxy[k] = __ldg(sxy + (long long)(t.j0 - R + k) * P);
     }
+    // own-column operands of row j+1 are fetched before row j is computed (this also
+    // brings the cache lines the x-neighbour loads of the row will hit into L1)
+    float nyy, nxy, nrip, nrjp, nvx, nvy, nsx, nsy;
+    auto fetch = [&](int j) {
+        const long long o = (long long)j * P;
+        nyy = __ldg(syy + o + R * P);
+        nxy = __ldg(sxy + o + (R - 1) * P);
+        nsx = __ldg(sxx + o);
+        nsy = __ldg(sxy + o);
+        nrip = __ldg(rip + o);
+        nrjp = __ldg(rjp + o);
+        nvx = vx[o];
+        nvy = vy[o];
+    };
+    fetch(t.j0);
     for (int j = t.j0; j <= t.j1; j++) {
-        wyy[2 * R - 1] = syy[(long long)(j + R) * P + i];
-        wxy[2 * R - 1] = sxy[(long long)(j + R - 1) * P + i];
-        const float *rs = sxx + (long long)j * P + i;
-        const float *rx = sxy + (long long)j * P + i;
-        float sxx_x = MUL<X>(hc[1], SUB<X>(rs[1], rs[0]));
-        float sxy_x = MUL<X>(hc[1], SUB<X>(rx[0], rx[-1]));
+        wyy[2 * R - 1] = nyy;
+        wxy[2 * R - 1] = nxy;
+        const float ripv = nrip, rjpv = nrjp, vxo = nvx, vyo = nvy, csx = nsx, csy = nsy;
+        if (j < t.j1) fetch(j + 1);
+        // ax[k] = sxx[j][i-R+1+k], bx[k] = sxy[j][i-R+k]; the own-column entries come from the prefetch
+        const float *rs = sxx + (long long)j * P;
+        const float *rx = sxy + (long long)j * P;
+        float ax[2 * R], bx[2 * R];
+#pragma unroll
+        for (int k = 0; k < 2 * R; k++) {
+            ax[k] = k == R - 1 ? csx : __ldg(rs + (k - R + 1));
+            bx[k] = k == R ? csy : __ldg(rx + (k - R));
+        }
+
+        float sxx_x = MUL<X>(hc[1], SUB<X>(ax[R], ax[R - 1]));
+        float sxy_x = MUL<X>(hc[1], SUB<X>(bx[R], bx[R - 1]));
         float sxy_y = MUL<X>(hc[1], SUB<X>(wxy[R], wxy[R - 1]));
         float syy_y = MUL<X>(hc[1], SUB<X>(wyy[R], wyy[R - 1]));
 #pragma unroll
         for (int m = 2; m <= R; m++) {
-            sxx_x = ADD<X>(sxx_x, MUL<X>(hc[m], SUB<X>(rs[m], rs[1 - m])));
-            sxy_x = ADD<X>(sxy_x, MUL<X>(hc[m], SUB<X>(rx[m - 1], rx[-m])));
+            sxx_x = ADD<X>(sxx_x, MUL<X>(hc[m], SUB<X>(ax[R - 1 + m], ax[R - m])));
+            sxy_x = ADD<X>(sxy_x, MUL<X>(hc[m], SUB<X>(bx[R + m - 1], bx[R - m])));
             sxy_y = ADD<X>(sxy_y, MUL<X>(hc[m], SUB<X>(wxy[R + m - 1], wxy[R - m])));
             syy_y = ADD<X>(syy_y, MUL<X>(hc[m], SUB<X>(wyy[R - 1 + m], wyy[R - m])));
         }
-        if (fw > 0) {
-            if (i <= fw) {   // left frame (BOUNDARY == 0)
-                const int h = i - 1;
+        if (xframe) {
+            // left frame h = i, right frame h1 = i - nx + 2 fw (BOUNDARY == 0); both apply when they overlap
+            for (int side = 0; side < 2; side++) {
+                if (side == 0 ? (i > fw) : (i < nx - fw + 1)) continue;
+                const int h = side == 0 ? i - 1 : i - nx + 2 * fw - 1;
                 float *ps = I.psi_sxx_x + (long long)(j - 1) * 2 * fw + h;
                 float v = ADD<X>(MUL<X>(I.b_xh[h], *ps), MUL<X>(I.a_xh[h], sxx_x));
                 *ps = v;
@@ -173,30 +209,11 @@ __global__ void __launch_bounds__(256) k_update_v(const Inst *__restrict__ insts
                 *pq = w;
                 sxy_x = ADD<X>(DIV<X>(sxy_x, I.K_x[h]), w);
             }
-            if (i >= nx - fw + 1) {   // right frame, h1 = i - nx + 2 fw
-                const int h = i - nx + 2 * fw - 1;
-                float *ps = I.psi_sxx_x + (long long)(j - 1) * 2 * fw + h;
-                float v = ADD<X>(MUL<X>(I.b_xh[h], *ps), MUL<X>(I.a_xh[h], sxx_x));
-                *ps = v;
-                sxx_x = ADD<X>(DIV<X>(sxx_x, I.K_xh[h]), v);
-                float *pq = I.psi_sxy_x + (long long)(j - 1) * 2 * fw + h;
-                float w = ADD<X>(MUL<X>(I.b_x[h], *pq), MUL<X>(I.a_x[h], sxy_x));
-                *pq = w;
-                sxy_x = ADD<X>(DIV<X>(sxy_x, I.K_x[h]), w);
-            }
-            if (!I.free_surf && j <= fw) {   // top frame
-                const int h = j - 1;
-                float *ps = I.psi_syy_y + (long long)h * nx + (i - 1);
-                float v = ADD<X>(MUL<X>(I.b_yh[h], *ps), MUL<X>(I.a_yh[h], syy_y));
-                *ps = v;
-                syy_y = ADD<X>(DIV<X>(syy_y, I.K_yh[h]), v);
-                float *pq = I.psi_sxy_y + (long long)h * nx + (i - 1);
-                float w = ADD<X>(MUL<X>(I.b_y[h], *pq), MUL<X>(I.a_y[h], sxy_y));
-                *pq = w;
-                sxy_y = ADD<X>(DIV<X>(sxy_y, I.K_y[h]), w);
-            }
-            if (j >= ny - fw + 1) {   // bottom frame, h1 = j - ny + 2 fw
-                const int h = j - ny + 2 * fw - 1;
+        }
+        if (fw > 0 && ((!free_surf && j <= fw) || j >= ny - fw + 1)) {
+            for (int side = 0; side < 2; side++) {
+                if (side == 0 ? (free_surf || j > fw) : (j < ny - fw + 1)) continue;
+                const int h = side == 0 ? j - 1 : j - ny + 2 * fw - 1;
                 float *ps = I.psi_syy_y + (long long)h * nx + (i - 1);
                 float v = ADD<X>(MUL<X>(I.b_yh[h], *ps), MUL<X>(I.a_yh[h], syy_y));
                 *ps = v;
@@ -207,20 +224,18 @@ __global__ void __launch_bounds__(256) k_update_v(const Inst *__restrict__ insts
                 sxy_y = ADD<X>(DIV<X>(sxy_y, I.K_y[h]), w);
             }
         }
-        const long long o = (long long)j * P + i;
+        const long long o = (long long)j * P;
         const float s1 = ADD<X>(sxx_x, sxy_y);
         const float s2 = ADD<X>(sxy_x, syy_y);
-        const float ripv = I.rip[o], rjpv = I.rjp[o];
-        float vxo = I.vx[o], vyo = I.vy[o];
         if (snapstep) {
-            I.vxp1[o] = DIV<X>(MUL<X>(ripv, s1), DH);
-            I.vyp1[o] = DIV<X>(MUL<X>(rjpv, s2), DH);
+            vxp1[o] = DIV<X>(MUL<X>(ripv, s1), DH);
+            vyp1[o] = DIV<X>(MUL<X>(rjpv, s2), DH);
         } else if (mode == 1) {
-            I.vxp1[o] = ADD<X>(I.vxp1[o], MUL<X>(DT, vxo));
-            I.vyp1[o] = ADD<X>(I.vyp1[o], MUL<X>(DT, vyo));
+            vxp1[o] = ADD<X>(vxp1[o], MUL<X>(DT, vxo));
+            vyp1[o] = ADD<X>(vyp1[o], MUL<X>(DT, vyo));
         }
-        I.vx[o] = ADD<X>(vxo, DIV<X>(MUL<X>(MUL<X>(DT, ripv), s1), DH));
-        I.vy[o] = ADD<X>(vyo, DIV<X>(MUL<X>(MUL<X>(DT, rjpv), s2), DH));
+        vx[o] = ADD<X>(vxo, DIV<X>(MUL<X>(MUL<X>(DT, ripv), s1), DH));
+        vy[o] = ADD<X>(vyo, DIV<X>(MUL<X>(MUL<X>(DT, rjpv), s2), DH));
 #pragma unroll
         for (int k = 0; k < 2 * R - 1; k++) {
             wyy[k] = wyy[k + 1];
@@ -236,7 +251,7 @@ __global__ void __launch_bounds__(256) k_update_v(const Inst *__restrict__ insts
 // ===========================================================================
 __global__ void k_inject_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = __ldg(ntb) + off;
+    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
     if (nt > I.nt) return;
     const long long P = I.pitch;
@@ -278,26 +293,47 @@ __global__ void k_inject_v(const Inst *__restrict__ insts, const int *__restrict
 // Stress derivatives shared by the elastic and viscoelastic updates:
 // vxx, vyx, vxy, vyy of update_s_*_PML_PSV.c (case 8 = :366-384 elastic),
 // multiplied by dhi, followed by the CPML correction (:386-438).
+// The operands of row j+1 are fetched before row j is computed.
 // ===========================================================================
 template <int R, bool X>
 struct VDeriv {
-    float wx[2 * R];   // vx rows j-R+1 .. j+R
-    float wy[2 * R];   // vy rows j-R .. j+R-1
+    const float *__restrict__ vx;   // column i
+    const float *__restrict__ vy;
+    long long P;
+    float wx[2 * R];                // vx rows j-R+1 .. j+R (vx[j] = wx[R-1])
+    float wy[2 * R];                // vy rows j-R .. j+R-1 (vy[j] = wy[R])
+    float cx[2 * R], dx[2 * R];     // cx[k] = vx[j][i-R+k], dx[k] = vy[j][i-R+1+k]
+    float nwx, nwy;
 
+    __device__ __forceinline__ void fetch(int j)
+    {
+        const long long o = (long long)j * P;
+        nwx = __ldg(vx + o + R * P);
+        nwy = __ldg(vy + o + (R - 1) * P);
+    }
     __device__ __forceinline__ void prime(const Inst &I, int i, int j0)
     {
-        const long long P = I.pitch;
+        vx = I.vx + i;
+        vy = I.vy + i;
+        P = I.pitch;
 #pragma unroll
         for (int k = 0; k < 2 * R - 1; k++) {
-            wx[k] = I.vx[(long long)(j0 - R + 1 + k) * P + i];
-            wy[k] = I.vy[(long long)(j0 - R + k) * P + i];
+            wx[k] = __ldg(vx + (long long)(j0 - R + 1 + k) * P);
+            wy[k] = __ldg(vy + (long long)(j0 - R + k) * P);
         }
+        fetch(j0);
     }
-    __device__ __forceinline__ void load_row(const Inst &I, int i, int j)
+    // makes row j current: completes the windows and reads the row's x-neighbours (L1)
+    __device__ __forceinline__ void advance(int j)
     {
-        const long long P = I.pitch;
-        wx[2 * R - 1] = I.vx[(long long)(j + R) * P + i];
-        wy[2 * R - 1] = I.vy[(long long)(j + R - 1) * P + i];
+        wx[2 * R - 1] = nwx;
+        wy[2 * R - 1] = nwy;
+        const long long o = (long long)j * P;
+#pragma unroll
+        for (int k = 0; k < 2 * R; k++) {
+            cx[k] = k == R ? wx[R - 1] : __ldg(vx + o + (k - R));
+            dx[k] = k == R - 1 ? wy[R] : __ldg(vy + o + (k - R + 1));
+        }
     }
     __device__ __forceinline__ void shift()
     {
@@ -310,17 +346,14 @@ struct VDeriv {
     __device__ __forceinline__ void compute(const Inst &I, const float *hc, int i, int j, float dhi, float &vxx,
                                             float &vyx, float &vxy, float &vyy)
     {
-        const long long P = I.pitch;
-        const float *rx = I.vx + (long long)j * P + i;
-        const float *ry = I.vy + (long long)j * P + i;
-        float a = MUL<X>(hc[1], SUB<X>(rx[0], rx[-1]));
-        float b = MUL<X>(hc[1], SUB<X>(ry[1], ry[0]));
+        float a = MUL<X>(hc[1], SUB<X>(cx[R], cx[R - 1]));
+        float b = MUL<X>(hc[1], SUB<X>(dx[R], dx[R - 1]));
         float c = MUL<X>(hc[1], SUB<X>(wx[R], wx[R - 1]));
         float d = MUL<X>(hc[1], SUB<X>(wy[R], wy[R - 1]));
 #pragma unroll
         for (int m = 2; m <= R; m++) {
-            a = ADD<X>(a, MUL<X>(hc[m], SUB<X>(rx[m - 1], rx[-m])));
-            b = ADD<X>(b, MUL<X>(hc[m], SUB<X>(ry[m], ry[1 - m])));
+            a = ADD<X>(a, MUL<X>(hc[m], SUB<X>(cx[R + m - 1], cx[R - m])));
+            b = ADD<X>(b, MUL<X>(hc[m], SUB<X>(dx[R - 1 + m], dx[R - m])));
             c = ADD<X>(c, MUL<X>(hc[m], SUB<X>(wx[R - 1 + m], wx[R - m])));
             d = ADD<X>(d, MUL<X>(hc[m], SUB<X>(wy[R + m - 1], wy[R - m])));
         }
@@ -329,9 +362,10 @@ struct VDeriv {
         vxy = MUL<X>(c, dhi);
         vyy = MUL<X>(d, dhi);
         const int fw = I.fw, nx = I.nx, ny = I.ny;
-        if (fw > 0) {
-            if (i <= fw) {
-                const int h = i - 1;
+        if (fw > 0 && (i <= fw || i >= nx - fw + 1)) {
+            for (int side = 0; side < 2; side++) {
+                if (side == 0 ? (i > fw) : (i < nx - fw + 1)) continue;
+                const int h = side == 0 ? i - 1 : i - nx + 2 * fw - 1;
                 float *p1 = I.psi_vxx + (long long)(j - 1) * 2 * fw + h;
                 float v = ADD<X>(MUL<X>(I.b_x[h], *p1), MUL<X>(I.a_x[h], vxx));
                 *p1 = v;
@@ -341,19 +375,11 @@ struct VDeriv {
                 *p2 = w;
                 vyx = ADD<X>(DIV<X>(vyx, I.K_xh[h]), w);
             }
-            if (i >= nx - fw + 1) {
-                const int h = i - nx + 2 * fw - 1;
-                float *p1 = I.psi_vxx + (long long)(j - 1) * 2 * fw + h;
-                float v = ADD<X>(MUL<X>(I.b_x[h], *p1), MUL<X>(I.a_x[h], vxx));
-                *p1 = v;
-                vxx = ADD<X>(DIV<X>(vxx, I.K_x[h]), v);
-                float *p2 = I.psi_vyx + (long long)(j - 1) * 2 * fw + h;
-                float w = ADD<X>(MUL<X>(I.b_xh[h], *p2), MUL<X>(I.a_xh[h], vyx));
-                *p2 = w;
-                vyx = ADD<X>(DIV<X>(vyx, I.K_xh[h]), w);
-            }
-            if (!I.free_surf && j <= fw) {
-                const int h = j - 1;
+        }
+        if (fw > 0 && ((!I.free_surf && j <= fw) || j >= ny - fw + 1)) {
+            for (int side = 0; side < 2; side++) {
+                if (side == 0 ? (I.free_surf || j > fw) : (j < ny - fw + 1)) continue;
+                const int h = side == 0 ? j - 1 : j - ny + 2 * fw - 1;
                 float *p1 = I.psi_vyy + (long long)h * nx + (i - 1);
                 float *p2 = I.psi_vxy + (long long)h * nx + (i - 1);
                 float v = ADD<X>(MUL<X>(I.b_y[h], *p1), MUL<X>(I.a_y[h], vyy));
@@ -361,17 +387,6 @@ struct VDeriv {
                 *p1 = v;
                 *p2 = w;
                 vyy = ADD<X>(DIV<X>(vyy, I.K_y[h]), v);
-                vxy = ADD<X>(DIV<X>(vxy, I.K_yh[h]), w);
-            }
-            if (j >= ny - fw + 1) {
-                const int h = j - ny + 2 * fw - 1;
-                float *p1 = I.psi_vyy + (long long)h * nx + (i - 1);
-                float v = ADD<X>(MUL<X>(I.b_y[h], *p1), MUL<X>(I.a_y[h], vyy));
-                *p1 = v;
-                vyy = ADD<X>(DIV<X>(vyy, I.K_y[h]), v);
-                float *p2 = I.psi_vxy + (long long)h * nx + (i - 1);
-                float w = ADD<X>(MUL<X>(I.b_yh[h], *p2), MUL<X>(I.a_yh[h], vxy));
-                *p2 = w;
                 vxy = ADD<X>(DIV<X>(vxy, I.K_yh[h]), w);
             }
         }
@@ -386,7 +401,7 @@ struct VDeriv {
 template <int R, bool X>
 __global__ void __launch_bounds__(256) k_update_s_el(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = __ldg(ntb) + off;
+    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
     if (nt > I.nt) return;
     TileLoc t;
@@ -397,22 +412,41 @@ __global__ void __launch_bounds__(256) k_update_s_el(const Inst *__restrict__ in
 #pragma unroll
     for (int m = 1; m <= R; m++) hc[m] = I.hc[m];
     const float dhi = I.dhi_el;
+    const float *__restrict__ uipjp = I.uipjp + i;
+    const float *__restrict__ mu = I.mu + i;
+    const float *__restrict__ lam = I.lam + i;
+    float *__restrict__ sxx = I.sxx + i;
+    float *__restrict__ syy = I.syy + i;
+    float *__restrict__ sxy = I.sxy + i;
     VDeriv<R, X> D;
     D.prime(I, i, t.j0);
+    float nfip, nf, ng, nsxx, nsyy, nsxy;
+    auto fetch = [&](int j) {
+        const long long o = (long long)j * P;
+        nfip = __ldg(uipjp + o);
+        nf = __ldg(mu + o);
+        ng = __ldg(lam + o);
+        nsxx = sxx[o];
+        nsyy = syy[o];
+        nsxy = sxy[o];
+    };
+    fetch(t.j0);
     for (int j = t.j0; j <= t.j1; j++) {
-        D.load_row(I, i, j);
+        D.advance(j);
+        const float fipjp = nfip, f = nf, g = ng, s_xx = nsxx, s_yy = nsyy, s_xy = nsxy;
+        if (j < t.j1) {
+            D.fetch(j + 1);
+            fetch(j + 1);
+        }
         float vxx, vyx, vxy, vyy;
         D.compute(I, hc, i, j, dhi, vxx, vyx, vxy, vyy);
-        const long long o = (long long)j * P + i;
-        const float fipjp = I.uipjp[o];
-        const float f = I.mu[o];
-        const float g = I.lam[o];
+        const long long o = (long long)j * P;
         const float div = ADD<X>(vxx, vyy);
         const float gdiv = MUL<X>(g, div);
         const double f2 = 2.0 * (double)f;
-        I.sxy[o] = ADD<X>(I.sxy[o], MUL<X>(fipjp, ADD<X>(vyx, vxy)));
-        I.sxx[o] = F(DADD((double)I.sxx[o], DADD((double)gdiv, DMUL(f2, (double)vxx))));
-        I.syy[o] = F(DADD((double)I.syy[o], DADD((double)gdiv, DMUL(f2, (double)vyy))));
+        sxy[o] = ADD<X>(s_xy, MUL<X>(fipjp, ADD<X>(vyx, vxy)));
+        sxx[o] = F(DADD((double)s_xx, DADD((double)gdiv, DMUL(f2, (double)vxx))));
+        syy[o] = F(DADD((double)s_yy, DADD((double)gdiv, DMUL(f2, (double)vyy))));
         D.shift();
     }
 }
@@ -425,12 +459,13 @@ __global__ void __launch_bounds__(256) k_update_s_el(const Inst *__restrict__ in
 template <int R, int L, bool X>
 __global__ void __launch_bounds__(256) k_update_s_vi(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = __ldg(ntb) + off;
+    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
     if (nt > I.nt) return;
     TileLoc t;
     if (!tile_of(I, t)) return;
     const long long P = I.pitch;
+    const long long PL = I.plane;
     const int i = t.i;
     float hc[R + 1];
 #pragma unroll
@@ -444,25 +479,64 @@ __global__ void __launch_bounds__(256) k_update_s_vi(const Inst *__restrict__ in
         bip[l] = I.bip[l];
         cip[l] = I.cip[l];
     }
+    const float *__restrict__ c_muipjp = I.c_muipjp + i;
+    const float *__restrict__ c_tausipjp = I.c_tausipjp + i;
+    const float *__restrict__ c_mu = I.c_mu + i;
+    const float *__restrict__ c_taus = I.c_taus + i;
+    const float *__restrict__ c_pi = I.c_pi + i;
+    const float *__restrict__ c_taup = I.c_taup + i;
+    float *__restrict__ sxxp = I.sxx + i;
+    float *__restrict__ syyp = I.syy + i;
+    float *__restrict__ sxyp = I.sxy + i;
+    float *__restrict__ rp = I.r + i;
+    float *__restrict__ pp_ = I.p + i;
+    float *__restrict__ qp = I.q + i;
     VDeriv<R, X> D;
     D.prime(I, i, t.j0);
+    float nm[6], ns[3], nr[L], np_[L], nq[L];
+    auto fetch = [&](int j) {
+        const long long o = (long long)j * P;
+        nm[0] = __ldg(c_muipjp + o);
+        nm[1] = __ldg(c_tausipjp + o);
+        nm[2] = __ldg(c_mu + o);
+        nm[3] = __ldg(c_taus + o);
+        nm[4] = __ldg(c_pi + o);
+        nm[5] = __ldg(c_taup + o);
+        ns[0] = sxxp[o];
+        ns[1] = syyp[o];
+        ns[2] = sxyp[o];
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            nr[l] = rp[o + l * PL];
+            np_[l] = pp_[o + l * PL];
+            nq[l] = qp[o + l * PL];
+        }
+    };
+    fetch(t.j0);
     for (int j = t.j0; j <= t.j1; j++) {
-        D.load_row(I, i, j);
+        D.advance(j);
+        const float muipjp = nm[0], tsij = nm[1], mu = nm[2], taus = nm[3], pi = nm[4], taup = nm[5];
+        const float s_xx = ns[0], s_yy = ns[1], s_xy = ns[2];
+        float rr[L], pp[L], qq[L];
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            rr[l] = nr[l];
+            pp[l] = np_[l];
+            qq[l] = nq[l];
+        }
+        if (j < t.j1) {
+            D.fetch(j + 1);
+            fetch(j + 1);
+        }
         float vxx, vyx, vxy, vyy;
         D.compute(I, hc, i, j, dhi, vxx, vyx, vxy, vyy);
-        const long long o = (long long)j * P + i;
-        const float muipjp = I.c_muipjp[o], tsij = I.c_tausipjp[o];
-        const float mu = I.c_mu[o], taus = I.c_taus[o], pi = I.c_pi[o], taup = I.c_taup[o];
+        const long long o = (long long)j * P;
         const float fipjp = F(DMUL((double)__fmul_rn(muipjp, DT), DADD(1.0, (double)__fmul_rn(fL, tsij))));
         const float f = F(DMUL((double)__fmul_rn(mu, DT), DADD(1.0, (double)__fmul_rn(fL, taus))));
         const float g = F(DMUL((double)__fmul_rn(pi, DT), DADD(1.0, (double)__fmul_rn(fL, taup))));
         float sumr = 0.0f, sump = 0.0f, sumq = 0.0f;
-        float rr[L], pp[L], qq[L];
 #pragma unroll
         for (int l = 0; l < L; l++) {
-            rr[l] = I.r[o + l * I.plane];
-            pp[l] = I.p[o + l * I.plane];
-            qq[l] = I.q[o + l * I.plane];
             sumr = ADD<X>(sumr, rr[l]);
             sump = ADD<X>(sump, pp[l]);
             sumq = ADD<X>(sumq, qq[l]);
@@ -471,9 +545,9 @@ __global__ void __launch_bounds__(256) k_update_s_vi(const Inst *__restrict__ in
         const float dv = ADD<X>(vxx, vyy);
         const float gdv = MUL<X>(g, dv);
         const double f2 = 2.0 * (double)f;
-        float sxy = ADD<X>(I.sxy[o], ADD<X>(MUL<X>(fipjp, sh), MUL<X>(dthalbe, sumr)));
-        float sxx = F(DADD((double)I.sxx[o], DADD(DSUB((double)gdv, DMUL(f2, (double)vyy)), (double)MUL<X>(dthalbe, sump))));
-        float syy = F(DADD((double)I.syy[o], DADD(DSUB((double)gdv, DMUL(f2, (double)vxx)), (double)MUL<X>(dthalbe, sumq))));
+        float sxy = ADD<X>(s_xy, ADD<X>(MUL<X>(fipjp, sh), MUL<X>(dthalbe, sumr)));
+        float sxx = F(DADD((double)s_xx, DADD(DSUB((double)gdv, DMUL(f2, (double)vyy)), (double)MUL<X>(dthalbe, sump))));
+        float syy = F(DADD((double)s_yy, DADD(DSUB((double)gdv, DMUL(f2, (double)vxx)), (double)MUL<X>(dthalbe, sumq))));
         sumr = sump = sumq = 0.0f;
 #pragma unroll
         for (int l = 0; l < L; l++) {
@@ -484,16 +558,16 @@ __global__ void __launch_bounds__(256) k_update_s_vi(const Inst *__restrict__ in
             const double d2 = 2.0 * (double)dd;
             const float pv = F(DMUL((double)bip[l], DADD((double)SUB<X>(MUL<X>(pp[l], cip[l]), MUL<X>(ee, dv)), DMUL(d2, (double)vyy))));
             const float qv = F(DMUL((double)bip[l], DADD((double)SUB<X>(MUL<X>(qq[l], cip[l]), MUL<X>(ee, dv)), DMUL(d2, (double)vxx))));
-            I.r[o + l * I.plane] = r;
-            I.p[o + l * I.plane] = pv;
-            I.q[o + l * I.plane] = qv;
+            rp[o + l * PL] = r;
+            pp_[o + l * PL] = pv;
+            qp[o + l * PL] = qv;
             sumr = ADD<X>(sumr, r);
             sump = ADD<X>(sump, pv);
             sumq = ADD<X>(sumq, qv);
         }
-        I.sxy[o] = ADD<X>(sxy, MUL<X>(dthalbe, sumr));
-        I.sxx[o] = ADD<X>(sxx, MUL<X>(dthalbe, sump));
-        I.syy[o] = ADD<X>(syy, MUL<X>(dthalbe, sumq));
+        sxyp[o] = ADD<X>(sxy, MUL<X>(dthalbe, sumr));
+        sxxp[o] = ADD<X>(sxx, MUL<X>(dthalbe, sump));
+        syyp[o] = ADD<X>(syy, MUL<X>(dthalbe, sumq));
         D.shift();
     }
 }
@@ -505,7 +579,7 @@ __global__ void __launch_bounds__(256) k_update_s_vi(const Inst *__restrict__ in
 // ===========================================================================
 __global__ void k_inject_s(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = __ldg(ntb) + off;
+    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
     if (nt > I.nt) return;
     const long long P = I.pitch;
@@ -568,7 +642,7 @@ __global__ void k_inject_s(const Inst *__restrict__ insts, const int *__restrict
 template <int R, bool X>
 __global__ void k_surface_el(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = __ldg(ntb) + off;
+    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
     if (nt > I.nt || !I.free_surf) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -618,7 +692,7 @@ __global__ void k_surface_el(const Inst *__restrict__ insts, const int *__restri
 template <int R, int L, bool X>
 __global__ void k_surface_vi(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = __ldg(ntb) + off;
+    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
     if (nt > I.nt || !I.free_surf) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -694,7 +768,7 @@ __global__ void k_surface_vi(const Inst *__restrict__ insts, const int *__restri
 template <int R>
 __global__ void k_seismo(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = __ldg(ntb) + off;
+    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
     if (nt > I.nt) return;
     const long long P = I.pitch;
@@ -772,7 +846,7 @@ __device__ __forceinline__ float pow2_scale(float amax)
 
 __global__ void k_snap_store(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = __ldg(ntb) + off;
+    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
     if (nt > I.nt || I.mode != 0 || !I.store || ((nt - 1) % I.dtinv) != 0) return;
     const int k = (nt - 1) / I.dtinv;
@@ -838,7 +912,7 @@ __device__ __forceinline__ float snap_load(const Inst &I, long long slot, long l
 // ===========================================================================
 __global__ void k_correlate(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = __ldg(ntb) + off;
+    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
     if (nt > I.nt || I.mode != 1) return;
     const int nf = I.nt - nt + 1;   // mirrored forward step

@@ -121,6 +121,7 @@ SIGNATURES = {
     "dn_run_steps": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "dn_shot_get_snapshot": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_float_p]),
     "dn_last_run_stats": (ctypes.c_int, [_c_double_p, _P(ctypes.c_longlong)]),
+    "dn_profile_steps": (ctypes.c_int, [_P(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_double_p]),
 }
 
 

@@ -265,3 +265,14 @@ def last_run_stats():
     nl = ctypes.c_longlong(0)
     lib.dn_last_run_stats(ctypes.byref(ms), ctypes.byref(nl))
     return ms.value, nl.value
+
+
+KERNEL_SLOTS = ("update_v", "inject_v", "update_s", "inject_s", "surface", "seismo", "snap_store", "correlate")
+
+
+def profile_steps(shots: Sequence[Shot], mode=_lib.MODE_FORWARD, nsteps=20):
+    """Average device ms per launch of each kernel of the batched step."""
+    arr = (ctypes.c_void_p * len(shots))(*[s.handle for s in shots])
+    out = (ctypes.c_double * 8)()
+    check(lib.dn_profile_steps(arr, len(shots), mode, nsteps, out))
+    return dict(zip(KERNEL_SLOTS, list(out)))

@@ -222,6 +222,13 @@ int dn_shot_get_snapshot(const dn_shot *s, int k, int field, float *out);
  * around the time loop only) and the number of kernel launches it issued. */
 int dn_last_run_stats(double *device_ms, long long *launches);
 
+/* Per-kernel device time of `nsteps` time steps of a batch (direct launches with
+ * CUDA events between kernels, for measurement only; leaves the shots' results
+ * undefined).  ms_out[8] = average ms per launch of: velocity update, velocity
+ * source injection, stress update, stress source injection, free surface,
+ * receivers, snapshot store, cross-correlation (0 where not launched). */
+int dn_profile_steps(dn_shot *const *shots, int n, int mode, int nsteps, double *ms_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -155,6 +155,11 @@ class Reference:
         assert self.lib.refh_set_acq(ctypes.c_int(ns), _fp(srcpos), _fp(self._keep[1]), ctypes.c_int(self.ntr),
                                      _ip(rec[0]), _ip(rec[1])) == 0
 
+    def __del__(self):
+        import shutil
+
+        shutil.rmtree(self.workdir, ignore_errors=True)
+
     def hc(self):
         a = np.zeros(7, np.float32)
         self.lib.refh_get_hc(_fp(a))
@@ -222,3 +227,10 @@ def rel_l2(a, b):
     b = np.asarray(b, np.float64)
     n = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (n if n > 0 else 1.0))
+
+
+def reference_forward_sections(p, model, src, rec):
+    """vx and vy sections of one forward run of the reference's code (run it in a fresh process)."""
+    r = Reference(p, model, src, rec, mode_global=0)
+    r.run(0)
+    return r.sections(0), r.sections(1)

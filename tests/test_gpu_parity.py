@@ -1,0 +1,200 @@
+"""GPU parity of the B200 propagator against the CPU oracles.
+
+Bar (all on seeded inputs at sizes the CPU oracle finishes in seconds):
+* DN_ARITH_EXACT (default) + FP32 snapshots + FP32 accumulation: sections,
+  final wavefields, correlation accumulators and gradients are bit-identical
+  to the float restatement, which is itself bit-identical to the reference's
+  compiled CPU code (tests/test_oracle_pin.py);
+* FP64 accumulation: gradients within 1e-6 relative L2 of the float oracle;
+* FP16 snapshots: gradients within 1e-3 relative L2 of the FP64 oracle;
+* DN_ARITH_FMA: sections within 1e-5 relative L2 of the exact path.
+"""
+import numpy as np
+import pytest
+
+import denise_b200 as dn
+from denise_b200 import synth
+
+import oracles as O
+
+pytestmark = pytest.mark.gpu
+
+FL5 = (2.0, 8.0, 25.0, 1.0, 60.0)   # relaxation frequencies for up to 5 mechanisms
+
+
+def small_case(L=0, fdorder=8, free_surf=1, nt=300, styp=1, nx=64, ny=48, seed=3, **kw):
+    p = synth.c0_params(nx=nx, ny=ny, nt=nt, fw=10, L=L, fl=FL5[:L], ts=0.1, fdorder=fdorder,
+                        free_surf=free_surf, dtinv=3, seismo=4, quelltypb=1, **kw)
+    vp, vs, rho = synth.base_model(p.nx, p.ny, p.dh, seed)
+    qp, qs = synth.q_model(p.nx, p.ny, seed)
+    sig = synth.ricker_source(p, 40.0)[None, :] * 1e3
+    src = (np.array([nx // 2 - 2], np.int32), np.array([3], np.int32), sig, np.array([styp], np.int32),
+           np.array([30.0], np.float32))
+    nr = (nx - 10) // 4
+    rec = (np.arange(5, 5 + 4 * nr, 4).astype(np.int32), np.full(nr, 4, np.int32))
+    return p, (vp, vs, rho, qp, qs), src, rec
+
+
+def gpu_shot(p, model, src, rec):
+    m = dn.Model(p, *model[:3], model[3] if p.L else None, model[4] if p.L else None)
+    s = dn.Shot(m, src[0], src[1], src[2], rec[0], rec[1], src_type=src[3], src_azi=src[4])
+    return m, s
+
+
+CASES = [
+    dict(L=0, fdorder=8, free_surf=1),
+    dict(L=0, fdorder=2, free_surf=1),
+    dict(L=0, fdorder=4, free_surf=0),
+    dict(L=0, fdorder=6, free_surf=1, styp=2),
+    dict(L=0, fdorder=10, free_surf=1, styp=3),
+    dict(L=0, fdorder=12, free_surf=0, styp=4),
+    dict(L=3, fdorder=8, free_surf=1),
+    dict(L=1, fdorder=4, free_surf=1),
+    dict(L=2, fdorder=12, free_surf=0),
+    dict(L=5, fdorder=6, free_surf=1, styp=5),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
+def test_forward_bitexact(case):
+    p, model, src, rec = small_case(**case)
+    ref = O.Restatement(p, model, src, rec, "f")
+    ref.forward(store=False)
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run([s], dn.MODE_FORWARD)
+    for comp in range(5):
+        np.testing.assert_array_equal(s.sections(comp), ref.sections(comp), err_msg=f"section {comp}")
+    for name, fid in (("vx", 0), ("vy", 1), ("sxx", 2), ("syy", 3), ("sxy", 4)):
+        np.testing.assert_array_equal(s.field(fid), ref.field(fid), err_msg=name)
+
+
+@pytest.mark.parametrize("case", [dict(L=0, fdorder=8), dict(L=3, fdorder=8), dict(L=0, fdorder=4, free_surf=0)],
+                         ids=["elastic8", "visco8", "elastic4-nofs"])
+def test_plain_path_bitexact(case):
+    p, model, src, rec = small_case(**case)
+    ref = O.Restatement(p, model, src, rec, "f")
+    ref.forward(store=False)
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run_plain(s, dn.MODE_FORWARD)
+    np.testing.assert_array_equal(s.sections(dn.SEC_VY), ref.sections(1))
+    np.testing.assert_array_equal(s.field(2), ref.field(2))
+
+
+def _residuals(p, syn_vx, syn_vy):
+    # L2 residual of calc_res (GRAD_FORM 1): time-integrated, reversed, first sample zeroed,
+    # against zero "observed" data scaled from the synthetics
+    out = []
+    for syn in (syn_vx, syn_vy):
+        obs = 0.7 * syn
+        d = syn - obs
+        d[:, 0] = 0.0
+        integ = np.zeros_like(d)
+        acc = np.zeros(d.shape[0], np.float32)
+        for t in range(p.nt):
+            acc = (acc + np.float32(p.dt) * d[:, t]).astype(np.float32)
+            integ[:, p.nt - 1 - t] = acc
+        out.append(integ.astype(np.float32))
+    return out
+
+
+@pytest.mark.parametrize("L", [0, 3])
+def test_gradient_bitexact(L):
+    p, model, src, rec = small_case(L=L, store_snapshots=1)
+    ref = O.Restatement(p, model, src, rec, "f")
+    ref.forward(store=True)
+    rvx, rvy = _residuals(p, ref.sections(0), ref.sections(1))
+    ref.adjoint(rvx, rvy, None)
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run([s], dn.MODE_FORWARD)
+    np.testing.assert_array_equal(s.sections(0), ref.sections(0))
+    s.set_residuals(rvx, rvy, None)
+    dn.run([s], dn.MODE_ADJOINT)
+    for fid in (7, 8, 9):
+        np.testing.assert_array_equal(s.field(fid), ref.field(fid), err_msg=f"accumulator {fid}")
+    s.accumulate_gradient()
+    for a, b, n in zip(m.gradient(), ref.gradient(), ("vp", "vs", "rho")):
+        np.testing.assert_array_equal(a, b, err_msg=f"gradient {n}")
+
+
+def test_gradient_fp64_accumulation():
+    p, model, src, rec = small_case(store_snapshots=1, grad_accum=dn.ACC_F64)
+    ref = O.Restatement(p, model, src, rec, "f")
+    ref.forward(store=True)
+    rvx, rvy = _residuals(p, ref.sections(0), ref.sections(1))
+    ref.adjoint(rvx, rvy, None)
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run([s], dn.MODE_FORWARD)
+    s.set_residuals(rvx, rvy, None)
+    dn.run([s], dn.MODE_ADJOINT)
+    s.accumulate_gradient()
+    for a, b in zip(m.gradient(), ref.gradient()):
+        assert O.rel_l2(a, b) < 1e-6
+
+
+@pytest.mark.parametrize("prec,tol", [(dn.SNAP_F16, 1e-3), (dn.SNAP_BF16, 1e-2)], ids=["fp16", "bf16"])
+def test_gradient_half_snapshots_vs_fp64(prec, tol):
+    p, model, src, rec = small_case(store_snapshots=1, snap_precision=prec, grad_accum=dn.ACC_F64, nt=400)
+    ref = O.Restatement(p, model, src, rec, "d")
+    ref.forward(store=True)
+    rvx, rvy = _residuals(p, ref.sections(0).astype(np.float32), ref.sections(1).astype(np.float32))
+    ref.adjoint(rvx, rvy, None)
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run([s], dn.MODE_FORWARD)
+    s.set_residuals(rvx, rvy, None)
+    dn.run([s], dn.MODE_ADJOINT)
+    s.accumulate_gradient()
+    errs = [O.rel_l2(a, b) for a, b in zip(m.gradient(), ref.gradient())]
+    assert max(errs) < tol, errs
+
+
+def test_fma_mode_close():
+    p, model, src, rec = small_case(nt=400)
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run([s])
+    exact = s.sections(1)
+    p2 = p.replace(arith=dn.ARITH_FMA)
+    m2, s2 = gpu_shot(p2, model, src, rec)
+    dn.run([s2])
+    assert O.rel_l2(s2.sections(1), exact) < 1e-5
+
+
+def test_batch_uneven_equals_individual():
+    cases = [small_case(nx=64, ny=48, nt=300, seed=1), small_case(nx=80, ny=40, nt=250, seed=2),
+             small_case(nx=50, ny=60, nt=320, seed=5)]
+    shots, refs = [], []
+    for p, model, src, rec in cases:
+        m, s = gpu_shot(p, model, src, rec)
+        shots.append((m, s))
+        r = O.Restatement(p, model, src, rec, "f")
+        r.forward()
+        refs.append(r)
+    dn.run([s for _, s in shots])
+    for (m, s), r in zip(shots, refs):
+        np.testing.assert_array_equal(s.sections(0), r.sections(0))
+        np.testing.assert_array_equal(s.field(3), r.field(3))
+    # a second run of the same batch replays the cached graph and must reproduce itself
+    first = [s.sections(1) for _, s in shots]
+    dn.run([s for _, s in shots])
+    for (m, s), f in zip(shots, first):
+        np.testing.assert_array_equal(s.sections(1), f)
+
+
+def test_unstable_model_reports_status():
+    p, model, src, rec = small_case(nt=50)
+    vp = model[0].copy()
+    vp[p.nx // 2 - 1, p.ny // 2 - 1] = np.nan   # a NaN planted in the model on the host
+    m, s = gpu_shot(p, (vp,) + model[1:], src, rec)
+    with pytest.raises(dn.DeniseError) as e:
+        dn.run([s])
+    assert e.value.code == -3
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="reference build not present")
+def test_forward_matches_reference_build():
+    p, model, src, rec = small_case(L=0, nt=200)
+
+    rx, ry = O.run_isolated(O.reference_forward_sections, p, model, src, rec)
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run([s])
+    np.testing.assert_array_equal(s.sections(0), rx)
+    np.testing.assert_array_equal(s.sections(1), ry)
