@@ -327,3 +327,19 @@ int refh_ass_grad(float *gvp, float *gvs, float *grho)
     to_file(FWI.waveconv_rho_shot, grho);
     return 0;
 }
+
+/* wavelet() of the reference (wavelet.c) for one source: QUELLART, tshift, fc, amp */
+extern int QUELLART, N_ORDER;
+int refh_wavelet(int quellart, int n_order, float tshift, float fc, float amp, float *out)
+{
+    float **sp = matrix(1, 8, 1, 1);
+    sp[4][1] = tshift;
+    sp[5][1] = fc;
+    sp[6][1] = amp;
+    QUELLART = quellart;
+    N_ORDER = n_order;
+    float **sig = wavelet(sp, 1, 1);
+    for (int t = 1; t <= NT; t++) out[t - 1] = sig[1][t];
+    N_ORDER = 0;
+    return 0;
+}
