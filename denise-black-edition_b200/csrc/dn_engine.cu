@@ -389,7 +389,8 @@ static void tile_shape(const dn_params *p, int &bx, int &zch)
     // (more CTAs), large ones long register streams.
     bx = 128;
     long long cells = (long long)p->nx * p->ny;
-    zch = cells < (1 << 19) ? 8 : 32;
+    zch = 8;   // measured best on B200 for the 2000 x 600 batched workload (4-32 swept)
+    (void)cells;
     const char *ev = getenv("DN_TILE");
     if (ev) {
         int a = 0, b = 0;
@@ -952,7 +953,9 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c)
     c.L = p0.L;
     c.exact = p0.arith == DN_ARITH_EXACT;
     c.bx = shots[0]->bx;
-    c.tma = c.bx == TMA_W && !(getenv("DN_KERNEL") && strcmp(getenv("DN_KERNEL"), "reg") == 0);
+    // stencil kernels: register streaming (default, fastest measured on B200) or, with
+    // DN_KERNEL=tma, the bulk-copy row pipeline of dn_kernels_tma.cuh
+    c.tma = c.bx == TMA_W && getenv("DN_KERNEL") && strcmp(getenv("DN_KERNEL"), "tma") == 0;
     c.any_surf = c.any_src_s = c.any_store = c.any_adj = c.any_rec = false;
     int maxtiles = 0, maxsrc = 1, maxnx = 1, maxtr = 1;
     for (int k = 0; k < n; k++) {
