@@ -23,7 +23,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_CFLAGS = ["-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-Wno-unused-function"]
 
-CU_SOURCES = ["dn_engine.cu"]
+CU_SOURCES = ["dn_engine.cu", "dn_residual.cu"]
 C_SOURCES = ["dn_setup.c"]
 HOST_SOURCES = ["dn_io.c", "dn_driver.c"]
 CLI_SOURCES = ["denise_b200_main.c"]

@@ -1441,3 +1441,50 @@ extern "C" int dn_profile_steps(dn_shot *const *shots, int n, int mode, int nste
     if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "dn_profile_steps: %s", cudaGetErrorString(e));
     return DN_OK;
 }
+
+// ---------------------------------------------------------------------------
+// data residual of a forward-run shot into its adjoint sources (calc_res_PSV +
+// calc_res, LNORM 2): obs [ntr][nt] host, comp DN_SEC_VX / VY / P
+// ---------------------------------------------------------------------------
+extern "C" int dn_residual_l2_launch(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt,
+                                     int grad_form, double *scratch, cudaStream_t stream);
+
+extern "C" int dn_shot_residual(dn_shot *s, int comp, const float *obs, double *l2)
+{
+    if (!s || !obs) return dn_fail(DN_EINVAL, "dn_shot_residual: null argument");
+    if (comp != DN_SEC_VX && comp != DN_SEC_VY && comp != DN_SEC_P)
+        return dn_fail(DN_EINVAL, "dn_shot_residual: component must be vx, vy or p");
+    if (s->ntr < 1) return dn_fail(DN_EINVAL, "dn_shot_residual: shot has no receivers");
+    DevState *ds;
+    int st = dev_state(s->m->device, &ds);
+    if (st) return st;
+    CU(cudaSetDevice(s->m->device));
+    const int nt = s->p.nt, ntr = s->ntr;
+    const size_t n = (size_t)ntr * nt;
+    float *dobs = nullptr;
+    double *scratch = nullptr;
+    if (cudaMalloc(&dobs, n * 4) != cudaSuccess || cudaMalloc(&scratch, sizeof(double) * (ntr + 1)) != cudaSuccess) {
+        cudaFree(dobs);
+        cudaGetLastError();
+        return dn_fail(DN_ENOMEM, "dn_shot_residual: device allocation failed");
+    }
+    const int k = comp == DN_SEC_VX ? 0 : (comp == DN_SEC_VY ? 1 : 2);
+    const size_t rs = (size_t)std::max(s->ntr, 1) * nt;
+    double h = 0.0;
+    cudaError_t e = cudaMemcpyAsync(dobs, obs, n * 4, cudaMemcpyHostToDevice, ds->stream);
+    if (e == cudaSuccess)
+        st = dn_residual_l2_launch(s->d_sec + (size_t)comp * nt * ntr, dobs, s->d_res + k * rs, ntr, nt, s->p.dt,
+                                   s->p.grad_form, scratch, ds->stream);
+    else st = dn_fail(DN_EDEVICE, "dn_shot_residual: %s", cudaGetErrorString(e));
+    if (!st) {
+        e = cudaMemcpyAsync(&h, scratch + ntr, sizeof(double), cudaMemcpyDeviceToHost, ds->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ds->stream);
+        if (e != cudaSuccess) st = dn_fail(DN_EDEVICE, "dn_shot_residual: %s", cudaGetErrorString(e));
+    }
+    cudaFree(dobs);
+    cudaFree(scratch);
+    if (st) return st;
+    s->has_res[k] = 1;
+    if (l2) *l2 = h;
+    return DN_OK;
+}

@@ -122,6 +122,9 @@ SIGNATURES = {
     "dn_shot_get_snapshot": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_float_p]),
     "dn_last_run_stats": (ctypes.c_int, [_c_double_p, _P(ctypes.c_longlong)]),
     "dn_profile_steps": (ctypes.c_int, [_P(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_double_p]),
+    "dn_residual_l2": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                      _c_double_p]),
+    "dn_shot_residual": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p, _c_double_p]),
 }
 
 

@@ -228,6 +228,14 @@ class Shot:
         arrs = [_f32(a, shp) if a is not None else None for a in (vx, vy, p)]
         check(lib.dn_shot_set_residuals(self.handle, *[fptr(a) for a in arrs]))
 
+    def residual(self, obs, comp=_lib.SEC_VX):
+        """L2 residual against observed data obs (ntr, nt) into this shot's adjoint
+        source of `comp`; returns the component's misfit 0.5*sum(r^2)."""
+        l2 = ctypes.c_double(0.0)
+        o = _f32(obs, (self.ntr, self.model.params.nt))
+        check(lib.dn_shot_residual(self.handle, comp, fptr(o), ctypes.byref(l2)))
+        return l2.value
+
     def accumulate_gradient(self):
         check(lib.dn_shot_accumulate_gradient(self.handle))
 

@@ -222,6 +222,20 @@ int dn_shot_get_snapshot(const dn_shot *s, int k, int field, float *out);
  * around the time loop only) and the number of kernel launches it issued. */
 int dn_last_run_stats(double *device_ms, long long *launches);
 
+/* calc_res() for LNORM = 2 (src/calc_res.c:306-445 residual, :514-568 misfit) on
+ * the device.  syn_tm: synthetic section, time-major [nt][ntr] (the layout the
+ * propagator records); obs: observed section [ntr][nt]; res (out): adjoint
+ * source [ntr][nt], time-reversed, first observed sample replaced by the
+ * synthetic one, time-integrated when grad_form == 1; l2 (out, host): the misfit
+ * 0.5*sum(res^2) accumulated in double.  All arrays are device pointers; the
+ * call allocates ntr+1 doubles of device scratch for the per-trace sums. */
+int dn_residual_l2(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt, int grad_form,
+                   double *l2);
+/* The same for a shot after its forward run: obs [ntr][nt] in host memory,
+ * comp = DN_SEC_VX / DN_SEC_VY / DN_SEC_P; the residual becomes the shot's
+ * adjoint source of that component (calc_res_PSV.c), l2 the component's misfit. */
+int dn_shot_residual(dn_shot *s, int comp, const float *obs, double *l2);
+
 /* Per-kernel device time of `nsteps` time steps of a batch (direct launches with
  * CUDA events between kernels, for measurement only; leaves the shots' results
  * undefined).  ms_out[8] = average ms per launch of: velocity update, velocity
