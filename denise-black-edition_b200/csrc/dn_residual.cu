@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <mutex>
 
 #include "dn_internal.h"
 
@@ -81,4 +82,79 @@ extern "C" int dn_residual_l2(const float *syn_tm, const float *obs, float *res,
     cudaFree(scratch);
     if (!st && l2) *l2 = h;
     return st;
+}
+
+// ---------------------------------------------------------------------------
+// dn_residual_l2_noalloc: the same residual and misfit for callers that must
+// not allocate device memory on the call, e.g. an inversion loop that runs
+// under a fixed device-memory budget (every byte pre-reserved for shots and
+// snapshots) or code that must not synchronise the device through
+// cudaMalloc/cudaFree between shots.  The per-trace partial sums live in a
+// file-scope device array of DN_RESIDUAL_NOALLOC_MAX_TRACES + 1 doubles
+// (128 KiB + 8 B per device); larger trace counts are rejected.
+//
+// Set-up: the first call on each device looks up the array's address with that
+// device current (cudaGetSymbolAddress, which may load this module on the
+// device) and caches it; make that first call before any stream capture.
+// Nothing in the scratch has to start at zero: k_residual_l2 writes every
+// partial sum k_sum_partials reads, and the misfit slot is written, not added
+// to.  There is one scratch array per device, so calls that overlap on the
+// same device (from several host threads at once) race on it and may return
+// each other's misfit; serialise them.  Each call returns only after its
+// kernels and the copy of the misfit have finished.
+// ---------------------------------------------------------------------------
+#define DN_RESIDUAL_NOALLOC_MAX_TRACES 16384
+#define DN_RESIDUAL_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) double g_residual_scratch[DN_RESIDUAL_NOALLOC_MAX_TRACES + 1];
+
+namespace {
+
+std::mutex g_scratch_mutex;
+double *g_scratch_ptr[DN_RESIDUAL_NOALLOC_MAX_DEVICES];
+
+// Address of this device's scratch array; looked up once per device.
+int residual_scratch(double **out)
+{
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "dn_residual_l2_noalloc: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= DN_RESIDUAL_NOALLOC_MAX_DEVICES)
+        return dn_fail(DN_ENOTSUP, "dn_residual_l2_noalloc: device %d beyond the %d supported", dev,
+                       DN_RESIDUAL_NOALLOC_MAX_DEVICES);
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[dev]) {
+        double *p = nullptr;
+        e = cudaGetSymbolAddress((void **)&p, g_residual_scratch);
+        if (e != cudaSuccess || !p)
+            return dn_fail(DN_EDEVICE, "dn_residual_l2_noalloc: scratch address lookup on device %d: %s", dev,
+                           cudaGetErrorString(e));
+        g_scratch_ptr[dev] = p;
+    }
+    *out = g_scratch_ptr[dev];
+    return DN_OK;
+}
+
+}   // namespace
+
+extern "C" int dn_residual_l2_noalloc(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt,
+                                      int grad_form, double *l2)
+{
+    if (!syn_tm || !obs || !res || ntr < 1 || nt < 1)
+        return dn_fail(DN_EINVAL, "dn_residual_l2_noalloc: bad arguments");
+    if (grad_form != 1 && grad_form != 2)
+        return dn_fail(DN_EINVAL, "dn_residual_l2_noalloc: GRAD_FORM must be 1 or 2");
+    if (ntr > DN_RESIDUAL_NOALLOC_MAX_TRACES)
+        return dn_fail(DN_EINVAL, "dn_residual_l2_noalloc: %d traces exceed the static scratch of %d traces "
+                       "(use dn_residual_l2)", ntr, DN_RESIDUAL_NOALLOC_MAX_TRACES);
+    double *scratch = nullptr;
+    int st = residual_scratch(&scratch);
+    if (st) return st;
+    st = dn_residual_l2_launch(syn_tm, obs, res, ntr, nt, dt, grad_form, scratch, 0);
+    if (st) return st;
+    double h = 0.0;
+    cudaError_t e = cudaMemcpy(&h, scratch + ntr, sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "dn_residual_l2_noalloc: %s", cudaGetErrorString(e));
+    if (l2) *l2 = h;
+    return DN_OK;
 }

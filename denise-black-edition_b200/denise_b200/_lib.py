@@ -125,6 +125,8 @@ SIGNATURES = {
     "dn_residual_l2": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
                                       _c_double_p]),
     "dn_shot_residual": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p, _c_double_p]),
+    "dn_residual_l2_noalloc": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                              ctypes.c_int, _c_double_p]),
 }
 
 

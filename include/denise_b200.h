@@ -231,6 +231,17 @@ int dn_last_run_stats(double *device_ms, long long *launches);
  * call allocates ntr+1 doubles of device scratch for the per-trace sums. */
 int dn_residual_l2(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt, int grad_form,
                    double *l2);
+/* dn_residual_l2 for callers that cannot allocate device memory during the
+ * call (an inversion loop that has reserved all device memory for its shots
+ * and snapshots, or that must not let cudaMalloc/cudaFree synchronise the
+ * device between shots).  No counterpart in the reference: calc_res() works
+ * on host arrays.  Same arguments and results as dn_residual_l2, but the
+ * per-trace sums use a static device array, so ntr <= 16384 (DN_EINVAL
+ * beyond).  The first call on each device (with that device current) looks up
+ * the array and should come before any stream capture.  Calls that overlap on
+ * one device share that array and race; serialise them. */
+int dn_residual_l2_noalloc(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt,
+                           int grad_form, double *l2);
 /* The same for a shot after its forward run: obs [ntr][nt] in host memory,
  * comp = DN_SEC_VX / DN_SEC_VY / DN_SEC_P; the residual becomes the shot's
  * adjoint source of that component (calc_res_PSV.c), l2 the component's misfit. */
