@@ -9,6 +9,7 @@ the reference's float/double rounding bit for bit.
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -23,7 +24,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_CFLAGS = ["-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-Wno-unused-function"]
 
-CU_SOURCES = ["dn_engine.cu", "dn_residual.cu"]
+CU_SOURCES = ["dn_engine.cu", "dn_residual.cu"] + [f"dn_launch_r{r}.cu" for r in range(1, 7)]
 C_SOURCES = ["dn_setup.c"]
 HOST_SOURCES = ["dn_io.c", "dn_driver.c"]
 CLI_SOURCES = ["denise_b200_main.c"]
@@ -49,14 +50,17 @@ def build(verbose=True):
     headers += [os.path.join(INC, "denise_b200.h")]
     if os.path.isdir(HOST):
         headers += [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".h")]
-    objs = []
+    objs, jobs = [], []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if _newer(o, [s] + headers):
-            _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
-                                  "-I", INC, "-I", CSRC, "-c", s, "-o", o])
+            jobs.append([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
+                                         "-I", INC, "-I", CSRC, "-c", s, "-o", o])
         objs.append(o)
+    # the CUDA translation units are independent: compile them concurrently
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        list(ex.map(_run, jobs))
     for d, srcs in ((CSRC, C_SOURCES), (HOST, HOST_SOURCES)):
         for src in srcs:
             s = os.path.join(d, src)

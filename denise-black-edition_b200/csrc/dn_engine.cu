@@ -16,7 +16,7 @@
 #include <vector>
 
 #include "dn_internal.h"
-#include "dn_kernels_tma.cuh"
+#include "dn_launch.cuh"
 
 using namespace dn;
 
@@ -131,6 +131,8 @@ struct dn_model {
     void *dgrad = nullptr;         // stacked gradient: 3 x nx*ny (float or double), row-major [j][i]
     int grad64;
     int nshots = 0;
+    float rdh = 0.0f;              // RN(1 / DH)
+    int fastdiv = 0;               // div_markstein verified for DH on this device
     float *field(int f) const { return dmat + (long long)f * lay.plane + lay.origin; }
 };
 
@@ -210,6 +212,62 @@ extern "C" int dn_model_footprint(const dn_params *p, size_t *bytes)
     size_t b = (size_t)nf * L.plane * 4 + 12 * 2 * (size_t)std::max(p->fw, 1) * 4 + 4 * (size_t)p->nx * 4;
     b += 3 * (size_t)p->nx * p->ny * (p->grad_accum == DN_ACC_F64 ? 8 : 4);
     if (bytes) *bytes = b;
+    return DN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Exhaustive check of the fast division by DH (div_markstein) against
+// __fdiv_rn over all 2^32 float dividends; ~5 ms once per distinct DH and
+// device.  DN_FASTDIV=0 skips it and keeps the general division.
+// ---------------------------------------------------------------------------
+__global__ void k_fastdiv_check(float d, unsigned long long n, unsigned long long *bad, float *y_out)
+{
+    const float y = __frcp_rn(d);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *y_out = y;
+    unsigned long long nbad = 0;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const float a = __uint_as_float((unsigned)k);
+        const float q0 = __fdiv_rn(a, d), q1 = div_markstein(a, d, y);
+        if (__float_as_uint(q0) != __float_as_uint(q1) && !(q0 != q0 && q1 != q1)) nbad++;
+    }
+    if (nbad) atomicAdd(bad, nbad);
+}
+
+static std::mutex g_fastdiv_mu;
+static std::map<std::pair<int, unsigned>, std::pair<int, float>> g_fastdiv;   // (device, DH bits) -> (ok, y)
+
+static int fastdiv_setup(int device, float dh, int *ok, float *y)
+{
+    unsigned bits;
+    memcpy(&bits, &dh, 4);
+    std::lock_guard<std::mutex> lk(g_fastdiv_mu);
+    auto it = g_fastdiv.find({device, bits});
+    if (it != g_fastdiv.end()) {
+        *ok = it->second.first;
+        *y = it->second.second;
+        return DN_OK;
+    }
+    const char *ev = getenv("DN_FASTDIV");
+    const bool enabled = !(ev && ev[0] == '0');
+    char *buf = nullptr;
+    if (cudaMalloc(&buf, 16) != cudaSuccess) return dn_fail(DN_ENOMEM, "fast division check: allocation failed");
+    unsigned long long hbad = 0;
+    float hy = 0.0f;
+    cudaError_t e = cudaMemset(buf, 0, 16);
+    if (e == cudaSuccess) {
+        // disabled: n = 0 computes y only
+        k_fastdiv_check<<<148 * 8, 256>>>(dh, enabled ? (1ull << 32) : 0ull, (unsigned long long *)buf,
+                                          (float *)(buf + 8));
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&hbad, buf, 8, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&hy, buf + 8, 4, cudaMemcpyDeviceToHost);
+    cudaFree(buf);
+    if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "fast division check: %s", cudaGetErrorString(e));
+    *ok = enabled && hbad == 0;
+    *y = hy;
+    g_fastdiv[{device, bits}] = {*ok, hy};
     return DN_OK;
 }
 
@@ -357,6 +415,11 @@ extern "C" int dn_model_create(const dn_params *p, const float *vp, const float 
         dn_model_destroy(m);
         return dn_fail(DN_EDEVICE, "dn_model_create: upload did not complete");
     }
+    st = fastdiv_setup(device, p->dh, &m->fastdiv, &m->rdh);
+    if (st) {
+        dn_model_destroy(m);
+        return st;
+    }
     *out = m;
     return DN_OK;
 }
@@ -387,10 +450,9 @@ static void tile_shape(const dn_params *p, int &bx, int &zch)
 {
     // Tile shapes measured on B200 per grid; small grids favour short tiles
     // (more CTAs), large ones long register streams.
+    (void)p;
     bx = 128;
-    long long cells = (long long)p->nx * p->ny;
     zch = 8;   // measured best on B200 for the 2000 x 600 batched workload (4-32 swept)
-    (void)cells;
     const char *ev = getenv("DN_TILE");
     if (ev) {
         int a = 0, b = 0;
@@ -650,6 +712,8 @@ static Inst make_inst(const dn_shot *s, int mode)
     I.seismo = p.seismo;
     I.DT = p.dt;
     I.DH = p.dh;
+    I.rdh = m->rdh;
+    I.fastdiv = m->fastdiv;
     I.dhi_el = p.dt / p.dh;
     I.dhi_vi = 1.0 / p.dh;
     I.dh1 = 1.0 / p.dh;
@@ -751,117 +815,8 @@ static Inst make_inst(const dn_shot *s, int mode)
 }
 
 // ---------------------------------------------------------------------------
-// kernel dispatch
+// kernel dispatch (per-order launch functions in dn_launch_impl.cuh)
 // ---------------------------------------------------------------------------
-struct LaunchCfg {
-    dim3 tile_grid, src_grid, surf_grid, rec_grid;
-    int bx;
-    int R, L;
-    bool exact;
-    bool tma;   // stencil kernels fed by the bulk-copy row pipeline
-    bool any_surf, any_src_s, any_store, any_adj, any_rec;
-};
-
-// marks (optional, profiling only): 9 events recorded around the 8 kernel slots
-// v, inject_v, s, inject_s, surface, seismo, snap, correlate
-#define MARK(k)                                                                                    \
-    do {                                                                                           \
-        if (marks) cudaEventRecord(marks[k], st);                                                  \
-    } while (0)
-
-template <int R, bool X>
-static void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int *ntb, int off, long long &nl,
-                          cudaEvent_t *marks)
-{
-    MARK(0);
-    if (c.tma) k_update_v_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QV>(slot_floats_v()), st>>>(d, ntb, off);
-    else k_update_v<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
-    MARK(1);
-    k_inject_v<<<c.src_grid, 128, 0, st>>>(d, ntb, off);
-    MARK(2);
-    nl += 2;
-    if (c.L == 0) {
-        if (c.tma)
-            k_update_s_el_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QS_EL>(slot_floats_s_el()), st>>>(d, ntb, off);
-        else k_update_s_el<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
-    } else if (c.tma) {
-#define DN_VI_TMA(LL)                                                                                          \
-    k_update_s_vi_tma<R, LL, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QS_VI>(slot_floats_s_vi(LL)), st>>>(d, ntb, off)
-        switch (c.L) {
-        case 1: DN_VI_TMA(1); break;
-        case 2: DN_VI_TMA(2); break;
-        case 3: DN_VI_TMA(3); break;
-        case 4: DN_VI_TMA(4); break;
-        default: DN_VI_TMA(5); break;
-        }
-#undef DN_VI_TMA
-    } else {
-        switch (c.L) {
-        case 1: k_update_s_vi<R, 1, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
-        case 2: k_update_s_vi<R, 2, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
-        case 3: k_update_s_vi<R, 3, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
-        case 4: k_update_s_vi<R, 4, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
-        default: k_update_s_vi<R, 5, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
-        }
-    }
-    nl++;
-    MARK(3);
-    if (c.any_src_s) {
-        k_inject_s<<<c.src_grid, 128, 0, st>>>(d, ntb, off);
-        nl++;
-    }
-    MARK(4);
-    if (c.any_surf) {
-        if (c.L == 0) {
-            k_surface_el<R, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off);
-        } else {
-            switch (c.L) {
-            case 1: k_surface_vi<R, 1, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off); break;
-            case 2: k_surface_vi<R, 2, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off); break;
-            case 3: k_surface_vi<R, 3, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off); break;
-            case 4: k_surface_vi<R, 4, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off); break;
-            default: k_surface_vi<R, 5, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off); break;
-            }
-        }
-        nl++;
-    }
-    MARK(5);
-    k_seismo<R><<<c.rec_grid, 128, 0, st>>>(d, ntb, off);
-    nl++;
-    MARK(6);
-    if (c.any_store) {
-        k_snap_store<<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
-        nl++;
-    }
-    MARK(7);
-    if (c.any_adj) {
-        k_correlate<<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
-        nl++;
-    }
-    MARK(8);
-}
-
-// opt the pipelined kernels into their dynamic shared memory (needed above 48 KB)
-template <int R, bool X>
-static int set_smem_attrs_R()
-{
-    cudaFuncSetAttribute(k_update_v_tma<R, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)pipe_smem_bytes<QV>(slot_floats_v()));
-    cudaFuncSetAttribute(k_update_s_el_tma<R, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)pipe_smem_bytes<QS_EL>(slot_floats_s_el()));
-    cudaFuncSetAttribute(k_update_s_vi_tma<R, 1, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)pipe_smem_bytes<QS_VI>(slot_floats_s_vi(1)));
-    cudaFuncSetAttribute(k_update_s_vi_tma<R, 2, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)pipe_smem_bytes<QS_VI>(slot_floats_s_vi(2)));
-    cudaFuncSetAttribute(k_update_s_vi_tma<R, 3, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)pipe_smem_bytes<QS_VI>(slot_floats_s_vi(3)));
-    cudaFuncSetAttribute(k_update_s_vi_tma<R, 4, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)pipe_smem_bytes<QS_VI>(slot_floats_s_vi(4)));
-    cudaError_t e = cudaFuncSetAttribute(k_update_s_vi_tma<R, 5, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)pipe_smem_bytes<QS_VI>(slot_floats_s_vi(5)));
-    return e == cudaSuccess ? 0 : -1;
-}
-
 template <bool X>
 static int set_smem_attrs_X(int R)
 {
@@ -955,7 +910,10 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c)
     c.bx = shots[0]->bx;
     // stencil kernels: register streaming (default, fastest measured on B200) or, with
     // DN_KERNEL=tma, the bulk-copy row pipeline of dn_kernels_tma.cuh
-    c.tma = c.bx == TMA_W && getenv("DN_KERNEL") && strcmp(getenv("DN_KERNEL"), "tma") == 0;
+    // stencil kernels: register streaming (default, fastest measured on B200) or, with
+    // DN_KERNEL=tma, the bulk-copy row pipeline of dn_kernels_tma.cuh
+    const char *kern = getenv("DN_KERNEL");
+    c.tma = c.bx == TMA_W && kern && strcmp(kern, "tma") == 0;
     c.any_surf = c.any_src_s = c.any_store = c.any_adj = c.any_rec = false;
     int maxtiles = 0, maxsrc = 1, maxnx = 1, maxtr = 1;
     for (int k = 0; k < n; k++) {

@@ -80,6 +80,8 @@ struct Inst {
     float *Ws, *Wr;
     // status
     int *flag;                        // bit 0: NaN seen at the psv.c:99 probe
+    float rdh;                        // RN(1 / DH)
+    int fastdiv;                      // division by DH through div_markstein (verified for this DH)
 };
 
 // ---------------------------------------------------------------------------
@@ -94,6 +96,42 @@ __device__ __forceinline__ double DADD(double a, double b) { return __dadd_rn(a,
 __device__ __forceinline__ double DSUB(double a, double b) { return __dadd_rn(a, -b); }
 __device__ __forceinline__ double DDIV(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ float F(double a) { return __double2float_rn(a); }
+
+// ---------------------------------------------------------------------------
+// Division by the grid spacing DH without the general division routine.
+// Markstein's correction step (P. W. Markstein, "Computation of elementary
+// functions on the IBM RISC System/6000 processor", IBM J. Res. Develop.
+// 34(1), 1990): with y = RN(1/d), q = RN(a y) and the exact residual
+// r = fma(-q, d, a), RN(q + r y) is the correctly rounded a / d while no
+// intermediate leaves the normal range.  Dividends outside [2^-100, 2^100]
+// (zeros, subnormals, huge values, inf, NaN) take __fdiv_rn; a zero dividend
+// returns q = a y, which carries the sign of a.  The host enables this path
+// for a DH only after comparing it with __fdiv_rn on all 2^32 dividends
+// (k_fastdiv_check), so the result is bit-identical to a / DH.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float div_markstein(float a, float d, float y)
+{
+    const float q = __fmul_rn(a, y);
+    const float r = __fmaf_rn(-q, d, a);
+    const float q1 = __fmaf_rn(r, y, q);
+    const float aa = fabsf(a);
+    if (aa >= 0x1p-100f && aa <= 0x1p100f) return q1;
+    if (a == 0.0f) return q;
+    return __fdiv_rn(a, d);
+}
+template <bool X>
+__device__ __forceinline__ float DIVH(float a, const Inst &I)
+{
+    if (!X) return a * I.rdh;
+    return I.fastdiv ? div_markstein(a, I.DH, I.rdh) : __fdiv_rn(a, I.DH);
+}
+// Division by a CPML K coefficient: K = 1 (k_max_PML = 1) divides exactly,
+// a / 1 = a in IEEE arithmetic, so only K != 1 needs the division.
+template <bool X>
+__device__ __forceinline__ float DIVK(float a, float k)
+{
+    return k == 1.0f ? a : DIV<X>(a, k);
+}
 
 // ---------------------------------------------------------------------------
 // tile location
@@ -118,9 +156,13 @@ __device__ __forceinline__ bool tile_of(const Inst &I, TileLoc &t)
 // mode 1: vxp1 += DT * vx with the old vx (:455-457).
 // Each thread streams down its column; the loads of row j+1 are issued before
 // row j is computed so two rows of DRAM traffic are in flight per thread.
+// The register caps of the stencil kernels (velocity 48, elastic stress 64,
+// viscoelastic stress 80 registers at FDORDER 8, no spills) were measured
+// faster than the uncapped 74 / 73 / 120: the kernels are bound by the loads
+// in flight per SM, so resident warps count more than registers per thread.
 // ===========================================================================
 template <int R, bool X>
-__global__ void __launch_bounds__(256) k_update_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+__global__ void __launch_bounds__(256, 5) k_update_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
@@ -141,7 +183,7 @@ __global__ void __launch_bounds__(256) k_update_v(const Inst *__restrict__ insts
     float hc[R + 1];
 #pragma unroll
     for (int m = 1; m <= R; m++) hc[m] = I.hc[m];
-    const float DT = I.DT, DH = I.DH;
+    const float DT = I.DT;
     const int mode = I.mode;
     const bool snapstep = (mode == 0) && I.store && ((nt - 1) % I.dtinv == 0);
     const int fw = I.fw, nx = I.nx, ny = I.ny, free_surf = I.free_surf;
@@ -203,11 +245,11 @@ __global__ void __launch_bounds__(256) k_update_v(const Inst *__restrict__ insts
                 float *ps = I.psi_sxx_x + (long long)(j - 1) * 2 * fw + h;
                 float v = ADD<X>(MUL<X>(I.b_xh[h], *ps), MUL<X>(I.a_xh[h], sxx_x));
                 *ps = v;
-                sxx_x = ADD<X>(DIV<X>(sxx_x, I.K_xh[h]), v);
+                sxx_x = ADD<X>(DIVK<X>(sxx_x, I.K_xh[h]), v);
                 float *pq = I.psi_sxy_x + (long long)(j - 1) * 2 * fw + h;
                 float w = ADD<X>(MUL<X>(I.b_x[h], *pq), MUL<X>(I.a_x[h], sxy_x));
                 *pq = w;
-                sxy_x = ADD<X>(DIV<X>(sxy_x, I.K_x[h]), w);
+                sxy_x = ADD<X>(DIVK<X>(sxy_x, I.K_x[h]), w);
             }
         }
         if (fw > 0 && ((!free_surf && j <= fw) || j >= ny - fw + 1)) {
@@ -217,25 +259,25 @@ __global__ void __launch_bounds__(256) k_update_v(const Inst *__restrict__ insts
                 float *ps = I.psi_syy_y + (long long)h * nx + (i - 1);
                 float v = ADD<X>(MUL<X>(I.b_yh[h], *ps), MUL<X>(I.a_yh[h], syy_y));
                 *ps = v;
-                syy_y = ADD<X>(DIV<X>(syy_y, I.K_yh[h]), v);
+                syy_y = ADD<X>(DIVK<X>(syy_y, I.K_yh[h]), v);
                 float *pq = I.psi_sxy_y + (long long)h * nx + (i - 1);
                 float w = ADD<X>(MUL<X>(I.b_y[h], *pq), MUL<X>(I.a_y[h], sxy_y));
                 *pq = w;
-                sxy_y = ADD<X>(DIV<X>(sxy_y, I.K_y[h]), w);
+                sxy_y = ADD<X>(DIVK<X>(sxy_y, I.K_y[h]), w);
             }
         }
         const long long o = (long long)j * P;
         const float s1 = ADD<X>(sxx_x, sxy_y);
         const float s2 = ADD<X>(sxy_x, syy_y);
         if (snapstep) {
-            vxp1[o] = DIV<X>(MUL<X>(ripv, s1), DH);
-            vyp1[o] = DIV<X>(MUL<X>(rjpv, s2), DH);
+            vxp1[o] = DIVH<X>(MUL<X>(ripv, s1), I);
+            vyp1[o] = DIVH<X>(MUL<X>(rjpv, s2), I);
         } else if (mode == 1) {
             vxp1[o] = ADD<X>(vxp1[o], MUL<X>(DT, vxo));
             vyp1[o] = ADD<X>(vyp1[o], MUL<X>(DT, vyo));
         }
-        vx[o] = ADD<X>(vxo, DIV<X>(MUL<X>(MUL<X>(DT, ripv), s1), DH));
-        vy[o] = ADD<X>(vyo, DIV<X>(MUL<X>(MUL<X>(DT, rjpv), s2), DH));
+        vx[o] = ADD<X>(vxo, DIVH<X>(MUL<X>(MUL<X>(DT, ripv), s1), I));
+        vy[o] = ADD<X>(vyo, DIVH<X>(MUL<X>(MUL<X>(DT, rjpv), s2), I));
 #pragma unroll
         for (int k = 0; k < 2 * R - 1; k++) {
             wyy[k] = wyy[k + 1];
@@ -249,7 +291,7 @@ __global__ void __launch_bounds__(256) k_update_v(const Inst *__restrict__ insts
 // (:755-768).  One thread per unique source cell; sources sharing a cell are
 // added in their list order, as the reference's sequential loop does.
 // ===========================================================================
-__global__ void k_inject_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+static __global__ void k_inject_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
@@ -369,11 +411,11 @@ struct VDeriv {
                 float *p1 = I.psi_vxx + (long long)(j - 1) * 2 * fw + h;
                 float v = ADD<X>(MUL<X>(I.b_x[h], *p1), MUL<X>(I.a_x[h], vxx));
                 *p1 = v;
-                vxx = ADD<X>(DIV<X>(vxx, I.K_x[h]), v);
+                vxx = ADD<X>(DIVK<X>(vxx, I.K_x[h]), v);
                 float *p2 = I.psi_vyx + (long long)(j - 1) * 2 * fw + h;
                 float w = ADD<X>(MUL<X>(I.b_xh[h], *p2), MUL<X>(I.a_xh[h], vyx));
                 *p2 = w;
-                vyx = ADD<X>(DIV<X>(vyx, I.K_xh[h]), w);
+                vyx = ADD<X>(DIVK<X>(vyx, I.K_xh[h]), w);
             }
         }
         if (fw > 0 && ((!I.free_surf && j <= fw) || j >= ny - fw + 1)) {
@@ -386,8 +428,8 @@ struct VDeriv {
                 float w = ADD<X>(MUL<X>(I.b_yh[h], *p2), MUL<X>(I.a_yh[h], vxy));
                 *p1 = v;
                 *p2 = w;
-                vyy = ADD<X>(DIV<X>(vyy, I.K_y[h]), v);
-                vxy = ADD<X>(DIV<X>(vxy, I.K_yh[h]), w);
+                vyy = ADD<X>(DIVK<X>(vyy, I.K_y[h]), v);
+                vxy = ADD<X>(DIVK<X>(vxy, I.K_yh[h]), w);
             }
         }
     }
@@ -399,7 +441,7 @@ struct VDeriv {
 // (:442-444) and the double-promoted 2.0*f*vxx terms (:454-456).
 // ===========================================================================
 template <int R, bool X>
-__global__ void __launch_bounds__(256) k_update_s_el(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+__global__ void __launch_bounds__(256, 4) k_update_s_el(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
@@ -457,7 +499,7 @@ __global__ void __launch_bounds__(256) k_update_s_el(const Inst *__restrict__ in
 // factors exactly as prepare_update_s_visc_PSV.c:52-62 forms them.
 // ===========================================================================
 template <int R, int L, bool X>
-__global__ void __launch_bounds__(256) k_update_s_vi(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+__global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
@@ -577,7 +619,7 @@ __global__ void __launch_bounds__(256) k_update_s_vi(const Inst *__restrict__ in
 // pressure source psource.c:41-53 (mode 1, QUELLTYPB >= 4) and the moment
 // tensor source msource.c:27-41 (QUELLTYP == 5, forward modes).
 // ===========================================================================
-__global__ void k_inject_s(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+static __global__ void k_inject_s(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
@@ -668,14 +710,14 @@ __global__ void k_surface_el(const Inst *__restrict__ insts, const int *__restri
             float *ps = I.psi_vxxs + (long long)(j - 1) * 2 * fw + h;
             float v = ADD<X>(MUL<X>(I.b_x[h], *ps), MUL<X>(I.a_x[h], vxx));
             *ps = v;
-            vxx = ADD<X>(DIV<X>(vxx, I.K_x[h]), v);
+            vxx = ADD<X>(DIVK<X>(vxx, I.K_x[h]), v);
         }
         if (i >= nx - fw + 1) {
             const int h = i - nx + 2 * fw - 1;
             float *ps = I.psi_vxxs + (long long)(j - 1) * 2 * fw + h;
             float v = ADD<X>(MUL<X>(I.b_x[h], *ps), MUL<X>(I.a_x[h], vxx));
             *ps = v;
-            vxx = ADD<X>(DIV<X>(vxx, I.K_x[h]), v);
+            vxx = ADD<X>(DIVK<X>(vxx, I.K_x[h]), v);
         }
     }
     const float g = I.lam[o];
@@ -720,14 +762,14 @@ __global__ void k_surface_vi(const Inst *__restrict__ insts, const int *__restri
             float *ps = I.psi_vxxs + (long long)(j - 1) * 2 * fw + h;
             float v = ADD<X>(MUL<X>(I.b_x[h], *ps), MUL<X>(I.a_x[h], vxx));
             *ps = v;
-            vxx = ADD<X>(DIV<X>(vxx, I.K_x[h]), v);
+            vxx = ADD<X>(DIVK<X>(vxx, I.K_x[h]), v);
         }
         if (i >= nx - fw + 1) {
             const int h = i - nx + 2 * fw - 1;
             float *ps = I.psi_vxxs + (long long)(j - 1) * 2 * fw + h;
             float v = ADD<X>(MUL<X>(I.b_x[h], *ps), MUL<X>(I.a_x[h], vxx));
             *ps = v;
-            vxx = ADD<X>(DIV<X>(vxx, I.K_x[h]), v);
+            vxx = ADD<X>(DIVK<X>(vxx, I.K_x[h]), v);
         }
     }
     const float mu = I.s_mu[i - 1], pi = I.s_pi[i - 1], taus = I.s_taus[i - 1], taup = I.s_taup[i - 1];
@@ -844,7 +886,7 @@ __device__ __forceinline__ float pow2_scale(float amax)
     return ldexpf(1.0f, e - 15);
 }
 
-__global__ void k_snap_store(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+static __global__ void k_snap_store(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
@@ -910,7 +952,7 @@ __device__ __forceinline__ float snap_load(const Inst &I, long long slot, long l
 // Adjoint cross-correlation, psv.c:313-387 (GRAD_FORM 1, INVMAT1 1), at the
 // adjoint steps whose mirrored forward step NT-nt+1 stored a snapshot.
 // ===========================================================================
-__global__ void k_correlate(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+static __global__ void k_correlate(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];

@@ -1,0 +1,35 @@
+// Launch of one time step of a batch: the kernel sequence of psv() for the
+// configured stencil kernels.  The per-order launch functions are compiled in
+// separate translation units (dn_launch_r1.cu .. dn_launch_r6.cu) so that the
+// many kernel instantiations build in parallel.
+#pragma once
+
+#include "dn_kernels_tma.cuh"
+
+namespace dn {
+
+struct LaunchCfg {
+    dim3 tile_grid, src_grid, surf_grid, rec_grid;
+    int bx;
+    int R, L;
+    bool exact;
+    bool tma;   // stencil kernels fed by the bulk-copy row pipeline
+    bool any_surf, any_src_s, any_store, any_adj, any_rec;
+};
+
+// marks (optional, profiling only): 9 events recorded around the 8 kernel slots
+// v, inject_v, s, inject_s, surface, seismo, snap, correlate
+#define MARK(k)                                                                                    \
+    do {                                                                                           \
+        if (marks) cudaEventRecord(marks[k], st);                                                  \
+    } while (0)
+
+
+template <int R, bool X>
+void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int *ntb, int off, long long &nl,
+                   cudaEvent_t *marks);
+// opts the bulk-copy pipeline kernels of order R into their dynamic shared memory
+template <int R, bool X>
+int set_smem_attrs_R();
+
+}   // namespace dn
