@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--plain-shots", type=int, default=4)
     ap.add_argument("--cpu-sample-nt", type=int, default=60)
+    ap.add_argument("--elastic-nt", type=int, default=1000,
+                    help="NT of the elastic batch measured beside the viscoelastic one (0: skip)")
     return ap.parse_args()
 
 
@@ -133,6 +135,15 @@ class ClockSampler:
         reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
+
+
+def traffic_per_cell(kernel):
+    """DRAM bytes per cell of one launch from the committed ncu capture (profiles/traffic.json)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return float(json.load(f)[kernel]["dram_bytes_per_cell"])
+    except Exception:
+        return None
 
 
 def measured_peak():
@@ -236,9 +247,12 @@ def run_ours(a, rank, world, local_rank):
         achieved = s_bytes / (prof["update_s"] * 1e-3) / 1e9
         step_bytes = (23 + 6 * p.L) * 4 * cells
         step_ms = sum(prof.values())
+        tpc = traffic_per_cell("k_update_s_vi<4,3>")
         roof = {"bound": "hbm", "kernel": "k_update_s_vi<4,3,true> (viscoelastic stress update)",
                 "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "peak_kind": peak_kind, "traffic": None,
+                "peak_kind": peak_kind + " (burst copy bandwidth)",
+                "traffic": round(tpc * cells) if tpc else None,
+                "traffic_note": "ncu dram bytes per cell of a 4-shot capture, scaled to this launch's cells",
                 "algorithmic_bytes_per_launch": s_bytes,
                 "v_kernel_gbs": round(v_bytes / (prof["update_v"] * 1e-3) / 1e9, 1),
                 "whole_step_gbs_direct": round(step_bytes / (step_ms * 1e-3) / 1e9, 1),
@@ -252,6 +266,9 @@ def run_ours(a, rank, world, local_rank):
             tp += dn.last_run_stats()[0] / 1e3
         plain_sps = len(plain_shots) / tp
         batched_sps = a.shots * a.steps / t_dev
+        elastic = None
+        if a.elastic_nt > 0:
+            elastic = run_elastic(a, inputs, device, peak)
         e2e = None
         if not a.no_e2e:
             e2e = run_e2e(p, inputs, device, cells_step)
@@ -273,6 +290,8 @@ def run_ours(a, rank, world, local_rank):
             "clocks": clk.summary(),
             "wall_s_timed": round(wall, 3),
         }
+        if elastic:
+            result["elastic"] = elastic
         if e2e:
             result["e2e"] = e2e
         if cpu:
@@ -284,6 +303,42 @@ def run_ours(a, rank, world, local_rank):
         dist.barrier()
         dist.destroy_process_group()
     return result
+
+
+def run_elastic(a, inputs, device, peak):
+    """The same shots with the elastic propagator (vp, vs, rho of each model, L = 0) at NT = a.elastic_nt:
+    device time of the batched run, and the elastic step's per-kernel roofline."""
+    import denise_b200 as dn
+    import torch
+    from denise_b200 import synth
+
+    p = synth.c1_params(nx=a.nx, ny=a.ny, nt=a.elastic_nt, L=0, fl=())
+    sig = synth.ricker_source(p, 8.0)[None, :]
+    pairs = []
+    for model, src, rec in inputs:
+        m = dn.Model(p, *model[:3], device=device)
+        pairs.append((m, dn.Shot(m, src[0], src[1], sig, rec[0], rec[1])))
+    shots = [s for _, s in pairs]
+    dn.run(shots)
+    torch.cuda.synchronize(device)
+    ms = 0.0
+    for _ in range(2):
+        dn.run(shots)
+        ms += dn.last_run_stats()[0]
+    ms /= 2
+    cells = len(shots) * p.nx * p.ny
+    prof = dn.api.profile_steps(shots, dn.MODE_FORWARD, nsteps=20)
+    step_ms = sum(prof.values())
+    out = {"value": round(cells * p.nt / (ms * 1e-3) / 1e6, 1), "unit": UNIT, "shots": len(shots), "nt": p.nt,
+           "ms_per_run": round(ms, 2),
+           "v_kernel_gbs": round(36 * cells / (prof["update_v"] * 1e-3) / 1e9, 1),
+           "s_kernel_gbs": round(44 * cells / (prof["update_s"] * 1e-3) / 1e9, 1),
+           "whole_step_gbs_direct": round(80 * cells / (step_ms * 1e-3) / 1e9, 1)}
+    out["whole_step_frac"] = round(out["whole_step_gbs_direct"] / peak, 4)
+    for m, s in pairs:
+        s.close()
+        m.close()
+    return out
 
 
 def run_e2e(p, inputs, device, cells_step):
