@@ -61,6 +61,18 @@ extern "C" int dn_device_count(int *count)
     return DN_OK;
 }
 
+extern "C" int dn_device_memory(int device, size_t *free_bytes, size_t *total_bytes)
+{
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+    size_t f = 0, t = 0;
+    e = cudaMemGetInfo(&f, &t);
+    if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "cudaMemGetInfo: %s", cudaGetErrorString(e));
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
+    return DN_OK;
+}
+
 // ---------------------------------------------------------------------------
 // per-device state: one stream, a zero step counter for direct launches
 // ---------------------------------------------------------------------------

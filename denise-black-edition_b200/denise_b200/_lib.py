@@ -125,6 +125,21 @@ SIGNATURES = {
     "dn_residual_l2": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
                                       _c_double_p]),
     "dn_shot_residual": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p, _c_double_p]),
+    "dn_device_memory": (ctypes.c_int, [ctypes.c_int, _P(ctypes.c_size_t), _P(ctypes.c_size_t)]),
+    "dn_inp_read": (ctypes.c_int, [ctypes.c_char_p, _vp]),
+    "dn_inp_nt": (ctypes.c_int, [_vp]),
+    "dn_inp_params": (ctypes.c_int, [_vp, ctypes.c_float, _P(Params)]),
+    "dn_read_model_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _c_float_p]),
+    "dn_read_sources": (ctypes.c_int, [ctypes.c_char_p, _P(ctypes.c_int), _P(_c_float_p), _P(ctypes.c_float)]),
+    "dn_source_cell": (ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.c_float, _P(ctypes.c_int),
+                                      _P(ctypes.c_int)]),
+    "dn_read_receivers": (ctypes.c_int, [ctypes.c_char_p, _c_float_p, ctypes.c_float, _P(ctypes.c_int),
+                                         _P(_P(ctypes.c_int)), _P(_P(ctypes.c_int))]),
+    "dn_write_su": (ctypes.c_int, [ctypes.c_char_p, _c_float_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_float, ctypes.c_float, ctypes.c_float, _P(ctypes.c_int),
+                                   _P(ctypes.c_int), _c_float_p, ctypes.c_float, ctypes.c_float]),
+    "dn_read_su": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _c_float_p]),
+    "dn_forward_inp": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "dn_residual_l2_noalloc": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                               ctypes.c_int, _c_double_p]),
 }

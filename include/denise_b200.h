@@ -148,6 +148,8 @@ typedef struct dn_shot dn_shot;     /* device-resident wavefield state of one sh
 const char *dn_last_error(void);      /* thread-local text of the last failure */
 int dn_version(int *major, int *minor);
 int dn_device_count(int *count);
+/* Free and total memory of a device (cudaMemGetInfo with that device current). */
+int dn_device_memory(int device, size_t *free_bytes, size_t *total_bytes);
 
 /* ---- host set-up numerics (bit-identical to the reference) ----------------- */
 /* holbergcoeff(): src/holbergcoeff.c:19-90; hc[0..6] */

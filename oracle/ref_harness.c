@@ -343,3 +343,105 @@ int refh_wavelet(int quellart, int n_order, float tshift, float fc, float amp, f
     N_ORDER = 0;
     return 0;
 }
+
+/* ---- host I/O of the reference --------------------------------------------- */
+extern char SOURCE_FILE[STRING_SIZE], REC_FILE[STRING_SIZE];
+extern float REFREC[4];
+extern int SRCREC, READREC, SEIS_FORMAT;
+
+static FILE *null_log(void)
+{
+    static FILE *f = NULL;
+    if (!f) f = fopen("/dev/null", "w");
+    return f;
+}
+
+/* read_par() on a parameter file; exports the globals the path reads:
+ * iv[0..15] = MODE PHYSICS NPROCX NPROCY FDORDER MAXRELERROR NX NY QUELLART SRCREC
+ *             RUN_MULTIPLE_SHOTS L FREE_SURF FW BOUNDARY SEISMO
+ * iv[16..21] = READREC NDT SEIS_FORMAT INVMAT1 GRAD_FORM QUELLTYPB, iv[22] = DTINV
+ * fv[0..12] = DH TIME DT TS DAMPING FPML npower k_max_PML REFREC[1] REFREC[2] FL[1] FL[2] FL[3]
+ * strs: 8 x 74 chars: SOURCE_FILE REC_FILE MFILE SEIS_FILE_VX SEIS_FILE_VY SEIS_FILE_P SIGNAL_FILE JACOBIAN */
+extern int RUN_MULTIPLE_SHOTS, BOUNDARY, INVMAT1;
+extern char SEIS_FILE_VX[STRING_SIZE], SEIS_FILE_VY[STRING_SIZE], SEIS_FILE_P[STRING_SIZE], SIGNAL_FILE[STRING_SIZE],
+    JACOBIAN[STRING_SIZE];
+int refh_read_par(const char *path, int *iv, float *fv, char *strs)
+{
+    FILE *f = fopen(path, "r");
+    if (!f) return -1;
+    if (!FL) FL = vector(1, 8);
+    read_par(f);   /* closes f */
+    const int I[23] = {MODE, PHYSICS, NPROCX, NPROCY, FDORDER, MAXRELERROR, NX, NY, QUELLART, SRCREC,
+                       RUN_MULTIPLE_SHOTS, L, FREE_SURF, FW, BOUNDARY, SEISMO, READREC, NDT, SEIS_FORMAT,
+                       INVMAT1, GRAD_FORM, QUELLTYPB, DTINV};
+    for (int k = 0; k < 23; k++) iv[k] = I[k];
+    const float F[10] = {DH, TIME, DT, TS, DAMPING, FPML, npower, k_max_PML, REFREC[1], REFREC[2]};
+    for (int k = 0; k < 10; k++) fv[k] = F[k];
+    for (int l = 1; l <= 3; l++) fv[9 + l] = l <= L ? FL[l] : 0.0f;
+    const char *S[8] = {SOURCE_FILE, REC_FILE, MFILE, SEIS_FILE_VX, SEIS_FILE_VY, SEIS_FILE_P, SIGNAL_FILE, JACOBIAN};
+    for (int k = 0; k < 8; k++) {
+        strncpy(strs + 74 * k, S[k], 73);
+        strs[74 * k + 73] = 0;
+    }
+    return 0;
+}
+
+/* sources() on a source file: srcpos[8][n] flattened as srcpos[l*8 + r-1], TS */
+int refh_sources(const char *path, int *nsrc, float *srcpos, int cap, float *ts)
+{
+    FP = null_log();
+    strncpy(SOURCE_FILE, path, STRING_SIZE - 1);
+    SRCREC = 1;
+    float **sp = sources(nsrc);
+    for (int l = 1; l <= *nsrc && l <= cap; l++)
+        for (int r = 1; r <= 8; r++) srcpos[(l - 1) * 8 + r - 1] = sp[r][l];
+    *ts = TS;
+    return 0;
+}
+
+/* receiver() with READREC = 1 on <base>.dat */
+int refh_receivers(const char *base, float refx, float refy, float dh, int *ntr, int *ri, int *rj, int cap)
+{
+    strncpy(REC_FILE, base, STRING_SIZE - 1);
+    READREC = 1;
+    REFREC[1] = refx;
+    REFREC[2] = refy;
+    REFREC[3] = 0.0f;
+    DH = dh;
+    int **rp = receiver(null_log(), ntr, 1);
+    for (int k = 1; k <= *ntr && k <= cap; k++) {
+        ri[k - 1] = rp[1][k];
+        rj[k - 1] = rp[2][k];
+    }
+    return 0;
+}
+
+/* outseis_glob() SEIS_FORMAT 1 of a section [ntr][ns] (ns = NT samples) */
+int refh_outseis(const char *path, const float *section, int ntr, int ns, const int *ri, const int *rj, float xs,
+                 float ys, int ndt, float time, float dt, float dh, float refx, float refy)
+{
+    float **sec = matrix(1, ntr, 1, ns);
+    int **rp = imatrix(1, 3, 1, ntr);
+    float **sp = matrix(1, 8, 1, 1);
+    for (int k = 1; k <= ntr; k++) {
+        for (int t = 1; t <= ns; t++) sec[k][t] = section[(size_t)(k - 1) * ns + t - 1];
+        rp[1][k] = ri[k - 1];
+        rp[2][k] = rj[k - 1];
+        rp[3][k] = 0;
+    }
+    sp[1][1] = xs;
+    sp[2][1] = ys;
+    NDT = ndt;
+    TIME = time;
+    DT = dt;
+    DH = dh;
+    REFREC[1] = refx;
+    REFREC[2] = refy;
+    FILE *f = fopen(path, "w");
+    if (!f) return -1;
+    outseis_glob(null_log(), f, 1, sec, rp, rp, ntr, sp, 1, ns, 1, 1, 1);
+    free_matrix(sec, 1, ntr, 1, ns);
+    free_imatrix(rp, 1, 3, 1, ntr);
+    free_matrix(sp, 1, 8, 1, 1);
+    return 0;
+}

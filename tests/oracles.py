@@ -213,13 +213,15 @@ class Reference:
         return tuple(g)
 
 
-def run_isolated(fn, *args):
-    """Runs fn(*args) in a fresh spawned process (the reference keeps globals)."""
+def run_isolated(fn, *args, timeout=600):
+    """Runs fn(*args) in a fresh spawned process (the reference keeps globals).
+    A reference error exits that process (its err() calls exit); that surfaces
+    here as BrokenProcessPool instead of a wait without end."""
     import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
 
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(1) as pool:
-        return pool.apply(fn, args)
+    with ProcessPoolExecutor(max_workers=1, mp_context=mp.get_context("spawn")) as ex:
+        return ex.submit(fn, *args).result(timeout=timeout)
 
 
 def rel_l2(a, b):

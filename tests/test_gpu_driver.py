@@ -1,0 +1,88 @@
+"""The forward-modelling driver end to end: a parameter file, its model,
+source and receiver files run by the reference's own program (oracle/_ref/denise,
+CPU) and by this library (dn_forward_inp and the denise_b200 command, GPU); the
+SU files must agree byte for byte: every trace's 210 header bytes the reference
+assigns and every sample (the propagation is bit-exact)."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracles as O
+import inp_case
+from denise_b200 import io
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "denise-black-edition_b200", "bin", "denise_b200")
+
+CASES = {
+    "elastic-fd8-fs": dict(),
+    "visco-l3-fd4": dict(L=3, FDORDER=4),
+    "elastic-all-components-ndt2": dict(SEISMO=4, NDT=2, FREE_SURF=0, FDORDER=6),
+    "one-shot-all-sources": dict(RUN_MULTIPLE_SHOTS=0, nshots=2),
+    "rotated-force-sources": dict(src_type=4),
+}
+
+
+def _su_equal(a_path, b_path, ntr):
+    a = np.fromfile(a_path, np.uint8)
+    b = np.fromfile(b_path, np.uint8)
+    assert a.size == b.size, (a_path, a.size, b.size)
+    per = a.size // ntr
+    for k in range(ntr):
+        o = k * per
+        np.testing.assert_array_equal(a[o:o + 210], b[o:o + 210], err_msg=f"{a_path} header {k}")
+        np.testing.assert_array_equal(a[o + 240:o + per], b[o + 240:o + per], err_msg=f"{a_path} trace {k}")
+
+
+def _make(root, kw):
+    kw = dict(kw)
+    nshots = kw.pop("nshots", 3)
+    styp = kw.pop("src_type", 1)
+    inp = inp_case.write_case(root, nshots=nshots, **kw)
+    if styp != 1:
+        path = os.path.join(root, "source", "sources.dat")
+        lines = open(path).read().splitlines()
+        out = [lines[0]]
+        for k, ln in enumerate(lines[1:]):
+            c = ln.split("\t")
+            c[6] = f"{30.0 + 20 * k:.2f}"
+            c[7] = str(styp)
+            out.append("\t".join(c))
+        open(path, "w").write("\n".join(out) + "\n")
+    return inp
+
+
+@pytest.mark.skipif(not os.path.exists(O.REF_BIN), reason="reference program not built")
+@pytest.mark.parametrize("name", list(CASES))
+def test_driver_matches_reference_program(tmp_path, name):
+    ref_dir, our_dir, cli_dir = (str(tmp_path / d) for d in ("ref", "ours", "cli"))
+    for d in (ref_dir, our_dir, cli_dir):
+        os.makedirs(d)
+    _make(ref_dir, CASES[name])
+    for d in (our_dir, cli_dir):
+        shutil.rmtree(d)
+        shutil.copytree(ref_dir, d)
+    r = subprocess.run([O.REF_BIN, "case.inp"], cwd=ref_dir, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    cwd = os.getcwd()
+    try:
+        os.chdir(our_dir)
+        io.forward_inp("case.inp", 0)
+    finally:
+        os.chdir(cwd)
+    r = subprocess.run([CLI, "case.inp"], cwd=cli_dir, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    ref_files = sorted(f for f in os.listdir(os.path.join(ref_dir, "su")) if ".shot" in f)
+    assert ref_files
+    inp = io.read_inp(os.path.join(ref_dir, "case.inp"))
+    ri, _ = io.read_receivers(os.path.join(ref_dir, "receiver", "receivers.dat"), inp.refrec, inp.dh)
+    for f in ref_files:
+        for d in (our_dir, cli_dir):
+            _su_equal(os.path.join(d, "su", f), os.path.join(ref_dir, "su", f), len(ri))
+    ours = sorted(f for f in os.listdir(os.path.join(our_dir, "su")) if ".shot" in f)
+    assert ours == ref_files
