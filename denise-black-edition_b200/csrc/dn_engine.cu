@@ -911,17 +911,16 @@ static void forget_shot(const dn_shot *s)
     }
 }
 
-static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c)
+// modes: per-shot modes of a mixed batch (a run queue), or null: every shot runs `mode`
+static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c, const int *modes = nullptr)
 {
     if (!shots || n < 1) return dn_fail(DN_EINVAL, "dn_run: empty batch");
-    if (mode < 0 || mode > 2) return dn_fail(DN_EINVAL, "dn_run: bad mode %d", mode);
+    if (!modes && (mode < 0 || mode > 2)) return dn_fail(DN_EINVAL, "dn_run: bad mode %d", mode);
     const dn_params &p0 = shots[0]->p;
     c.R = p0.fdorder / 2;
     c.L = p0.L;
     c.exact = p0.arith == DN_ARITH_EXACT;
     c.bx = shots[0]->bx;
-    // stencil kernels: register streaming (default, fastest measured on B200) or, with
-    // DN_KERNEL=tma, the bulk-copy row pipeline of dn_kernels_tma.cuh
     // stencil kernels: register streaming (default, fastest measured on B200) or, with
     // DN_KERNEL=tma, the bulk-copy row pipeline of dn_kernels_tma.cuh
     const char *kern = getenv("DN_KERNEL");
@@ -931,24 +930,26 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c)
     for (int k = 0; k < n; k++) {
         const dn_shot *s = shots[k];
         if (!s) return dn_fail(DN_EINVAL, "dn_run: null shot %d", k);
+        const int m = modes ? modes[k] : mode;
+        if (m < 0 || m > 2) return dn_fail(DN_EINVAL, "dn_run: bad mode %d", m);
         if (s->m->device != shots[0]->m->device) return dn_fail(DN_EINVAL, "dn_run: shots on different devices");
         if (s->p.fdorder != p0.fdorder || s->p.L != p0.L)
             return dn_fail(DN_EINVAL, "dn_run: a batch must share FDORDER and L (shot %d differs)", k);
         if (s->p.arith != p0.arith || s->bx != c.bx) return dn_fail(DN_EINVAL, "dn_run: mixed arithmetic/tile width");
-        if (mode == 1) {
+        if (m == 1) {
             if (!s->stored) return dn_fail(DN_ESTATE, "dn_run: adjoint run of shot %d without a stored forward run", k);
             for (int l = 0; l < s->nsrc; l++)
                 if (s->src_type[l] == 5)
                     return dn_fail(DN_ENOTSUP, "moment-tensor sources are not supported in the adjoint pass");
         }
         maxtiles = std::max(maxtiles, s->tiles);
-        maxsrc = std::max(maxsrc, std::max(s->nsrc_cells, mode == 1 ? s->ntr : 0));
+        maxsrc = std::max(maxsrc, std::max(s->nsrc_cells, m == 1 ? s->ntr : 0));
         maxnx = std::max(maxnx, s->p.nx);
         maxtr = std::max(maxtr, s->ntr);
         if (s->p.free_surf) c.any_surf = true;
-        if (mode == 1 ? s->p.quelltypb >= 4 : (s->quelltyp_last == 1 || s->quelltyp_last == 5)) c.any_src_s = true;
-        if (mode == 0 && s->p.store_snapshots && s->nsnap > 0) c.any_store = true;
-        if (mode == 1) c.any_adj = true;
+        if (m == 1 ? s->p.quelltypb >= 4 : (s->quelltyp_last == 1 || s->quelltyp_last == 5)) c.any_src_s = true;
+        if (m == 0 && s->p.store_snapshots && s->nsnap > 0) c.any_store = true;
+        if (m == 1) c.any_adj = true;
     }
     c.tile_grid = dim3(maxtiles, n);
     c.src_grid = dim3((maxsrc + 127) / 128, n);
@@ -1137,6 +1138,202 @@ extern "C" int dn_last_run_stats(double *ms, long long *launches)
 {
     if (ms) *ms = g_last_ms;
     if (launches) *launches = g_last_launches;
+    return DN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// run queues: continuous batching
+//
+// A queue runs shots that share FDORDER, L and arithmetic, each at its own
+// time step: an instance that joined when the queue's step counter stood at t0
+// computes step *ntb + off - t0.  Membership changes only between chunks of
+// `chunk` time steps: dn_queue_step waits for the chunk in flight, retires the
+// shots it finished, admits the shots added since, re-captures the chunk graph
+// if the membership changed and enqueues the next chunk without waiting for
+// it.  Each queue owns a stream, so chunks of different queues overlap.
+// ---------------------------------------------------------------------------
+struct QSlot {
+    dn_shot *s;
+    int mode;
+    long long t0;
+};
+
+struct dn_queue {
+    int device = 0, chunk = 50;
+    cudaStream_t stream = nullptr;
+    int *d_step = nullptr;
+    cudaEvent_t ev = nullptr;
+    bool inflight = false, dirty = true;
+    long long gstep = 0;                 // value of *d_step once the enqueued chunks have run
+    std::vector<QSlot> active, pending;
+    std::vector<Inst> h_insts;
+    Inst *d_insts = nullptr;
+    int cap_insts = 0;
+    cudaGraphExec_t exec = nullptr;
+    long long launches_per_chunk = 0;
+};
+
+extern "C" int dn_queue_create(int device, int chunk, dn_queue **out)
+{
+    if (!out) return dn_fail(DN_EINVAL, "dn_queue_create: null out");
+    *out = nullptr;
+    if (chunk < 1 || chunk > 4096) return dn_fail(DN_EINVAL, "dn_queue_create: chunk %d outside 1..4096", chunk);
+    CU(cudaSetDevice(device));
+    dn_queue *q = new dn_queue();
+    q->device = device;
+    q->chunk = chunk;
+    if (cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&q->d_step, sizeof(int)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&q->ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMemset(q->d_step, 0, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        dn_queue_destroy(q);
+        return dn_fail(DN_EDEVICE, "dn_queue_create: stream/counter set-up failed");
+    }
+    *out = q;
+    return DN_OK;
+}
+
+extern "C" int dn_queue_destroy(dn_queue *q)
+{
+    if (!q) return DN_OK;
+    cudaSetDevice(q->device);
+    if (q->stream) cudaStreamSynchronize(q->stream);
+    if (q->exec) cudaGraphExecDestroy(q->exec);
+    cudaFree(q->d_insts);
+    cudaFree(q->d_step);
+    if (q->ev) cudaEventDestroy(q->ev);
+    if (q->stream) cudaStreamDestroy(q->stream);
+    delete q;
+    return DN_OK;
+}
+
+extern "C" int dn_queue_add(dn_queue *q, dn_shot *s, int mode)
+{
+    if (!q || !s) return dn_fail(DN_EINVAL, "dn_queue_add: null argument");
+    if (mode < 0 || mode > 2) return dn_fail(DN_EINVAL, "dn_queue_add: bad mode %d", mode);
+    if (s->m->device != q->device) return dn_fail(DN_EINVAL, "dn_queue_add: shot on device %d, queue on %d",
+                                                  s->m->device, q->device);
+    const dn_shot *ref = !q->active.empty() ? q->active[0].s : !q->pending.empty() ? q->pending[0].s : nullptr;
+    if (ref && (ref->p.fdorder != s->p.fdorder || ref->p.L != s->p.L || ref->p.arith != s->p.arith ||
+                ref->bx != s->bx))
+        return dn_fail(DN_EINVAL, "dn_queue_add: a queue runs one FDORDER, L and arithmetic");
+    for (const QSlot &x : q->active)
+        if (x.s == s) return dn_fail(DN_ESTATE, "dn_queue_add: shot already running in this queue");
+    for (const QSlot &x : q->pending)
+        if (x.s == s) return dn_fail(DN_ESTATE, "dn_queue_add: shot already waiting in this queue");
+    if (mode == 1 && !s->stored) return dn_fail(DN_ESTATE, "dn_queue_add: adjoint run without a stored forward run");
+    q->pending.push_back({s, mode, 0});
+    return DN_OK;
+}
+
+extern "C" int dn_queue_count(const dn_queue *q, int *running, int *waiting)
+{
+    if (!q) return dn_fail(DN_EINVAL, "dn_queue_count: null queue");
+    if (running) *running = (int)q->active.size();
+    if (waiting) *waiting = (int)q->pending.size();
+    return DN_OK;
+}
+
+static int queue_capture(dn_queue *q)
+{
+    const int n = (int)q->active.size();
+    std::vector<dn_shot *> shots(n);
+    std::vector<int> modes(n);
+    q->h_insts.clear();
+    for (int k = 0; k < n; k++) {
+        shots[k] = q->active[k].s;
+        modes[k] = q->active[k].mode;
+        Inst I = make_inst(shots[k], modes[k]);
+        I.t0 = (int)q->active[k].t0;
+        q->h_insts.push_back(I);
+    }
+    LaunchCfg c;
+    int st = check_batch(shots.data(), n, 0, c, modes.data());
+    if (st) return st;
+    st = prepare_launch(c);
+    if (st) return st;
+    if (n > q->cap_insts) {
+        cudaFree(q->d_insts);
+        q->d_insts = nullptr;
+        q->cap_insts = 0;
+        if (cudaMalloc(&q->d_insts, sizeof(Inst) * n) != cudaSuccess)
+            return dn_fail(DN_ENOMEM, "dn_queue_step: descriptor allocation failed");
+        q->cap_insts = n;
+    }
+    CU(cudaMemcpyAsync(q->d_insts, q->h_insts.data(), sizeof(Inst) * n, cudaMemcpyHostToDevice, q->stream));
+    if (q->exec) {
+        cudaGraphExecDestroy(q->exec);
+        q->exec = nullptr;
+    }
+    cudaGraph_t g;
+    CU(cudaStreamBeginCapture(q->stream, cudaStreamCaptureModeThreadLocal));
+    long long nl = 0;
+    for (int k = 0; k < q->chunk; k++) launch_step(c, q->stream, q->d_insts, q->d_step, k + 1, nl);
+    k_advance<<<1, 1, 0, q->stream>>>(q->d_step, q->chunk);
+    nl++;
+    cudaError_t e = cudaStreamEndCapture(q->stream, &g);
+    if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "queue graph capture failed: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&q->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        q->exec = nullptr;
+        return dn_fail(DN_EDEVICE, "queue graph instantiate failed: %s", cudaGetErrorString(e));
+    }
+    q->launches_per_chunk = nl;
+    q->dirty = false;
+    return DN_OK;
+}
+
+extern "C" int dn_queue_step(dn_queue *q, dn_shot **done, int *status, int cap, int *ndone)
+{
+    if (!q || !ndone || (cap > 0 && (!done || !status))) return dn_fail(DN_EINVAL, "dn_queue_step: bad arguments");
+    *ndone = 0;
+    CU(cudaSetDevice(q->device));
+    if (q->inflight) {
+        CU(cudaEventSynchronize(q->ev));
+        q->inflight = false;
+        CU(cudaGetLastError());
+    }
+    // retire the shots whose last step has run (as many as `done` holds)
+    for (size_t k = 0; k < q->active.size() && *ndone < cap;) {
+        QSlot &x = q->active[k];
+        if (x.t0 + x.s->p.nt > q->gstep) {
+            k++;
+            continue;
+        }
+        int f = 0;
+        CU(cudaMemcpy(&f, x.s->d_flag, 4, cudaMemcpyDeviceToHost));
+        int st = DN_OK;
+        if (f & 2) st = DN_ETIMEDOUT;
+        else if (f & 1) st = DN_EUNSTABLE;
+        if (x.mode == 0 && x.s->p.store_snapshots) x.s->stored = st == DN_OK;
+        if (x.mode == 1) x.s->correlated = st == DN_OK;
+        done[*ndone] = x.s;
+        status[*ndone] = st;
+        (*ndone)++;
+        q->active.erase(q->active.begin() + k);
+        q->dirty = true;
+    }
+    // admit the shots added since the last chunk: their step 1 is the next one
+    for (QSlot &x : q->pending) {
+        int st = zero_for_run(x.s, x.mode, q->stream);
+        if (st) return st;
+        x.t0 = q->gstep;
+        q->active.push_back(x);
+        q->dirty = true;
+    }
+    q->pending.clear();
+    if (q->active.empty()) return DN_OK;
+    if (q->gstep + q->chunk > INT32_MAX - 1) return dn_fail(DN_ENOTSUP, "dn_queue_step: step counter range exhausted");
+    if (q->dirty) {
+        int st = queue_capture(q);
+        if (st) return st;
+    }
+    CU(cudaGraphLaunch(q->exec, q->stream));
+    CU(cudaEventRecord(q->ev, q->stream));
+    q->inflight = true;
+    q->gstep += q->chunk;
     return DN_OK;
 }
 

@@ -82,6 +82,7 @@ struct Inst {
     int *flag;                        // bit 0: NaN seen at the psv.c:99 probe
     float rdh;                        // RN(1 / DH)
     int fastdiv;                      // division by DH through div_markstein (verified for this DH)
+    int t0;                           // step base when the instance joined: its step is *ntb + off - t0
 };
 
 // ---------------------------------------------------------------------------
@@ -164,9 +165,9 @@ __device__ __forceinline__ bool tile_of(const Inst &I, TileLoc &t)
 template <int R, bool X>
 __global__ void __launch_bounds__(256, 5) k_update_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt) return;
     TileLoc t;
     if (!tile_of(I, t)) return;
     const long long P = I.pitch;
@@ -293,9 +294,9 @@ __global__ void __launch_bounds__(256, 5) k_update_v(const Inst *__restrict__ in
 // ===========================================================================
 static __global__ void k_inject_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt) return;
     const long long P = I.pitch;
     if (I.mode == 1) {
         const int q = I.quelltypb;
@@ -443,9 +444,9 @@ struct VDeriv {
 template <int R, bool X>
 __global__ void __launch_bounds__(256, 4) k_update_s_el(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt) return;
     TileLoc t;
     if (!tile_of(I, t)) return;
     const long long P = I.pitch;
@@ -501,9 +502,9 @@ __global__ void __launch_bounds__(256, 4) k_update_s_el(const Inst *__restrict__
 template <int R, int L, bool X>
 __global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt) return;
     TileLoc t;
     if (!tile_of(I, t)) return;
     const long long P = I.pitch;
@@ -621,9 +622,9 @@ __global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__
 // ===========================================================================
 static __global__ void k_inject_s(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt) return;
     const long long P = I.pitch;
     if (I.mode == 1) {
         if (I.quelltypb < 4) return;
@@ -684,9 +685,9 @@ static __global__ void k_inject_s(const Inst *__restrict__ insts, const int *__r
 template <int R, bool X>
 __global__ void k_surface_el(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt || !I.free_surf) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt || !I.free_surf) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     if (i > I.nx) return;
     const long long P = I.pitch;
@@ -734,9 +735,9 @@ __global__ void k_surface_el(const Inst *__restrict__ insts, const int *__restri
 template <int R, int L, bool X>
 __global__ void k_surface_vi(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt || !I.free_surf) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt || !I.free_surf) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     if (i > I.nx) return;
     const long long P = I.pitch;
@@ -810,9 +811,9 @@ __global__ void k_surface_vi(const Inst *__restrict__ insts, const int *__restri
 template <int R>
 __global__ void k_seismo(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt) return;
     const long long P = I.pitch;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         float v = I.vy[(long long)(I.ny / 2) * P + I.nx / 2];
@@ -888,9 +889,9 @@ __device__ __forceinline__ float pow2_scale(float amax)
 
 static __global__ void k_snap_store(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt || I.mode != 0 || !I.store || ((nt - 1) % I.dtinv) != 0) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt || I.mode != 0 || !I.store || ((nt - 1) % I.dtinv) != 0) return;
     const int k = (nt - 1) / I.dtinv;
     if (k >= I.nsnap) return;
     const int b = blockIdx.x;
@@ -954,9 +955,9 @@ __device__ __forceinline__ float snap_load(const Inst &I, long long slot, long l
 // ===========================================================================
 static __global__ void k_correlate(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt || I.mode != 1) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt || I.mode != 1) return;
     const int nf = I.nt - nt + 1;   // mirrored forward step
     if (((nf - 1) % I.dtinv) != 0) return;
     const int k = (nf - 1) / I.dtinv;

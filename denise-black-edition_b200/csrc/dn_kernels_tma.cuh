@@ -62,9 +62,9 @@ __global__ void __launch_bounds__(TMA_W) k_update_v_tma(const Inst *__restrict__
                                                         int off)
 {
     extern __shared__ __align__(128) float smem[];
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt) return;
     StripGeom g;
     if (!strip_of(I, g)) return;
     constexpr int W = TMA_W, WH = TMA_WH;
@@ -281,9 +281,9 @@ __global__ void __launch_bounds__(TMA_W) k_update_s_el_tma(const Inst *__restric
                                                            const int *__restrict__ ntb, int off)
 {
     extern __shared__ __align__(128) float smem[];
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt) return;
     StripGeom g;
     if (!strip_of(I, g)) return;
     constexpr int W = TMA_W, WH = TMA_WH;
@@ -353,9 +353,9 @@ __global__ void __launch_bounds__(TMA_W) k_update_s_vi_tma(const Inst *__restric
                                                            const int *__restrict__ ntb, int off)
 {
     extern __shared__ __align__(128) float smem[];
-    const int nt = *ntb + off;
     const Inst &I = insts[blockIdx.y];
-    if (nt > I.nt) return;
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt) return;
     StripGeom g;
     if (!strip_of(I, g)) return;
     constexpr int W = TMA_W, WH = TMA_WH;

@@ -125,6 +125,11 @@ SIGNATURES = {
     "dn_residual_l2": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
                                       _c_double_p]),
     "dn_shot_residual": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p, _c_double_p]),
+    "dn_queue_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _P(_vp)]),
+    "dn_queue_destroy": (ctypes.c_int, [_vp]),
+    "dn_queue_add": (ctypes.c_int, [_vp, _vp, ctypes.c_int]),
+    "dn_queue_step": (ctypes.c_int, [_vp, _P(_vp), _c_int_p, ctypes.c_int, _c_int_p]),
+    "dn_queue_count": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
     "dn_device_memory": (ctypes.c_int, [ctypes.c_int, _P(ctypes.c_size_t), _P(ctypes.c_size_t)]),
     "dn_inp_read": (ctypes.c_int, [ctypes.c_char_p, _vp]),
     "dn_inp_nt": (ctypes.c_int, [_vp]),

@@ -256,6 +256,24 @@ int dn_shot_residual(dn_shot *s, int comp, const float *obs, double *l2);
  * receivers, snapshot store, cross-correlation (0 where not launched). */
 int dn_profile_steps(dn_shot *const *shots, int n, int mode, int nsteps, double *ms_out);
 
+/* ---- run queues: continuous batching ---------------------------------------
+ * A queue runs shots of one FDORDER, L and arithmetic together, each at its own
+ * time step, on its own CUDA stream (queues overlap on the device).  Shots join
+ * and leave between chunks of `chunk` time steps.  A shot must not be destroyed
+ * or run elsewhere while it is in a queue (until dn_queue_step returns it).
+ * The batched launch this builds on replaces the reference's one-shot psv()
+ * loop; the queue itself has no counterpart in the reference. */
+typedef struct dn_queue dn_queue;
+int dn_queue_create(int device, int chunk, dn_queue **out);
+int dn_queue_destroy(dn_queue *q);
+/* the shot runs `mode` (DN_MODE_*) from its step 1, joining at the next dn_queue_step */
+int dn_queue_add(dn_queue *q, dn_shot *s, int mode);
+/* Waits for the chunk in flight; returns the shots it finished (at most cap) in
+ * done[0..*ndone) with their status (DN_OK, DN_EUNSTABLE); admits the added
+ * shots; enqueues the next chunk and returns without waiting for it. */
+int dn_queue_step(dn_queue *q, dn_shot **done, int *status, int cap, int *ndone);
+int dn_queue_count(const dn_queue *q, int *running, int *waiting);
+
 #ifdef __cplusplus
 }
 #endif
