@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--plain-shots", type=int, default=4)
     ap.add_argument("--cpu-sample-nt", type=int, default=60)
+    ap.add_argument("--serve-requests", type=int, default=32,
+                    help="requests of the serving workload run after the batch measurement (0: skip)")
+    ap.add_argument("--serve-scale", type=float, default=1.0, help="shrinks NX, NZ and NT of served requests")
     ap.add_argument("--elastic-nt", type=int, default=1000,
                     help="NT of the elastic batch measured beside the viscoelastic one (0: skip)")
     return ap.parse_args()
@@ -269,6 +272,12 @@ def run_ours(a, rank, world, local_rank):
         elastic = None
         if a.elastic_nt > 0:
             elastic = run_elastic(a, inputs, device, peak)
+        serving = None
+        if a.serve_requests > 0:
+            for m_, s_ in pairs:       # free the batch's HBM for the served requests
+                s_.close()
+                m_.close()
+            serving = run_serving(a, device, value)
         e2e = None
         if not a.no_e2e:
             e2e = run_e2e(p, inputs, device, cells_step)
@@ -292,6 +301,8 @@ def run_ours(a, rank, world, local_rank):
         }
         if elastic:
             result["elastic"] = elastic
+        if serving:
+            result["serving"] = serving
         if e2e:
             result["e2e"] = e2e
         if cpu:
@@ -339,6 +350,49 @@ def run_elastic(a, inputs, device, peak):
         s.close()
         m.close()
     return out
+
+
+def run_serving(a, device, mcells_per_s):
+    """The serving workload: requests arrive as a Poisson process at 1.2x the
+    capacity implied by the batched throughput just measured; the server admits
+    them by HBM footprint into its run queues.  Latency = scheduled arrival ->
+    result on the host."""
+    from denise_b200 import serve, synth
+
+    reqs = synth.serve_requests(a.serve_requests, seed=3, scale=a.serve_scale)
+    work = []
+    for kind, p, model, shots, obs in reqs:
+        w = p.nx * p.ny * p.nt * len(shots)
+        work.append(2 * w if kind == "gradient" else w)
+    rate = 1.2 * mcells_per_s * 1e6 / float(np.mean(work))      # requests per second
+    rng = np.random.default_rng(3)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+    srv = serve.Server(device=device, chunk=50)
+    t0 = time.perf_counter()
+    i = 0
+    while i < len(reqs) or not srv.idle():
+        now = time.perf_counter() - t0
+        while i < len(reqs) and arrivals[i] <= now:
+            kind, p, model, shots, obs = reqs[i]
+            srv.submit(serve.Request(kind, p, model, shots, obs, rid=i), now=t0 + arrivals[i])
+            i += 1
+        if srv.idle():
+            time.sleep(max(0.0, min(0.05, arrivals[i] - (time.perf_counter() - t0))))
+            continue
+        srv.step()
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    bad = sum(1 for r in srv.results if r.status != 0)
+    return {"requests": len(reqs), "failed": bad, "p50_latency_s": round(st["p50_s"], 3),
+            "p99_latency_s": round(st["p99_s"], 3), "shots_per_s": round(st["shots_done_total"] / wall, 3),
+            "mcell_updates_per_s": round(sum(work) / wall / 1e6, 1), "wall_s": round(wall, 2),
+            "arrival_rate_per_s": round(rate, 3), "max_running_shots": st["max_running_shots"],
+            "joins_while_running": st["joins_while_running"],
+            "workload": "seeded serving mix: 70% elastic forward, 20% visco L=3 forward, 10% elastic FWI gradient "
+                        "(FP16 snapshots); NX 300-3000, NZ 150-1000, NT 2000-8000 (x scale "
+                        f"{a.serve_scale}), FDORDER 4/8/12, 1-4 shots, 50-500 receivers; Poisson arrivals at 1.2x "
+                        "the batched capacity"}
 
 
 def run_e2e(p, inputs, device, cells_step):

@@ -250,7 +250,7 @@ class Server:
         return {"requests": len(self.results), "p50_s": float(np.percentile(lat, 50)),
                 "p99_s": float(np.percentile(lat, 99)), "shots_per_s": self.shots_done / max(wall, 1e-9),
                 "max_running_shots": self.max_running, "joins_while_running": self.joins_while_running,
-                "rounds": self.rounds}
+                "rounds": self.rounds, "shots_done_total": self.shots_done}
 
     def close(self):
         for q in self.queues.values():

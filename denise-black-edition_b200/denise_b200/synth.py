@@ -150,3 +150,66 @@ def c2_params(**kw):
                 store_snapshots=1)
     base.update(kw)
     return PsvParams(**base)
+
+
+# ---------------------------------------------------------------------------
+# the serving workload: a seeded stream of requests of mixed size and kind
+# ---------------------------------------------------------------------------
+SERVE_MIX = (("forward", 0, 0.7), ("forward", 3, 0.2), ("gradient", 0, 0.1))   # kind, L, share
+
+
+def serve_requests(n, seed=3, scale=1.0, snap_budget=16e9):
+    """n requests: 70 % elastic forward, 20 % viscoelastic (L = 3) forward, 10 %
+    elastic FWI gradients; NX in U[300, 3000], NZ in U[150, 1000], DH in U[5, 10],
+    NT in U[2000, 8000], FDORDER in {4, 8, 12}, 1-4 shots and 50-500 receivers
+    per request, the model of request k from seed 1000 + k, DT = 0.9 of the CFL
+    limit (checkfd_ssg_elastic.c:89).  `scale` shrinks NX, NZ and NT for quick
+    runs.  Gradient requests store FP16 snapshots every DTINV steps, DTINV the
+    smallest even interval that keeps one shot's snapshots under snap_budget
+    bytes; their observed data are zero traces.  Returns (kind, params, model,
+    shots, obs) tuples; shots are (src_i, src_j, signals, rec_i, rec_j)."""
+    from .api import cfl_limit
+
+    rng = np.random.default_rng(seed)
+    kinds = rng.choice(len(SERVE_MIX), size=n, p=[m[2] for m in SERVE_MIX])
+    out = []
+    for k in range(n):
+        kind, L, _ = SERVE_MIX[kinds[k]]
+        nx = max(60, int(rng.integers(300, 3001) * scale))
+        ny = max(40, int(rng.integers(150, 1001) * scale))
+        dh = float(rng.uniform(5.0, 10.0))
+        nt = max(200, int(rng.integers(2000, 8001) * scale))
+        fdorder = int(rng.choice([4, 8, 12]))
+        nshots = int(rng.integers(1, 5))
+        nrec = int(rng.integers(50, 501))
+        vp, vs, rho = base_model(nx, ny, dh, 1000 + k, smooth_sigma=4.0)
+        model = (vp, vs, rho)
+        kw = dict(nx=nx, ny=ny, dh=dh, nt=nt, fdorder=fdorder, maxrelerror=1, free_surf=1, fw=20,
+                  damping=1500.0, fpml=10.0, npower=4.0, k_max_pml=1.0, L=L, fl=C1_FL[:L], ts=1.0 / 8.0)
+        if L:
+            model = model + q_model(nx, ny, 1000 + k, smooth_sigma=4.0)
+        if kind == "gradient":
+            per_snap = 5 * 2 * nx * ny
+            dtinv = 2
+            while nt / dtinv * per_snap > snap_budget:
+                dtinv += 2
+            kw.update(store_snapshots=1, dtinv=dtinv, snap_precision=1)
+        p = PsvParams(dt=1e-3, **kw)
+        dtstab, _ = cfl_limit(p, float(vp.max()))
+        p = p.replace(dt=float(np.float32(0.9 * dtstab)))
+        sig = wavelet(1, nt, p.dt, 0.0, 8.0, 1.0)[None, :]
+        xmax = (nx - 1) * dh
+        nr = min(nrec, nx - 2 * 20 - 2)
+        ri, rj = receivers_line(min(100.0, 0.1 * xmax), xmax - min(100.0, 0.1 * xmax), nr, 20.0, dh)
+        rj = np.maximum(rj, 1)
+        shots = []
+        for s in range(nshots):
+            xs = 0.2 * xmax + 0.6 * xmax * s / max(nshots - 1, 1)
+            shots.append((np.array([max(1, grid_index(xs, dh))], np.int32),
+                          np.array([max(1, grid_index(10.0, dh))], np.int32), sig, ri, rj))
+        obs = None
+        if kind == "gradient":
+            z = np.zeros((len(ri), nt), np.float32)
+            obs = [(z, z) for _ in range(nshots)]
+        out.append((kind, p, model, shots, obs))
+    return out
