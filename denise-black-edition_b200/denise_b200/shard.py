@@ -1,0 +1,85 @@
+"""Shot sharding over ranks (one process per GPU) and the FWI gradient sum.
+
+Shots are independent until the gradient sum, so each rank runs its own shots
+as one batch on its own GPU with no collective on the data path; the only
+exchange is the per-iteration sum of the three gradient arrays and the misfit
+over ranks, which replaces the reference's element-wise MPI_Allreduce of the
+stacked gradient (src/PSV/grad_obj_psv.c:371-390).  Shots go to ranks by
+longest-processing-time first on their cost (cells x time steps), so ranks
+with uneven shot sizes finish together.
+
+torch.distributed carries the collective: NCCL on GPU tensors in production,
+gloo on CPU tensors in the tests.
+"""
+import numpy as np
+
+
+def assign_shots(costs, world):
+    """LPT assignment: shot indices per rank, each rank's list in shot order."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = [0.0] * world
+    out = [[] for _ in range(world)]
+    for k in sorted(range(len(costs)), key=lambda k: (-costs[k], k)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        out[r].append(k)
+        load[r] += costs[k]
+    return [sorted(x) for x in out]
+
+
+def allreduce_sum(arrays, dist=None, device=None):
+    """Sums float arrays over all ranks (in float64) and returns them on the host.
+    dist: torch.distributed (initialised) or None for a single process."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return [np.asarray(a, np.float64) for a in arrays]
+    import torch
+
+    flat = np.concatenate([np.asarray(a, np.float64).ravel() for a in arrays])
+    t = torch.from_numpy(flat)
+    if device is not None:
+        t = t.to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    flat = t.cpu().numpy()
+    out, o = [], 0
+    for a in arrays:
+        n = np.asarray(a).size
+        out.append(flat[o:o + n].reshape(np.shape(a)))
+        o += n
+    return out
+
+
+def sharded_gradient(params, model, shots, obs, dist=None, device_index=0):
+    """FWI gradient of `shots` sharded over the ranks of `dist` (all ranks pass
+    the same arguments).  Each rank runs its share as one batch on its GPU:
+    forward with snapshots, device residuals against `obs`, adjoint, and stacks
+    its shots' gradients in shot order; the partial gradients and misfits are
+    then summed over ranks.  Returns (g_vp, g_vs, g_rho, misfit), float64, on
+    every rank."""
+    from . import api as dn
+    from ._lib import MODE_ADJOINT, MODE_FORWARD, SEC_VX, SEC_VY
+
+    rank = dist.get_rank() if dist is not None and dist.is_initialized() else 0
+    world = dist.get_world_size() if dist is not None and dist.is_initialized() else 1
+    costs = [params.nx * params.ny * params.nt for _ in shots]
+    mine = assign_shots(costs, world)[rank]
+    g = [np.zeros((params.nx, params.ny), np.float64) for _ in range(3)]
+    misfit = 0.0
+    if mine:
+        m = dn.Model(params, *model[:3], model[3] if params.L else None, model[4] if params.L else None,
+                     device=device_index)
+        ss = [dn.Shot(m, *shots[k][:5]) for k in mine]
+        dn.run(ss, MODE_FORWARD)
+        for s, k in zip(ss, mine):
+            misfit += s.residual(obs[k][0], SEC_VX) + s.residual(obs[k][1], SEC_VY)
+        dn.run(ss, MODE_ADJOINT)
+        for s in ss:
+            s.accumulate_gradient()
+        g = [x.astype(np.float64) for x in m.gradient()]
+        for s in ss:
+            s.close()
+        m.close()
+    dev = None
+    if dist is not None and dist.is_initialized() and dist.get_backend() == "nccl":
+        dev = f"cuda:{device_index}"
+    red = allreduce_sum(g + [np.array([misfit])], dist, dev)
+    return red[0], red[1], red[2], float(red[3][0])
