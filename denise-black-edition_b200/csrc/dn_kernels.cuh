@@ -197,26 +197,30 @@ __global__ void __launch_bounds__(256, 5) k_update_v(const Inst *__restrict__ in
         wyy[k] = __ldg(syy + (long long)(t.j0 - R + 1 + k) * P);
         wxy[k] = __ldg(sxy + (long long)(t.j0 - R + k) * P);
     }
-    // own-column operands of row j+1 are fetched before row j is computed (this also
-    // brings the cache lines the x-neighbour loads of the row will hit into L1)
-    float nyy, nxy, nrip, nrjp, nvx, nvy, nsx, nsy;
+    // own-column operands of row j+1 are fetched before row j is computed
+    // (this also brings the cache lines the x-neighbour loads of the row will hit
+    // into L1); the own sxy of row j is the window's wxy[R]
+    struct Ops {
+        float yy, xy, sx, rip, rjp, vx, vy;
+    };
     auto fetch = [&](int j) {
         const long long o = (long long)j * P;
-        nyy = __ldg(syy + o + R * P);
-        nxy = __ldg(sxy + o + (R - 1) * P);
-        nsx = __ldg(sxx + o);
-        nsy = __ldg(sxy + o);
-        nrip = __ldg(rip + o);
-        nrjp = __ldg(rjp + o);
-        nvx = vx[o];
-        nvy = vy[o];
+        Ops n;
+        n.yy = __ldg(syy + o + R * P);
+        n.xy = __ldg(sxy + o + (R - 1) * P);
+        n.sx = __ldg(sxx + o);
+        n.rip = __ldg(rip + o);
+        n.rjp = __ldg(rjp + o);
+        n.vx = vx[o];
+        n.vy = vy[o];
+        return n;
     };
-    fetch(t.j0);
+    Ops n1 = fetch(t.j0);
     for (int j = t.j0; j <= t.j1; j++) {
-        wyy[2 * R - 1] = nyy;
-        wxy[2 * R - 1] = nxy;
-        const float ripv = nrip, rjpv = nrjp, vxo = nvx, vyo = nvy, csx = nsx, csy = nsy;
-        if (j < t.j1) fetch(j + 1);
+        wyy[2 * R - 1] = n1.yy;
+        wxy[2 * R - 1] = n1.xy;
+        const float ripv = n1.rip, rjpv = n1.rjp, vxo = n1.vx, vyo = n1.vy, csx = n1.sx, csy = wxy[R];
+        if (j < t.j1) n1 = fetch(j + 1);
         // ax[k] = sxx[j][i-R+1+k], bx[k] = sxy[j][i-R+k]; the own-column entries come from the prefetch
         const float *rs = sxx + (long long)j * P;
         const float *rx = sxy + (long long)j * P;
