@@ -43,14 +43,6 @@ extern "C" int dn_version(int *major, int *minor)
     return DN_OK;
 }
 
-#define CU(call)                                                                                   \
-    do {                                                                                           \
-        cudaError_t e_ = (call);                                                                   \
-        if (e_ != cudaSuccess) {                                                                   \
-            return dn_fail(e_ == cudaErrorMemoryAllocation ? DN_ENOMEM : DN_EDEVICE, "%s: %s (%s:%d)", \
-                           #call, cudaGetErrorString(e_), __FILE__, __LINE__);                     \
-        }                                                                                          \
-    } while (0)
 
 extern "C" int dn_device_count(int *count)
 {

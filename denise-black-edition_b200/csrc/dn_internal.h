@@ -22,6 +22,18 @@ int dn_visc_cell_factors(const dn_params *p, const float *vp, const float *vs, c
 }
 #endif
 
+#ifdef __CUDACC__
+/* Returns a DN_E* status from the calling function when a CUDA call fails. */
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            return dn_fail(e_ == cudaErrorMemoryAllocation ? DN_ENOMEM : DN_EDEVICE, "%s: %s (%s:%d)", \
+                           #call, cudaGetErrorString(e_), __FILE__, __LINE__);                     \
+        }                                                                                          \
+    } while (0)
+#endif
+
 /* Grid padding of every device field: HX columns left/right, HZ rows above/below
  * the interior.  HZ >= FDORDER/2 covers the free-surface image rows and the
  * stencil reach; HX = 8 keeps column i = 1 16-byte aligned. */

@@ -130,6 +130,15 @@ SIGNATURES = {
     "dn_queue_add": (ctypes.c_int, [_vp, _vp, ctypes.c_int]),
     "dn_queue_step": (ctypes.c_int, [_vp, _P(_vp), _c_int_p, ctypes.c_int, _c_int_p]),
     "dn_queue_count": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
+    "dn_dot": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _c_double_p]),
+    "dn_lbfgs_create": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int, _P(_vp)]),
+    "dn_lbfgs_destroy": (ctypes.c_int, [_vp]),
+    "dn_lbfgs_push": (ctypes.c_int, [_vp, _vp, _vp]),
+    "dn_lbfgs_count": (ctypes.c_int, [_vp, _c_int_p]),
+    "dn_lbfgs_direction": (ctypes.c_int, [_vp, _vp, _vp]),
+    "dn_calc_opt_step": (ctypes.c_int, [_c_double_p, _c_float_p, _c_float_p]),
+    "dn_mat_update": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [_c_float_p] * 6 + [ctypes.c_float, _c_float_p,
+                                     ctypes.c_int, _c_int_p, ctypes.c_float] + [_c_float_p] * 4),
     "dn_device_memory": (ctypes.c_int, [ctypes.c_int, _P(ctypes.c_size_t), _P(ctypes.c_size_t)]),
     "dn_inp_read": (ctypes.c_int, [ctypes.c_char_p, _vp]),
     "dn_inp_nt": (ctypes.c_int, [_vp]),

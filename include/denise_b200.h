@@ -274,6 +274,37 @@ int dn_queue_add(dn_queue *q, dn_shot *s, int mode);
 int dn_queue_step(dn_queue *q, dn_shot **done, int *status, int cap, int *ndone);
 int dn_queue_count(const dn_queue *q, int *running, int *waiting);
 
+/* ---- FWI outer loop (FP64) ------------------------------------------------- */
+/* Deterministic FP64 dot product of two device vectors (fixed reduction order). */
+int dn_dot(const double *a, const double *b, long long n, double *out);
+
+/* L-BFGS of src/LBFGS.c (two-loop recursion, H0 = gamma I from the newest pair)
+ * on device-resident FP64 vectors of length n, keeping the m newest pairs. */
+typedef struct dn_lbfgs dn_lbfgs;
+int dn_lbfgs_create(long long n, int m, int device, dn_lbfgs **out);
+int dn_lbfgs_destroy(dn_lbfgs *L);
+/* s = x_{k+1} - x_k, y = g_{k+1} - g_k (device); rho = 1/(y.s), 0 when y.s = 0 */
+int dn_lbfgs_push(dn_lbfgs *L, const double *d_s, const double *d_y);
+int dn_lbfgs_count(const dn_lbfgs *L, int *count);
+/* r = H g (device vectors); the model update is x - eps r */
+int dn_lbfgs_direction(dn_lbfgs *L, const double *d_g, double *d_r);
+
+/* calc_opt_step (src/calc_opt_step.c): the step length at the extremum of the
+ * parabola through (epst[k], L2t[k]), k = 0..2, with the reference's clamping
+ * (beyond epst[2] or a maximum: epst[2]; negative: epst[0]); solved in FP64. */
+int dn_calc_opt_step(const double L2t[3], const float epst[3], float *opteps);
+
+/* calc_mat_change_test_PSV (INVMAT1 = 1): vp/vs/rho (file order, host) moved
+ * against the direction d* by eps_scale times max(model)/max|d| per parameter
+ * (rho additionally times scalerho; a parameter whose INV_*_ITER is above iter
+ * stays), then values outside lim = {vp_lo, vp_hi, vs_lo, vs_hi, rho_lo,
+ * rho_hi} or below 0 keep their old value (vs below vs_lo only when above
+ * 1e-6).  eps_out = {EPSILON, EPSILON_u, EPSILON_rho}. */
+int dn_mat_update(int nx, int ny, const float *vp, const float *vs, const float *rho, const float *dvp,
+                  const float *dvs, const float *drho, float eps_scale, const float lim[6], int iter,
+                  const int inv_iter[3], float scalerho, float *vp_out, float *vs_out, float *rho_out,
+                  float eps_out[3]);
+
 #ifdef __cplusplus
 }
 #endif

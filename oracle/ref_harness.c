@@ -445,3 +445,70 @@ int refh_outseis(const char *path, const float *section, int ntr, int ns, const 
     free_matrix(sp, 1, 8, 1, 1);
     return 0;
 }
+
+/* ---- FWI outer loop of the reference ---------------------------------------- */
+extern float EPSILON, EPSILON_u, EPSILON_rho, SCALERHO;
+extern float VPUPPERLIM, VPLOWERLIM, VSUPPERLIM, VSLOWERLIM, RHOUPPERLIM, RHOLOWERLIM;
+
+/* calc_opt_step() on three (step, misfit) pairs, 0-based in, the reference's 1-based inside */
+float refh_calc_opt_step(const double *L2t3, const float *epst3)
+{
+    double L[4] = {0.0, L2t3[0], L2t3[1], L2t3[2]};
+    float e[4] = {0.0f, epst3[0], epst3[1], epst3[2]};
+    return calc_opt_step(L, e, 1);
+}
+
+/* calc_mat_change_test_PSV(itest = 1): arrays in file order */
+int refh_mat_change(int nx, int ny, const float *vp, const float *vs, const float *rho, const float *gvp,
+                    const float *gvs, const float *grho, float eps_scale, const float *lim, int iter,
+                    const int *inv_iter, float scalerho, float *vp_out, float *vs_out, float *rho_out, float *eps3)
+{
+    NX = nx;
+    NY = ny;
+    MYID = 0;
+    INVMAT1 = 1;
+    VPLOWERLIM = lim[0];
+    VPUPPERLIM = lim[1];
+    VSLOWERLIM = lim[2];
+    VSUPPERLIM = lim[3];
+    RHOLOWERLIM = lim[4];
+    RHOUPPERLIM = lim[5];
+    INV_VP_ITER = inv_iter[0];
+    INV_VS_ITER = inv_iter[1];
+    INV_RHO_ITER = inv_iter[2];
+    SCALERHO = scalerho;
+    float **P = matrix(1, ny, 1, nx), **U = matrix(1, ny, 1, nx), **R = matrix(1, ny, 1, nx);
+    float **Pn = matrix(1, ny, 1, nx), **Un = matrix(1, ny, 1, nx), **Rn = matrix(1, ny, 1, nx);
+    float **Gp = matrix(1, ny, 1, nx), **Gu = matrix(1, ny, 1, nx), **Gr = matrix(1, ny, 1, nx);
+    for (int i = 1; i <= nx; i++)
+        for (int j = 1; j <= ny; j++) {
+            const size_t o = (size_t)(i - 1) * ny + (j - 1);
+            P[j][i] = vp[o];
+            U[j][i] = vs[o];
+            R[j][i] = rho[o];
+            Gp[j][i] = gvp[o];
+            Gu[j][i] = gvs[o];
+            Gr[j][i] = grho[o];
+        }
+    calc_mat_change_test_PSV(Gp, Gr, Gu, R, Rn, P, Pn, U, Un, iter, 1, eps_scale, 1);
+    for (int i = 1; i <= nx; i++)
+        for (int j = 1; j <= ny; j++) {
+            const size_t o = (size_t)(i - 1) * ny + (j - 1);
+            vp_out[o] = Pn[j][i];
+            vs_out[o] = Un[j][i];
+            rho_out[o] = Rn[j][i];
+        }
+    eps3[0] = EPSILON;
+    eps3[1] = EPSILON_u;
+    eps3[2] = EPSILON_rho;
+    free_matrix(P, 1, ny, 1, nx);
+    free_matrix(U, 1, ny, 1, nx);
+    free_matrix(R, 1, ny, 1, nx);
+    free_matrix(Pn, 1, ny, 1, nx);
+    free_matrix(Un, 1, ny, 1, nx);
+    free_matrix(Rn, 1, ny, 1, nx);
+    free_matrix(Gp, 1, ny, 1, nx);
+    free_matrix(Gu, 1, ny, 1, nx);
+    free_matrix(Gr, 1, ny, 1, nx);
+    return 0;
+}

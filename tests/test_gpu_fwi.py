@@ -1,0 +1,83 @@
+"""FWI outer loop on the GPU: the FP64 L-BFGS direction against a numpy
+restatement of the two-loop recursion, the secant condition, the deterministic
+dot product, and two FWI iterations lowering the misfit of a small problem."""
+import numpy as np
+import pytest
+
+from denise_b200 import fwi, synth
+
+import oracles as O
+from test_gpu_serve import _request
+
+pytestmark = pytest.mark.gpu
+
+
+def _two_loop(S, Y, g):
+    """Nocedal & Wright algorithm 7.4 with H0 = (s.y / y.y) I of the newest pair."""
+    q = g.copy()
+    rho = [1.0 / (y @ s) if (y @ s) != 0 else 0.0 for s, y in zip(S, Y)]
+    alpha = [0.0] * len(S)
+    for k in reversed(range(len(S))):
+        alpha[k] = rho[k] * (S[k] @ q)
+        q -= alpha[k] * Y[k]
+    r = (S[-1] @ Y[-1]) / (Y[-1] @ Y[-1]) * q
+    for k in range(len(S)):
+        beta = rho[k] * (Y[k] @ r)
+        r += S[k] * (alpha[k] - beta)
+    return r
+
+
+def test_lbfgs_direction_and_secant():
+    import torch
+
+    rng = np.random.default_rng(0)
+    n, m = 50_000, 5
+    A = rng.uniform(0.5, 4.0, n)                  # a diagonal SPD Hessian
+    L = fwi.LBFGS(n, m, 0)
+    xs = [rng.standard_normal(n) for _ in range(m + 3)]
+    S, Y = [], []
+    for a, b in zip(xs[:-1], xs[1:]):
+        s, y = b - a, A * (b - a)
+        L.push(s, y)
+        S.append(s)
+        Y.append(y)
+    S, Y = S[-m:], Y[-m:]
+    assert L.count() == m
+    g = A * xs[-1]
+    r = L.direction(g)
+    want = _two_loop(S, Y, g)
+    assert np.linalg.norm(r - want) <= 1e-10 * np.linalg.norm(want)
+    # secant: H y_newest = s_newest
+    assert np.linalg.norm(L.direction(Y[-1]) - S[-1]) <= 1e-9 * np.linalg.norm(S[-1])
+    L.close()
+    a = torch.as_tensor(rng.standard_normal(1_000_003)).cuda()
+    b = torch.as_tensor(rng.standard_normal(1_000_003)).cuda()
+    d1, d2 = fwi.dot(a, b), fwi.dot(a, b)
+    assert d1 == d2
+    assert abs(d1 - float(a.cpu().numpy() @ b.cpu().numpy())) <= 1e-10 * abs(d1)
+
+
+def test_two_fwi_iterations_lower_the_misfit():
+    import denise_b200 as dn
+
+    req = _request(0, "gradient", 90, 60, 500, 8, 0, 4, 11)
+    p = req.params
+    vp, vs, rho = req.model
+    vpt, vst, rhot = synth.add_ellipse(vp, vs, rho, p.dh, 3, v=3600.0)
+    # observed data from the true model
+    m = dn.Model(p.replace(store_snapshots=0), vpt, vst, rhot)
+    ss = [dn.Shot(m, *sh[:5]) for sh in req.shots]
+    dn.run(ss)
+    obs = [(s.sections(dn.SEC_VX), s.sections(dn.SEC_VY)) for s in ss]
+    for s in ss:
+        s.close()
+    m.close()
+    start = tuple(synth.smoothed(a, 3.0) for a in (vp, vs, rho))
+    lim = (1000.0, 6000.0, 500.0, 3500.0, 1000.0, 3500.0)
+    f = fwi.FWI(p, start, req.shots, obs, lim, device=0, nlbfgs=5, eps_scale=0.01)
+    L0 = f.iterate(1)
+    L1 = f.iterate(2)
+    L2 = f.misfit((f.vp, f.vs, f.rho))
+    assert all(h["found"] for h in f.history), f.history
+    assert L1 < L0 and L2 < L1, (L0, L1, L2)
+    f.lbfgs.close()
