@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=32,
                     help="requests of the serving workload run after the batch measurement (0: skip)")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="shrinks NX, NZ and NT of served requests")
+    ap.add_argument("--gradient-shots", type=int, default=32,
+                    help="shots of the FWI-gradient measurement (1700x500, NT 4000, FP16 snapshots; 0: skip)")
     ap.add_argument("--elastic-nt", type=int, default=1000,
                     help="NT of the elastic batch measured beside the viscoelastic one (0: skip)")
     return ap.parse_args()
@@ -181,6 +183,15 @@ def create_batch(p, inputs, device):
         return list(ex.map(mk, inputs))
 
 
+def workload_config(a, p, world):
+    return {"workload": f"batched viscoelastic forward: {a.shots} shots x {p.nx}x{p.ny} grid, NT={p.nt}, "
+                        f"L=3, FDORDER 8, FW 20, free surface, 400 receivers/shot",
+            "shots_per_gpu": a.shots, "nx": p.nx, "nz": p.ny, "nt": p.nt, "fdorder": p.fdorder, "L": p.L,
+            "arith": "exact (bit-identical to the reference)",
+            "l2_flush": "inputs larger than L2 (resident state ~15 GB)",
+            "parallelism": f"shots-dp{world}"}
+
+
 def run_ours(a, rank, world, local_rank):
     import denise_b200 as dn
     from denise_b200 import synth
@@ -272,6 +283,12 @@ def run_ours(a, rank, world, local_rank):
         elastic = None
         if a.elastic_nt > 0:
             elastic = run_elastic(a, inputs, device, peak)
+        gradient = None
+        if a.gradient_shots > 0:
+            for m_, s_ in pairs:       # the gradient batches need the HBM
+                s_.close()
+                m_.close()
+            gradient = run_gradient(a, device)
         serving = None
         if a.serve_requests > 0:
             for m_, s_ in pairs:       # free the batch's HBM for the served requests
@@ -285,12 +302,7 @@ def run_ours(a, rank, world, local_rank):
             "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(ms_step, 2), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model family, see denise_b200/synth.py)",
-            "config": {"workload": f"batched viscoelastic forward: {a.shots} shots x {p.nx}x{p.ny} grid, NT={p.nt}, "
-                                   f"L=3, FDORDER 8, FW 20, free surface, 400 receivers/shot",
-                       "shots_per_gpu": a.shots, "nx": p.nx, "nz": p.ny, "nt": p.nt, "fdorder": p.fdorder, "L": p.L,
-                       "arith": "exact (bit-identical to the reference)",
-                       "l2_flush": "inputs larger than L2 (resident state ~15 GB)",
-                       "parallelism": f"shots-dp{world}"},
+            "config": workload_config(a, p, world),
             "shots_per_s": {"batched": round(batched_sps, 3), "plain": round(plain_sps, 3),
                             "speedup": round(batched_sps / plain_sps, 3),
                             "plain_sample_shots": len(plain_shots)},
@@ -303,6 +315,8 @@ def run_ours(a, rank, world, local_rank):
             result["elastic"] = elastic
         if serving:
             result["serving"] = serving
+        if gradient:
+            result["gradient"] = gradient
         if e2e:
             result["e2e"] = e2e
         if cpu:
@@ -350,6 +364,79 @@ def run_elastic(a, inputs, device, peak):
         s.close()
         m.close()
     return out
+
+
+def run_gradient(a, device):
+    """FWI gradient (forward with snapshots + adjoint) of the 1700 x 500 elastic workload:
+    true model = the seeded family (seed 2), starting model = it smoothed with sigma 25
+    cells, observed data synthesised on the GPU from the true model; FP16 snapshots
+    every 2 steps; shots streamed through HBM in batches that fit."""
+    import ctypes
+
+    import denise_b200 as dn
+    import torch
+    from denise_b200 import synth
+
+    import oracles as O
+
+    p = synth.c2_params(snap_precision=dn.SNAP_F16)
+    n = a.gradient_shots
+    vpt, vst, rhot = synth.base_model(p.nx, p.ny, p.dh, 2)
+    start = tuple(synth.smoothed(x, 25.0) for x in (vpt, vst, rhot))
+    xmax = (p.nx - 1) * p.dh
+    sig = synth.ricker_source(p, 8.0)[None, :]
+    ri, rj = synth.receivers_line(100.0, xmax - 100.0, 400, 20.0, p.dh)
+    shots = [(np.array([synth.grid_index(200.0 + (xmax - 400.0) * k / max(n - 1, 1), p.dh)], np.int32),
+              np.array([max(synth.grid_index(10.0, p.dh), 1)], np.int32), sig, ri, rj) for k in range(n)]
+    # observed data from the true model (batched forward, no snapshots)
+    mt = dn.Model(p.replace(store_snapshots=0), vpt, vst, rhot, device=device)
+    st_ = [dn.Shot(mt, *sh) for sh in shots]
+    dn.run(st_)
+    obs = [(s.sections(dn.SEC_VX), s.sections(dn.SEC_VY)) for s in st_]
+    for s in st_:
+        s.close()
+    mt.close()
+    fp = ctypes.c_size_t()
+    pc = p.to_c()
+    dn._lib.check(dn._lib.lib.dn_shot_footprint(ctypes.byref(pc), len(ri), 1, ctypes.byref(fp)))
+    free, total = torch.cuda.mem_get_info(device)
+    batch = max(1, min(n, int(0.8 * free / fp.value) - 1))
+
+    def grad(params, idx):
+        m = dn.Model(params, *start, device=device)
+        L2, dev_ms = 0.0, 0.0
+        for b0 in range(0, len(idx), batch):
+            ss = [dn.Shot(m, *shots[k]) for k in idx[b0:b0 + batch]]
+            dn.run(ss, dn.MODE_FORWARD)
+            dev_ms += dn.last_run_stats()[0]
+            for s, k in zip(ss, idx[b0:b0 + batch]):
+                L2 += s.residual(obs[k][0], dn.SEC_VX) + s.residual(obs[k][1], dn.SEC_VY)
+            dn.run(ss, dn.MODE_ADJOINT)
+            dev_ms += dn.last_run_stats()[0]
+            for s in ss:
+                s.accumulate_gradient()
+                s.close()
+        g = m.gradient()
+        m.close()
+        return g, L2, dev_ms
+
+    grad(p, [0])                                   # warm-up (graphs, module load)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    g16, L2, dev_ms = grad(p, list(range(n)))
+    torch.cuda.synchronize(device)
+    wall = time.perf_counter() - t0
+    cells = n * p.nx * p.ny * p.nt * 2
+    g32, _, _ = grad(p.replace(snap_precision=dn.SNAP_F32), [0, n // 2])
+    g16s, _, _ = grad(p, [0, n // 2])
+    err = max(O.rel_l2(x, y) for x, y in zip(g16s, g32))
+    return {"workload": f"FWI gradient, elastic {p.nx}x{p.ny}, DH {p.dh} m, DT {p.dt} s, NT {p.nt}, FDORDER 8, "
+                        f"{n} shots x 400 receivers, FP16 snapshots every DTINV={p.dtinv} steps, "
+                        "starting model smoothed sigma 25 cells, observed data synthesised on the GPU",
+            "shots": n, "batch_shots": batch, "seconds": round(wall, 2),
+            "device_ms": round(dev_ms, 1), "shots_per_s": round(n / wall, 3),
+            "mcell_updates_per_s": round(cells / wall / 1e6, 1),
+            "misfit": L2, "fp16_vs_fp32_gradient_rel_l2": float(err)}
 
 
 def run_serving(a, device, mcells_per_s):
@@ -438,8 +525,9 @@ def run_reference(a, rank, world):
     return {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(ms, 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"batched viscoelastic forward: {p.nx}x{p.ny}, L=3, FDORDER 8 (bounded sample)",
-                       "parallelism": "host processes"},
+            "config": dict(workload_config(a, p, world), parallelism="host processes",
+                           sample="bounded: one single-rank process per host core, each on its own shot of this "
+                                  f"workload for {a.cpu_sample_nt} time steps"),
             "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 

@@ -882,13 +882,15 @@ __device__ __forceinline__ float block_max(float v, float *red)
     return m;
 }
 
-// scale s = 2^e with e chosen so max|x| / s lies in [2^14, 2^15)
+// scale s = 2^e with e chosen so max|x| / s lies in [2^14, 2^15); e >= -126 keeps
+// s normal and its inverse finite (a tile whose values are all below 2^-111 is
+// stored with s = 2^-126 and keeps fewer bits, which FP16 could not hold anyway)
 __device__ __forceinline__ float pow2_scale(float amax)
 {
     if (!(amax > 0.0f) || isinf(amax)) return 1.0f;
     int e;
     frexpf(amax, &e);   // amax = f * 2^e, f in [0.5, 1)
-    return ldexpf(1.0f, e - 15);
+    return ldexpf(1.0f, max(e - 15, -126));
 }
 
 static __global__ void k_snap_store(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)

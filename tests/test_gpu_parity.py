@@ -198,3 +198,19 @@ def test_forward_matches_reference_build():
     dn.run([s])
     np.testing.assert_array_equal(s.sections(0), rx)
     np.testing.assert_array_equal(s.sections(1), ry)
+
+
+@pytest.mark.parametrize("prec", [dn.SNAP_F16, dn.SNAP_BF16], ids=["fp16", "bf16"])
+def test_half_snapshots_of_tiny_wavefields_stay_finite(prec):
+    """A source 1e-40 times weaker: every snapshot tile's maximum is far below
+    2^-111, where a per-tile scale without a floor would overflow on inversion."""
+    p, model, src, rec = small_case(store_snapshots=1, snap_precision=prec, nt=300)
+    src = (src[0], src[1], src[2] * np.float32(1e-40)) + src[3:]
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run([s], dn.MODE_FORWARD)
+    syn = [s.sections(c) for c in (0, 1)]
+    s.set_residuals(syn[0], syn[1], None)
+    dn.run([s], dn.MODE_ADJOINT)
+    s.accumulate_gradient()
+    for g in m.gradient():
+        assert np.all(np.isfinite(g))
