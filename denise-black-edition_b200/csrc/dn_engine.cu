@@ -450,21 +450,72 @@ extern "C" int dn_model_params(const dn_model *m, dn_params *out)
 // ---------------------------------------------------------------------------
 // shots
 // ---------------------------------------------------------------------------
+// Tile shapes of new shots: rules set by dn_set_tile_shape (the autotuner of
+// denise_b200/tune.py measures them per FDORDER, L and grid size on the device),
+// the last matching rule winning; DN_TILE="WxZ" overrides everything; else the
+// 128 x 8 tile measured best for the 2000 x 600 batched workload (4-32 rows swept).
+struct TileRule {
+    int fdorder, L;
+    long long cells_min, cells_max;
+    int bx, zch;
+};
+static std::mutex g_tile_mu;
+static std::vector<TileRule> g_tile_rules;
+
+static bool tile_ok(int bx, int zch) { return bx >= 32 && bx <= 256 && (bx % 32) == 0 && zch >= 1 && zch <= 256; }
+
 static void tile_shape(const dn_params *p, int &bx, int &zch)
 {
-    // Tile shapes measured on B200 per grid; small grids favour short tiles
-    // (more CTAs), large ones long register streams.
-    (void)p;
     bx = 128;
-    zch = 8;   // measured best on B200 for the 2000 x 600 batched workload (4-32 swept)
+    zch = 8;
+    const long long cells = (long long)p->nx * p->ny;
+    {
+        std::lock_guard<std::mutex> lk(g_tile_mu);
+        for (const TileRule &r : g_tile_rules)
+            if (r.fdorder == p->fdorder && r.L == p->L && cells >= r.cells_min && cells <= r.cells_max) {
+                bx = r.bx;
+                zch = r.zch;
+            }
+    }
     const char *ev = getenv("DN_TILE");
     if (ev) {
         int a = 0, b = 0;
-        if (sscanf(ev, "%dx%d", &a, &b) == 2 && a >= 32 && a <= 256 && (a % 32) == 0 && b >= 1 && b <= 256) {
+        if (sscanf(ev, "%dx%d", &a, &b) == 2 && tile_ok(a, b)) {
             bx = a;
             zch = b;
         }
     }
+}
+
+extern "C" int dn_set_tile_shape(int fdorder, int L, long long cells_min, long long cells_max, int bx, int zch)
+{
+    if (fdorder < 2 || fdorder > 12 || (fdorder % 2) || L < 0 || L > DN_MAX_L || cells_min > cells_max)
+        return dn_fail(DN_EINVAL, "dn_set_tile_shape: bad class");
+    if (!tile_ok(bx, zch))
+        return dn_fail(DN_EINVAL, "dn_set_tile_shape: %d x %d (width a multiple of 32 up to 256, 1-256 rows)", bx, zch);
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    for (TileRule &r : g_tile_rules)
+        if (r.fdorder == fdorder && r.L == L && r.cells_min == cells_min && r.cells_max == cells_max) {
+            r.bx = bx;
+            r.zch = zch;
+            return DN_OK;
+        }
+    g_tile_rules.push_back({fdorder, L, cells_min, cells_max, bx, zch});
+    return DN_OK;
+}
+
+extern "C" int dn_clear_tile_shapes(void)
+{
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    g_tile_rules.clear();
+    return DN_OK;
+}
+
+extern "C" int dn_get_tile_shape(const dn_params *p, int *bx, int *zch)
+{
+    if (!p || !bx || !zch) return dn_fail(DN_EINVAL, "dn_get_tile_shape: null argument");
+    tile_shape(p, *bx, *zch);
+    return DN_OK;
 }
 
 static int shot_counts(const dn_params *p, int bx, int zch, int &tiles_x, int &tiles, int &nsnap)

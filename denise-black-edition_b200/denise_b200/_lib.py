@@ -130,6 +130,10 @@ SIGNATURES = {
     "dn_queue_add": (ctypes.c_int, [_vp, _vp, ctypes.c_int]),
     "dn_queue_step": (ctypes.c_int, [_vp, _P(_vp), _c_int_p, ctypes.c_int, _c_int_p]),
     "dn_queue_count": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
+    "dn_set_tile_shape": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong,
+                                         ctypes.c_int, ctypes.c_int]),
+    "dn_clear_tile_shapes": (ctypes.c_int, []),
+    "dn_get_tile_shape": (ctypes.c_int, [_P(Params), _c_int_p, _c_int_p]),
     "dn_dot": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _c_double_p]),
     "dn_lbfgs_create": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int, _P(_vp)]),
     "dn_lbfgs_destroy": (ctypes.c_int, [_vp]),

@@ -274,6 +274,16 @@ int dn_queue_add(dn_queue *q, dn_shot *s, int mode);
 int dn_queue_step(dn_queue *q, dn_shot **done, int *status, int cap, int *ndone);
 int dn_queue_count(const dn_queue *q, int *running, int *waiting);
 
+/* ---- tile shapes ------------------------------------------------------------
+ * Shots created after this call whose FDORDER and L match and whose nx*ny lies in
+ * [cells_min, cells_max] use tiles of bx columns (a multiple of 32, <= 256) by zch
+ * rows; the last matching rule wins; the environment variable DN_TILE="WxZ"
+ * overrides all rules.  Results do not depend on the tile shape. */
+int dn_set_tile_shape(int fdorder, int L, long long cells_min, long long cells_max, int bx, int zch);
+int dn_clear_tile_shapes(void);
+/* the tile shape a new shot with these parameters gets */
+int dn_get_tile_shape(const dn_params *p, int *bx, int *zch);
+
 /* ---- FWI outer loop (FP64) ------------------------------------------------- */
 /* Deterministic FP64 dot product of two device vectors (fixed reduction order). */
 int dn_dot(const double *a, const double *b, long long n, double *out);
