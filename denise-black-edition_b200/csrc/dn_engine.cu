@@ -170,6 +170,11 @@ struct dn_shot {
     int *d_flag = nullptr;
     int stored = 0;                // a mode-0 run with snapshots completed
     int correlated = 0;            // a mode-1 run completed
+    // checkpointed adjoint (ckpt_steps > 0): full states at segment starts, and the
+    // adjoint's own wavefield state (the forward state is recomputed per segment)
+    int nseg = 0;
+    char *dckpt = nullptr;         // nseg x state_bytes
+    char *dstate2 = nullptr;       // adjoint state, state_bytes
 };
 
 static size_t snap_elem_bytes(int prec) { return prec == DN_SNAP_F32 ? 4 : 2; }
@@ -191,6 +196,8 @@ static int validate_params(const dn_params *p)
     if (p->invmat1 != 1) return dn_fail(DN_ENOTSUP, "INVMAT1=%d is not built; use 1 (vp, vs, rho)", p->invmat1);
     if (p->grad_form != 1) return dn_fail(DN_ENOTSUP, "GRAD_FORM=%d is not built; use 1", p->grad_form);
     if (p->store_snapshots && p->dtinv < 1) return dn_fail(DN_EINVAL, "DTINV must be >= 1");
+    if (p->ckpt_steps < 0 || (p->ckpt_steps > 0 && (!p->store_snapshots || p->ckpt_steps % p->dtinv)))
+        return dn_fail(DN_EINVAL, "ckpt_steps must be 0 or a positive multiple of DTINV with snapshots stored");
     if (p->snap_precision < 0 || p->snap_precision > 2) return dn_fail(DN_EINVAL, "bad snapshot precision");
     if (p->seismo < 0 || p->seismo > 4) return dn_fail(DN_EINVAL, "SEISMO must be 0..4");
     if (p->L > 0 && !(p->ts > 0.0f) && p->free_surf)
@@ -523,6 +530,7 @@ static int shot_counts(const dn_params *p, int bx, int zch, int &tiles_x, int &t
     tiles_x = (p->nx + bx - 1) / bx;
     tiles = tiles_x * ((p->ny + zch - 1) / zch);
     nsnap = p->store_snapshots ? (int)ceil((float)p->nt / (float)p->dtinv) : 0;   // FD_PSV.c:82
+    if (p->store_snapshots && p->ckpt_steps > 0) nsnap = std::min(nsnap, p->ckpt_steps / p->dtinv);   // one segment
     return DN_OK;
 }
 
@@ -540,6 +548,11 @@ extern "C" int dn_shot_footprint(const dn_params *p, int ntr, int store, size_t 
     b += (size_t)9 * 2 * std::max(p->fw, 1) * std::max(p->nx, p->ny) * 4;
     b += (size_t)5 * p->nt * std::max(ntr, 1) * 4 + (size_t)3 * p->nt * std::max(ntr, 1) * 4;
     b += (size_t)nsnap * 5 * tiles * bx * zch * snap_elem_bytes(p->snap_precision);
+    if (store && p->ckpt_steps > 0) {   // checkpoints and the adjoint state
+        const size_t nseg = (p->nt + p->ckpt_steps - 1) / p->ckpt_steps;
+        b += (nseg + 1) * ((size_t)(7 + 3 * p->L) * L.plane * 4 + (size_t)9 * 2 * std::max(p->fw, 1) *
+                           std::max(p->nx, p->ny) * 4);
+    }
     b += (size_t)p->nx * p->ny * (3 * (p->grad_accum == DN_ACC_F64 ? 8 : 4) + 8);
     if (bytes) *bytes = b;
     return DN_OK;
@@ -651,6 +664,11 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
         ok = cudaMalloc(&s->d_snap, std::max(snap_n, (size_t)1) * snap_elem_bytes(p->snap_precision)) == cudaSuccess &&
              cudaMalloc(&s->d_snap_scale, std::max((size_t)s->nsnap * 5 * s->tiles, (size_t)1) * 4) == cudaSuccess;
     }
+    if (ok && p->store_snapshots && p->ckpt_steps > 0) {
+        s->nseg = (p->nt + p->ckpt_steps - 1) / p->ckpt_steps;
+        ok = cudaMalloc(&s->dckpt, s->state_bytes * s->nseg) == cudaSuccess &&
+             cudaMalloc(&s->dstate2, s->state_bytes) == cudaSuccess;
+    }
     if (!ok) {
         cudaGetLastError();
         dn_shot_destroy(s);
@@ -725,6 +743,8 @@ extern "C" int dn_shot_destroy(dn_shot *s)
     cudaFree(s->d_snap);
     cudaFree(s->d_snap_scale);
     cudaFree(s->d_acc);
+    cudaFree(s->dckpt);
+    cudaFree(s->dstate2);
     s->m->nshots--;
     delete s;
     return DN_OK;
@@ -1038,11 +1058,126 @@ static int graph_chunk(int maxnt)
     return std::min(k, maxnt);
 }
 
+// ---------------------------------------------------------------------------
+// checkpointed adjoint (ckpt_steps > 0)
+//
+// Forward (mode 0): the full state (fields, memory variables, CPML memory) is
+// copied aside at the start of every segment of ckpt_steps steps; no snapshot
+// is kept.  Adjoint (mode 1): for the segments from last to first, the forward
+// state is restored from the segment's checkpoint and the segment is recomputed
+// with its snapshots stored (slots relative to the segment), then the adjoint
+// steps whose mirrored forward steps lie in the segment run, in their own state.
+// The adjoint steps still run in increasing order and the recomputed forward
+// states are bit-identical, so the gradient equals the one with every snapshot
+// stored.  Direct launches: the grids that need checkpoints are large.
+// ---------------------------------------------------------------------------
+static Inst make_inst_state2(const dn_shot *s, int mode)
+{
+    Inst I = make_inst(s, mode);
+    const ptrdiff_t d = s->dstate2 - s->dstate;
+    auto mv = [d](float *&p) {
+        if (p) p = (float *)((char *)p + d);
+    };
+    mv(I.vx), mv(I.vy), mv(I.sxx), mv(I.syy), mv(I.sxy), mv(I.vxp1), mv(I.vyp1);
+    mv(I.r), mv(I.p), mv(I.q);
+    mv(I.psi_sxx_x), mv(I.psi_sxy_x), mv(I.psi_syy_y), mv(I.psi_sxy_y);
+    mv(I.psi_vxx), mv(I.psi_vyx), mv(I.psi_vyy), mv(I.psi_vxy), mv(I.psi_vxxs);
+    return I;
+}
+
+static int run_ckpt(dn_shot *s, int mode, double &ms_total, long long &nl)
+{
+    dn_shot *arr[1] = {s};
+    LaunchCfg c, cf;
+    int st = check_batch(arr, 1, mode, c);
+    if (!st && mode == 1) st = check_batch(arr, 1, 0, cf);
+    if (st) return st;
+    DevState *ds;
+    st = dev_state(s->m->device, &ds);
+    if (st) return st;
+    CU(cudaSetDevice(s->m->device));
+    st = prepare_launch(c);
+    if (st) return st;
+    const int Ls = s->p.ckpt_steps, nt = s->p.nt, nseg = s->nseg, per = Ls / s->p.dtinv;
+    const size_t sb = s->state_bytes;
+    cudaStream_t sm = ds->stream;
+    std::vector<Inst> h;
+    if (mode != 1) {
+        h.push_back(make_inst(s, mode));
+        h[0].store = 0;
+    } else {
+        for (int g = 0; g < nseg; g++) {
+            Inst f = make_inst(s, 0), a = make_inst_state2(s, 1);
+            f.snap_base = a.snap_base = g * per;
+            f.nsnap = a.nsnap = s->nsnap;   // the segment buffer's slots (fewer than per when NT < ckpt_steps)
+            h.push_back(f);
+            h.push_back(a);
+        }
+    }
+    Inst *d = nullptr;
+    CU(cudaMalloc(&d, sizeof(Inst) * h.size()));
+    cudaError_t e = cudaMemcpyAsync(d, h.data(), sizeof(Inst) * h.size(), cudaMemcpyHostToDevice, sm);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sm);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return dn_fail(DN_EDEVICE, "checkpointed run: %s", cudaGetErrorString(e));
+    }
+    if (mode != 1) {
+        st = zero_for_run(s, mode, sm);
+    } else if (cudaMemsetAsync(s->dstate2, 0, sb, sm) != cudaSuccess ||
+               cudaMemsetAsync(s->d_flag, 0, 4, sm) != cudaSuccess) {
+        st = dn_fail(DN_EDEVICE, "checkpointed adjoint: state reset failed");
+    }
+    if (st) {
+        cudaFree(d);
+        return st;
+    }
+    cudaEventRecord(ds->ev0, sm);
+    if (mode != 1) {
+        for (int g = 0; g < nseg; g++) {
+            if (mode == 0) cudaMemcpyAsync(s->dckpt + sb * g, s->dstate, sb, cudaMemcpyDeviceToDevice, sm);
+            for (int k = g * Ls + 1; k <= std::min((g + 1) * Ls, nt); k++) launch_step(c, sm, d, ds->d_zero, k, nl);
+        }
+    } else {
+        for (int g = nseg - 1; g >= 0; g--) {
+            const int a = g * Ls + 1, b = std::min((g + 1) * Ls, nt);
+            cudaMemcpyAsync(s->dstate, s->dckpt + sb * g, sb, cudaMemcpyDeviceToDevice, sm);
+            for (int k = a; k <= b; k++) launch_step(cf, sm, d + 2 * g, ds->d_zero, k, nl);
+            for (int k = nt - b + 1; k <= nt - a + 1; k++) launch_step(c, sm, d + 2 * g + 1, ds->d_zero, k, nl);
+        }
+    }
+    cudaEventRecord(ds->ev1, sm);
+    cudaError_t le = cudaGetLastError();
+    st = finish_run(arr, 1, mode, sm);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ds->ev0, ds->ev1);
+    ms_total += ms;
+    cudaFree(d);
+    if (le != cudaSuccess) return dn_fail(DN_EDEVICE, "kernel launch failed: %s", cudaGetErrorString(le));
+    return st;
+}
+
 extern "C" int dn_run(dn_shot *const *shots, int n, int mode)
 {
+    if (shots && n > 0 && shots[0] && shots[0]->nseg > 0) {
+        // checkpointed shots run one after the other
+        double ms = 0.0;
+        long long nl = 0;
+        for (int k = 0; k < n; k++) {
+            if (!shots[k] || shots[k]->nseg == 0)
+                return dn_fail(DN_EINVAL, "dn_run: checkpointed and stored-snapshot shots cannot share a batch");
+            int st = run_ckpt(shots[k], mode, ms, nl);
+            if (st) return st;
+        }
+        g_last_ms = ms;
+        g_last_launches = nl;
+        return DN_OK;
+    }
     LaunchCfg c;
     int st = check_batch(shots, n, mode, c);
     if (st) return st;
+    for (int k = 0; k < n; k++)
+        if (shots[k]->nseg > 0) return dn_fail(DN_EINVAL, "dn_run: checkpointed and stored-snapshot shots cannot share a batch");
     const int device = shots[0]->m->device;
     DevState *ds;
     st = dev_state(device, &ds);
@@ -1167,6 +1302,7 @@ static int run_direct(dn_shot *s, int mode, int nt0, int nt1, bool zero)
 extern "C" int dn_run_plain(dn_shot *s, int mode)
 {
     if (!s) return dn_fail(DN_EINVAL, "null shot");
+    if (s->nseg > 0) return dn_run(&s, 1, mode);
     return run_direct(s, mode, 1, s->p.nt, true);
 }
 
@@ -1174,6 +1310,7 @@ extern "C" int dn_run_steps(dn_shot *s, int mode, int nt0, int nt1)
 {
     if (!s) return dn_fail(DN_EINVAL, "null shot");
     if (nt0 < 1 || nt1 > s->p.nt || nt0 > nt1) return dn_fail(DN_EINVAL, "bad step range %d..%d", nt0, nt1);
+    if (s->nseg > 0) return dn_fail(DN_ENOTSUP, "dn_run_steps: not for checkpointed shots");
     return run_direct(s, mode, nt0, nt1, nt0 == 1);
 }
 
@@ -1266,6 +1403,7 @@ extern "C" int dn_queue_add(dn_queue *q, dn_shot *s, int mode)
     for (const QSlot &x : q->pending)
         if (x.s == s) return dn_fail(DN_ESTATE, "dn_queue_add: shot already waiting in this queue");
     if (mode == 1 && !s->stored) return dn_fail(DN_ESTATE, "dn_queue_add: adjoint run without a stored forward run");
+    if (s->nseg > 0) return dn_fail(DN_ENOTSUP, "dn_queue_add: checkpointed shots run through dn_run");
     q->pending.push_back({s, mode, 0});
     return DN_OK;
 }
@@ -1447,6 +1585,7 @@ extern "C" int dn_shot_get_field(const dn_shot *s, int field, float *out)
 extern "C" int dn_shot_get_snapshot(const dn_shot *s, int k, int field, float *out)
 {
     if (!s || !out) return dn_fail(DN_EINVAL, "null argument");
+    if (s->nseg > 0) return dn_fail(DN_ENOTSUP, "dn_shot_get_snapshot: a checkpointed shot keeps no snapshot set");
     if (k < 0 || k >= s->nsnap || field < 0 || field > 4) return dn_fail(DN_EINVAL, "bad snapshot index");
     const dn_params &p = s->p;
     const size_t tc = (size_t)s->bx * s->zch;

@@ -83,6 +83,7 @@ struct Inst {
     float rdh;                        // RN(1 / DH)
     int fastdiv;                      // division by DH through div_markstein (verified for this DH)
     int t0;                           // step base when the instance joined: its step is *ntb + off - t0
+    int snap_base;                    // snapshot k lives in slot k - snap_base (checkpointed segments)
 };
 
 // ---------------------------------------------------------------------------
@@ -898,8 +899,8 @@ static __global__ void k_snap_store(const Inst *__restrict__ insts, const int *_
     const Inst &I = insts[blockIdx.y];
     const int nt = *ntb + off - I.t0;   // the instance's own time step
     if (nt < 1 || nt > I.nt || I.mode != 0 || !I.store || ((nt - 1) % I.dtinv) != 0) return;
-    const int k = (nt - 1) / I.dtinv;
-    if (k >= I.nsnap) return;
+    const int k = (nt - 1) / I.dtinv - I.snap_base;
+    if (k < 0 || k >= I.nsnap) return;
     const int b = blockIdx.x;
     if (b >= I.tiles) return;
     __shared__ float red[32];
@@ -966,8 +967,8 @@ static __global__ void k_correlate(const Inst *__restrict__ insts, const int *__
     if (nt < 1 || nt > I.nt || I.mode != 1) return;
     const int nf = I.nt - nt + 1;   // mirrored forward step
     if (((nf - 1) % I.dtinv) != 0) return;
-    const int k = (nf - 1) / I.dtinv;
-    if (k >= I.nsnap) return;
+    const int k = (nf - 1) / I.dtinv - I.snap_base;
+    if (k < 0 || k >= I.nsnap) return;
     const int b = blockIdx.x;
     if (b >= I.tiles) return;
     const int tx = b % I.tiles_x, tz = b / I.tiles_x;

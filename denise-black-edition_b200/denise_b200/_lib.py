@@ -60,6 +60,7 @@ class Params(ctypes.Structure):
         ("seismo", ctypes.c_int), ("dtinv", ctypes.c_int), ("eprecond", ctypes.c_int),
         ("store_snapshots", ctypes.c_int), ("snap_precision", ctypes.c_int),
         ("grad_accum", ctypes.c_int), ("arith", ctypes.c_int), ("honor_q", ctypes.c_int),
+        ("ckpt_steps", ctypes.c_int),
     ]
 
 

@@ -57,6 +57,7 @@ class PsvParams:
     grad_accum: int = _lib.ACC_F32
     arith: int = _lib.ARITH_EXACT
     honor_q: int = 0
+    ckpt_steps: int = 0
 
     def to_c(self):
         p = _lib.Params()

@@ -118,6 +118,10 @@ typedef struct dn_params {
     int grad_accum;          /* DN_ACC_* */
     int arith;               /* DN_ARITH_* */
     int honor_q;             /* 0: Q forced to 30 as readmod_visc_PSV.c:106-107; 1: use the qp/qs arrays */
+    int ckpt_steps;          /* 0: store every snapshot of the forward run; > 0 (a multiple of dtinv):
+                                checkpointed adjoint - the forward run keeps the full state every
+                                ckpt_steps steps and the adjoint recomputes one segment of snapshots
+                                at a time (no counterpart in the reference, which stores all) */
 } dn_params;
 
 /* One shot's acquisition: sources (psource/update_v injection points) and
