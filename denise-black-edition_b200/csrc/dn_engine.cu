@@ -1795,10 +1795,10 @@ extern "C" int dn_profile_steps(dn_shot *const *shots, int n, int mode, int nste
 // data residual of a forward-run shot into its adjoint sources (calc_res_PSV +
 // calc_res, LNORM 2): obs [ntr][nt] host, comp DN_SEC_VX / VY / P
 // ---------------------------------------------------------------------------
-extern "C" int dn_residual_l2_launch(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt,
-                                     int grad_form, double *scratch, cudaStream_t stream);
+extern "C" int dn_adjoint_source_launch(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt,
+                                        int grad_form, int rtm, double *scratch, cudaStream_t stream);
 
-extern "C" int dn_shot_residual(dn_shot *s, int comp, const float *obs, double *l2)
+static int shot_source(dn_shot *s, int comp, const float *obs, double *l2, int rtm)
 {
     if (!s || !obs) return dn_fail(DN_EINVAL, "dn_shot_residual: null argument");
     if (comp != DN_SEC_VX && comp != DN_SEC_VY && comp != DN_SEC_P)
@@ -1822,8 +1822,8 @@ extern "C" int dn_shot_residual(dn_shot *s, int comp, const float *obs, double *
     double h = 0.0;
     cudaError_t e = cudaMemcpyAsync(dobs, obs, n * 4, cudaMemcpyHostToDevice, ds->stream);
     if (e == cudaSuccess)
-        st = dn_residual_l2_launch(s->d_sec + (size_t)comp * nt * ntr, dobs, s->d_res + k * rs, ntr, nt, s->p.dt,
-                                   s->p.grad_form, scratch, ds->stream);
+        st = dn_adjoint_source_launch(s->d_sec + (size_t)comp * nt * ntr, dobs, s->d_res + k * rs, ntr, nt, s->p.dt,
+                                      s->p.grad_form, rtm, scratch, ds->stream);
     else st = dn_fail(DN_EDEVICE, "dn_shot_residual: %s", cudaGetErrorString(e));
     if (!st) {
         e = cudaMemcpyAsync(&h, scratch + ntr, sizeof(double), cudaMemcpyDeviceToHost, ds->stream);
@@ -1836,4 +1836,14 @@ extern "C" int dn_shot_residual(dn_shot *s, int comp, const float *obs, double *
     s->has_res[k] = 1;
     if (l2) *l2 = h;
     return DN_OK;
+}
+
+extern "C" int dn_shot_residual(dn_shot *s, int comp, const float *obs, double *l2)
+{
+    return shot_source(s, comp, obs, l2, 0);
+}
+
+extern "C" int dn_shot_rtm_source(dn_shot *s, int comp, const float *obs)
+{
+    return shot_source(s, comp, obs, nullptr, 1);
 }

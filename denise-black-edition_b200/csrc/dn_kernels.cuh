@@ -158,13 +158,14 @@ __device__ __forceinline__ bool tile_of(const Inst &I, TileLoc &t)
 // mode 1: vxp1 += DT * vx with the old vx (:455-457).
 // Each thread streams down its column; the loads of row j+1 are issued before
 // row j is computed so two rows of DRAM traffic are in flight per thread.
-// The register caps of the stencil kernels (velocity 48, elastic stress 64,
-// viscoelastic stress 80 registers at FDORDER 8, no spills) were measured
-// faster than the uncapped 74 / 73 / 120: the kernels are bound by the loads
-// in flight per SM, so resident warps count more than registers per thread.
+// The register caps of the stencil kernels (velocity 40, elastic stress 64,
+// viscoelastic stress 80 registers at FDORDER 8) were measured fastest of the
+// caps tried (velocity 40/48/56/74, stresses 48-96): the kernels are bound by
+// the loads in flight per SM, so resident warps count more than registers per
+// thread (the velocity kernel spills 48 bytes at 40 and is still 4% faster).
 // ===========================================================================
 template <int R, bool X>
-__global__ void __launch_bounds__(256, 5) k_update_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+__global__ void __maxnreg__(40) k_update_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
     const int nt = *ntb + off - I.t0;   // the instance's own time step

@@ -17,8 +17,11 @@
 
 namespace {
 
+// rtm = 1: the reverse-time-migration source of calc_res.c:436/441 (MODE 2): the
+// observed trace itself (first sample replaced by the synthetic one), integrated
+// for GRAD_FORM 1, instead of the difference
 __global__ void k_residual_l2(const float *__restrict__ syn, const float *__restrict__ obs, float *__restrict__ res,
-                              int ntr, int nt, float dt, int grad_form, double *__restrict__ part)
+                              int ntr, int nt, float dt, int grad_form, int rtm, double *__restrict__ part)
 {
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= ntr) return;
@@ -29,7 +32,7 @@ __global__ void k_residual_l2(const float *__restrict__ syn, const float *__rest
     for (int t = 0; t < nt; t++) {
         const float s = syn[(size_t)t * ntr + l];
         const float d = t == 0 ? s : ob[t];
-        const float diff = __fsub_rn(s, d);
+        const float diff = rtm ? d : __fsub_rn(s, d);
         float r;
         if (grad_form == 1) {
             intseis = __fadd_rn(intseis, __fmul_rn(dt, diff));
@@ -54,14 +57,20 @@ __global__ void k_sum_partials(const double *__restrict__ part, int n, double *_
 }   // namespace
 
 // Launches the two kernels on `stream` with `scratch` holding ntr + 1 doubles.
-extern "C" int dn_residual_l2_launch(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt,
-                                     int grad_form, double *scratch, cudaStream_t stream)
+extern "C" int dn_adjoint_source_launch(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt,
+                                        int grad_form, int rtm, double *scratch, cudaStream_t stream)
 {
-    k_residual_l2<<<(ntr + 127) / 128, 128, 0, stream>>>(syn_tm, obs, res, ntr, nt, dt, grad_form, scratch);
+    k_residual_l2<<<(ntr + 127) / 128, 128, 0, stream>>>(syn_tm, obs, res, ntr, nt, dt, grad_form, rtm, scratch);
     k_sum_partials<<<1, 1, 0, stream>>>(scratch, ntr, scratch + ntr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "residual kernels: %s", cudaGetErrorString(e));
     return DN_OK;
+}
+
+extern "C" int dn_residual_l2_launch(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt,
+                                     int grad_form, double *scratch, cudaStream_t stream)
+{
+    return dn_adjoint_source_launch(syn_tm, obs, res, ntr, nt, dt, grad_form, 0, scratch, stream);
 }
 
 extern "C" int dn_residual_l2(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt,

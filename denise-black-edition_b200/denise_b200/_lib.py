@@ -126,6 +126,7 @@ SIGNATURES = {
     "dn_residual_l2": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
                                       _c_double_p]),
     "dn_shot_residual": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p, _c_double_p]),
+    "dn_shot_rtm_source": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p]),
     "dn_queue_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _P(_vp)]),
     "dn_queue_destroy": (ctypes.c_int, [_vp]),
     "dn_queue_add": (ctypes.c_int, [_vp, _vp, ctypes.c_int]),

@@ -237,6 +237,12 @@ class Shot:
         check(lib.dn_shot_residual(self.handle, comp, fptr(o), ctypes.byref(l2)))
         return l2.value
 
+    def rtm_source(self, obs, comp=_lib.SEC_VX):
+        """Reverse-time-migration source (calc_res MODE 2): the observed data
+        itself, time-reversed and integrated, as this shot's adjoint source."""
+        o = _f32(obs, (self.ntr, self.model.params.nt))
+        check(lib.dn_shot_rtm_source(self.handle, comp, fptr(o)))
+
     def accumulate_gradient(self):
         check(lib.dn_shot_accumulate_gradient(self.handle))
 

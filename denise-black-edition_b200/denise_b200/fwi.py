@@ -203,3 +203,29 @@ class FWI:
             self.vp, self.vs, self.rho, _ = mat_update(self.vp, self.vs, self.rho, *d, eps, self.limits, it)
         self.history.append({"iteration": it, "misfit": L2, "eps": eps, "L2t": L2t, "epst": epst, "found": found})
         return L2
+
+
+def rtm_image(params, model, shots, obs, device=0, batch=None):
+    """Reverse-time migration (RTM_PSV.c): per shot, a forward run with
+    snapshots, the observed data as adjoint source (dn_shot_rtm_source) and the
+    adjoint run; the images are the stacked vp and vs gradients (the P and S
+    images RTM_PSV_out.c writes).  `params` must store snapshots.  Returns
+    (P image, S image) in file order."""
+    from . import api as dn
+
+    m = dn.Model(params, *model[:3], model[3] if params.L else None, model[4] if params.L else None,
+                 device=device)
+    batch = batch or len(shots)
+    for b0 in range(0, len(shots), batch):
+        ss = [dn.Shot(m, *sh[:5]) for sh in shots[b0:b0 + batch]]
+        dn.run(ss, _lib.MODE_FORWARD)
+        for s, (ovx, ovy) in zip(ss, obs[b0:b0 + batch]):
+            s.rtm_source(ovx, _lib.SEC_VX)
+            s.rtm_source(ovy, _lib.SEC_VY)
+        dn.run(ss, _lib.MODE_ADJOINT)
+        for s in ss:
+            s.accumulate_gradient()
+            s.close()
+    g = m.gradient()
+    m.close()
+    return g[0], g[1]

@@ -252,6 +252,12 @@ int dn_residual_l2_noalloc(const float *syn_tm, const float *obs, float *res, in
  * comp = DN_SEC_VX / DN_SEC_VY / DN_SEC_P; the residual becomes the shot's
  * adjoint source of that component (calc_res_PSV.c), l2 the component's misfit. */
 int dn_shot_residual(dn_shot *s, int comp, const float *obs, double *l2);
+/* Reverse-time migration (MODE 2): the shot's adjoint source of `comp` becomes the
+ * observed data itself, time-reversed and (GRAD_FORM 1) time-integrated, as
+ * calc_res.c:436/441 forms it for MODE 2; the adjoint run then images instead
+ * of computing a gradient (RTM_PSV.c: P image = the vp gradient, S image = the
+ * vs gradient of dn_model_get_gradient). */
+int dn_shot_rtm_source(dn_shot *s, int comp, const float *obs);
 
 /* Per-kernel device time of `nsteps` time steps of a batch (direct launches with
  * CUDA events between kernels, for measurement only; leaves the shots' results
