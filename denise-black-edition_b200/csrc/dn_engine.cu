@@ -1629,9 +1629,38 @@ extern "C" int dn_shot_get_snapshot(const dn_shot *s, int k, int field, float *o
 // ---------------------------------------------------------------------------
 // gradient assembly: ass_gradPSV.c:29-150 (INVMAT1 1, GRAD_FORM 1) + stacking
 // ---------------------------------------------------------------------------
+// Energy weight of a shot (eprecond1.c): EPRECOND 1, We = sqrt(Ws Wr); EPRECOND 3,
+// We = sqrt(Ws) (asinh((xmax - x) / y) - asinh((xmin - x) / y)) with x = i DH,
+// y = j DH, xmin = DH, xmax = NX DH (the receiver Green's function approximation
+// of Plessix and Mulder 2004); its maximum is kept as float bits (We >= 0, so
+// the bit patterns order like the values).
+__global__ void k_energy_weight(int nx, int ny, int ep, float dh, const float *Ws, const float *Wr, float *We,
+                                unsigned *maxbits)
+{
+    const long long n = (long long)nx * ny;
+    const float xmin = dh, xmax = __fmul_rn((float)nx, dh);
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(w / nx) + 1, i = (int)(w % nx) + 1;
+        float we;
+        if (ep == 1) {
+            we = (float)sqrt((double)__fmul_rn(Ws[w], Wr[w]));
+        } else {
+            const float x = __fmul_rn((float)i, dh), y = __fmul_rn((float)j, dh);
+            const double a = asinh((double)__fdiv_rn(__fsub_rn(xmax, x), y));
+            const double b = asinh((double)__fdiv_rn(__fsub_rn(xmin, x), y));
+            we = (float)(sqrt((double)Ws[w]) * (a - b));
+        }
+        We[w] = we;
+        atomicMax(maxbits, __float_as_uint(we));
+    }
+}
+
+// We: energy weights (or null: no preconditioning); we_add = EPSILON_WE max(We);
+// c: the C_vp, C_vs, C_rho of grad_obj_psv.c:230-236
 __global__ void k_ass_grad(int nx, int ny, int pitch, const float *rho, const float *vp, const float *vs,
                            const float *gmuss, const float *glamss, const void *wc, const void *wcu, const void *wcr,
-                           int acc64, float DT, void *gsum, int out64)
+                           int acc64, float DT, void *gsum, int out64, const float *We, const unsigned *maxbits,
+                           float cvp, float cvs, float crho)
 {
     const long long n = (long long)nx * ny;
     for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x) {
@@ -1656,6 +1685,12 @@ __global__ void k_ass_grad(int nx, int ny, int pitch, const float *rho, const fl
             gvp = fvp;
             gvs = fvs;
             grho = frho;
+            if (We) {   // grad_obj_psv.c:230-236, float
+                const float wr = __fadd_rn(We[w], __fmul_rn(0.005f, __uint_as_float(*maxbits)));
+                gvp = __fdiv_rn(fvp, __fmul_rn(__fmul_rn(wr, cvp), cvp));
+                gvs = cvs == 0.0f ? 0.0f : __fdiv_rn(fvs, __fmul_rn(__fmul_rn(wr, cvs), cvs));
+                grho = __fdiv_rn(frho, __fmul_rn(__fmul_rn(wr, crho), crho));
+            }
         } else {
             const double ws = ((const double *)wc)[w], wus = ((const double *)wcu)[w], wrs = ((const double *)wcr)[w];
             double lam = -(double)DT * ws;
@@ -1668,6 +1703,12 @@ __global__ void k_ass_grad(int nx, int ny, int pitch, const float *rho, const fl
             gvs = -4.0 * (double)r * (double)u * lam + 2.0 * (double)r * (double)u * mu;
             const double rs = -(double)DT * wrs;
             grho = ((double)pi * pi - 2.0 * (double)u * u) * lam + (double)u * u * mu + rs;
+            if (We) {
+                const double wr = (double)We[w] + 0.005 * (double)__uint_as_float(*maxbits);
+                gvp /= wr * cvp * cvp;
+                gvs = cvs == 0.0f ? 0.0 : gvs / (wr * cvs * cvs);
+                grho /= wr * crho * crho;
+            }
         }
         if (out64) {
             double *g = (double *)gsum;
@@ -1683,10 +1724,13 @@ __global__ void k_ass_grad(int nx, int ny, int pitch, const float *rho, const fl
     }
 }
 
-extern "C" int dn_shot_accumulate_gradient(dn_shot *s)
+static int accumulate(dn_shot *s, bool precond, float cvp, float cvs, float crho)
 {
     if (!s) return dn_fail(DN_EINVAL, "null shot");
     if (!s->correlated) return dn_fail(DN_ESTATE, "dn_shot_accumulate_gradient: no completed adjoint run");
+    const int ep = s->p.eprecond;
+    if (precond && ep != 1 && ep != 3)
+        return dn_fail(DN_EINVAL, "energy preconditioning needs EPRECOND 1 or 3 in the shot's parameters (got %d)", ep);
     dn_model *m = s->m;
     DevState *ds;
     int st = dev_state(m->device, &ds);
@@ -1694,12 +1738,33 @@ extern "C" int dn_shot_accumulate_gradient(dn_shot *s)
     CU(cudaSetDevice(m->device));
     const long long n = (long long)s->p.nx * s->p.ny;
     int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+    char *buf = nullptr;
+    float *We = nullptr;
+    unsigned *maxbits = nullptr;
+    if (precond) {
+        CU(cudaMalloc(&buf, carve_size(n, 4) + 256));
+        We = (float *)buf;
+        maxbits = (unsigned *)(buf + carve_size(n, 4));
+        CU(cudaMemsetAsync(maxbits, 0, 4, ds->stream));
+        k_energy_weight<<<blocks, 256, 0, ds->stream>>>(s->p.nx, s->p.ny, ep, s->p.dh, (const float *)acc_ptr(s, 3),
+                                                        (const float *)acc_ptr(s, 4), We, maxbits);
+    }
     k_ass_grad<<<blocks, 256, 0, ds->stream>>>(s->p.nx, s->p.ny, m->lay.pitch, m->field(MF_RHO), m->field(MF_VP),
                                                m->field(MF_VS), m->field(MF_GMUSS), m->field(MF_GLAMSS), acc_ptr(s, 0),
-                                               acc_ptr(s, 1), acc_ptr(s, 2), s->acc64, s->p.dt, m->dgrad, m->grad64);
-    CU(cudaGetLastError());
-    CU(cudaStreamSynchronize(ds->stream));
+                                               acc_ptr(s, 1), acc_ptr(s, 2), s->acc64, s->p.dt, m->dgrad, m->grad64,
+                                               We, maxbits, cvp, cvs, crho);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ds->stream);
+    cudaFree(buf);
+    if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "gradient assembly: %s", cudaGetErrorString(e));
     return DN_OK;
+}
+
+extern "C" int dn_shot_accumulate_gradient(dn_shot *s) { return accumulate(s, false, 0.0f, 0.0f, 0.0f); }
+
+extern "C" int dn_shot_accumulate_gradient_precond(dn_shot *s, float c_vp, float c_vs, float c_rho)
+{
+    return accumulate(s, true, c_vp, c_vs, c_rho);
 }
 
 extern "C" int dn_model_get_gradient(const dn_model *m, float *g_vp, float *g_vs, float *g_rho)

@@ -116,6 +116,7 @@ SIGNATURES = {
     "dn_shot_get_sections": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p]),
     "dn_shot_set_residuals": (ctypes.c_int, [_vp, _c_float_p, _c_float_p, _c_float_p]),
     "dn_shot_accumulate_gradient": (ctypes.c_int, [_vp]),
+    "dn_shot_accumulate_gradient_precond": (ctypes.c_int, [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float]),
     "dn_model_get_gradient": (ctypes.c_int, [_vp, _c_float_p, _c_float_p, _c_float_p]),
     "dn_model_zero_gradient": (ctypes.c_int, [_vp]),
     "dn_shot_get_field": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p]),

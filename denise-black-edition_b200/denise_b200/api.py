@@ -246,6 +246,10 @@ class Shot:
     def accumulate_gradient(self):
         check(lib.dn_shot_accumulate_gradient(self.handle))
 
+    def accumulate_gradient_precond(self, c_vp, c_vs, c_rho):
+        """ass_gradPSV with the per-shot energy preconditioning (EPRECOND 1 or 3)."""
+        check(lib.dn_shot_accumulate_gradient_precond(self.handle, float(c_vp), float(c_vs), float(c_rho)))
+
     def field(self, fid):
         out = np.zeros((self.model.params.nx, self.model.params.ny), np.float32)
         check(lib.dn_shot_get_field(self.handle, fid, fptr(out)))

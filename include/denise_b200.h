@@ -211,6 +211,13 @@ int dn_shot_set_residuals(dn_shot *s, const float *vxdiff, const float *vydiff, 
 /* ass_gradPSV (src/PSV/ass_gradPSV.c:10-152) of this shot's correlation, then
  * added to the model's stacked gradient (grad_obj_psv.c:253-261). */
 int dn_shot_accumulate_gradient(dn_shot *s);
+/* The same with the per-shot energy preconditioning of grad_obj_psv.c:218-240
+ * (eprecond1.c): the shot must have run with params.eprecond 1 (We = sqrt(Ws Wr),
+ * forward and adjoint energies) or 3 (We = sqrt(Ws) times the asinh receiver
+ * term); We += 0.005 max(We); the shot's vp, vs, rho gradients are divided by
+ * We c^2 with c = c_vp, c_vs, c_rho (the reference's model averages; c_vs = 0
+ * zeroes the vs gradient) before they are stacked. */
+int dn_shot_accumulate_gradient_precond(dn_shot *s, float c_vp, float c_vs, float c_rho);
 /* The model's stacked gradients (waveconv, waveconv_u, waveconv_rho) in file order. */
 int dn_model_get_gradient(const dn_model *m, float *g_vp, float *g_vs, float *g_rho);
 int dn_model_zero_gradient(dn_model *m);

@@ -512,3 +512,26 @@ int refh_mat_change(int nx, int ny, const float *vp, const float *vs, const floa
     free_matrix(Gr, 1, ny, 1, nx);
     return 0;
 }
+
+/* ass_gradPSV followed by the per-shot energy preconditioning of
+ * grad_obj_psv.c:218-240 (eprecond1 with the run's Ws/Wr; EPRECOND from set-up) */
+extern float C_vp, C_vs, C_rho;
+int refh_ass_grad_ep(const float *c3, float *gvp, float *gvs, float *grho)
+{
+    ass_gradPSV(&FWI, &M, 1);
+    C_vp = c3[0];
+    C_vs = c3[1];
+    C_rho = c3[2];
+    eprecond1(We, Ws, Wr);
+    for (int i = 1; i <= NX; i++)
+        for (int j = 1; j <= NY; j++) {
+            FWI.waveconv_shot[j][i] = FWI.waveconv_shot[j][i] / (We[j][i] * C_vp * C_vp);
+            FWI.waveconv_u_shot[j][i] = FWI.waveconv_u_shot[j][i] / (We[j][i] * C_vs * C_vs);
+            if (C_vs == 0.0) FWI.waveconv_u_shot[j][i] = 0.0;
+            FWI.waveconv_rho_shot[j][i] = FWI.waveconv_rho_shot[j][i] / (We[j][i] * C_rho * C_rho);
+        }
+    to_file(FWI.waveconv_shot, gvp);
+    to_file(FWI.waveconv_u_shot, gvs);
+    to_file(FWI.waveconv_rho_shot, grho);
+    return 0;
+}

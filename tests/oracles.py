@@ -212,6 +212,13 @@ class Reference:
         self.lib.refh_ass_grad(*[x.ctypes.data_as(_f) for x in g])
         return tuple(g)
 
+    def ass_grad_ep(self, c_vp, c_vs, c_rho):
+        """ass_gradPSV + the per-shot energy preconditioning (EPRECOND of the set-up)."""
+        g = [np.zeros((self.p.nx, self.p.ny), np.float32) for _ in range(3)]
+        c = np.array([c_vp, c_vs, c_rho], np.float32)
+        self.lib.refh_ass_grad_ep(c.ctypes.data_as(_f), *[x.ctypes.data_as(_f) for x in g])
+        return tuple(g)
+
 
 def run_isolated(fn, *args, timeout=600):
     """Runs fn(*args) in a fresh spawned process (the reference keeps globals).
