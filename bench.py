@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--serve-scale", type=float, default=1.0, help="shrinks NX, NZ and NT of served requests")
     ap.add_argument("--gradient-shots", type=int, default=32,
                     help="shots of the FWI-gradient measurement (1700x500, NT 4000, FP16 snapshots; 0: skip)")
+    ap.add_argument("--fwi-large-shots", type=int, default=0,
+                    help="shots of a sample of the 8000x2000, NT 12000 FWI iteration (0: skip)")
     ap.add_argument("--elastic-nt", type=int, default=1000,
                     help="NT of the elastic batch measured beside the viscoelastic one (0: skip)")
     return ap.parse_args()
@@ -289,6 +291,12 @@ def run_ours(a, rank, world, local_rank):
                 s_.close()
                 m_.close()
             gradient = run_gradient(a, device)
+        fwi_large = None
+        if a.fwi_large_shots > 0:
+            for m_, s_ in pairs:
+                s_.close()
+                m_.close()
+            fwi_large = run_fwi_large(a, device)
         serving = None
         if a.serve_requests > 0:
             for m_, s_ in pairs:       # free the batch's HBM for the served requests
@@ -317,6 +325,8 @@ def run_ours(a, rank, world, local_rank):
             result["serving"] = serving
         if gradient:
             result["gradient"] = gradient
+        if fwi_large:
+            result["fwi_large"] = fwi_large
         if e2e:
             result["e2e"] = e2e
         if cpu:
@@ -437,6 +447,65 @@ def run_gradient(a, device):
             "device_ms": round(dev_ms, 1), "shots_per_s": round(n / wall, 3),
             "mcell_updates_per_s": round(cells / wall / 1e6, 1),
             "misfit": L2, "fp16_vs_fp32_gradient_rel_l2": float(err)}
+
+
+def run_fwi_large(a, device):
+    """A sample of the large FWI iteration: elastic 8000 x 2000, DH 2.5 m, DT 0.2 ms
+    (0.25 ms breaks the CFL limit of this model), NT 12000, FDORDER 8, shots of the
+    96-shot line with 1600 receivers; true model = the seeded family (seed 4) plus a
+    5500 m/s ellipse, starting model smoothed with sigma 25 cells; one FWI iteration
+    with FP16 snapshots every 4 steps and checkpointed adjoints (segments of 400
+    steps), the FP64 L-BFGS direction, the parabolic step search and the update."""
+    import denise_b200 as dn
+    from denise_b200 import fwi, synth
+    from denise_b200.api import PsvParams
+
+    n = a.fwi_large_shots
+    p = PsvParams(nx=8000, ny=2000, dh=2.5, dt=2e-4, nt=12000, fdorder=8, fw=20, free_surf=1, ts=0.125,
+                  store_snapshots=1, dtinv=4, snap_precision=dn.SNAP_F16, ckpt_steps=400)
+    t0 = time.perf_counter()
+    vp, vs, rho = synth.base_model(p.nx, p.ny, p.dh, 4)
+    true = synth.add_ellipse(vp, vs, rho, p.dh, 4, v=5500.0)
+    start = tuple(synth.smoothed(x, 25.0) for x in true)
+    xmax = (p.nx - 1) * p.dh
+    sig = synth.ricker_source(p, 8.0)[None, :]
+    ri, rj = synth.receivers_line(100.0, xmax - 100.0, 1600, 20.0, p.dh)
+    picks = np.linspace(0, 95, n).round().astype(int)
+    shots = [(np.array([synth.grid_index(200.0 + (xmax - 400.0) * k / 95.0, p.dh)], np.int32),
+              np.array([max(synth.grid_index(10.0, p.dh), 1)], np.int32), sig, ri, rj) for k in picks]
+    t1 = time.perf_counter()
+    po = p.replace(store_snapshots=0, ckpt_steps=0)
+    mt = dn.Model(po, *true, device=device)
+    st_ = [dn.Shot(mt, *sh) for sh in shots]
+    dn.run(st_)
+    fwd_ms = dn.last_run_stats()[0]
+    obs = [(s.sections(dn.SEC_VX), s.sections(dn.SEC_VY)) for s in st_]
+    for s in st_:
+        s.close()
+    mt.close()
+    t2 = time.perf_counter()
+    lim = (1000.0, 6500.0, 500.0, 4000.0, 1000.0, 3500.0)
+    f = fwi.FWI(p, start, shots, obs, lim, device=device, nlbfgs=5, eps_scale=0.01)
+    L2 = f.iterate(1)
+    h = f.history[-1]
+    L2_new = f.misfit((f.vp, f.vs, f.rho))
+    f.lbfgs.close()
+    t3 = time.perf_counter()
+    cells = p.nx * p.ny * p.nt
+    per_shot_grad = h["gradient_s"] / n
+    per_shot_fwd = fwd_ms / 1e3 / n
+    return {"workload": "FWI iteration sample: elastic 8000x2000, DH 2.5 m, DT 0.2 ms, NT 12000, FDORDER 8, "
+                        f"{n} of 96 shots x 1600 receivers, FP16 snapshots every 4 steps, checkpointed adjoint "
+                        "(400-step segments), FP64 L-BFGS, parabolic step search",
+            "shots": n, "setup_s": round(t1 - t0, 1), "observed_data_s": round(t2 - t1, 1),
+            "forward_device_s_per_shot": round(per_shot_fwd, 2),
+            "forward_mcell_updates_per_s": round(cells / per_shot_fwd / 1e6, 1),
+            "gradient_s": round(h["gradient_s"], 1), "gradient_s_per_shot": round(per_shot_grad, 2),
+            "lbfgs_s": round(h["lbfgs_s"], 3), "step_search_s": round(h["step_search_s"], 1),
+            "test_models": h["test_models"], "step_found": h["found"], "eps": h["eps"],
+            "misfit_before": L2, "misfit_after": L2_new,
+            "iteration_s": round(t3 - t2, 1),
+            "iteration_96_shots_estimate_s": round(96 * per_shot_grad + h["test_models"] * 96 * per_shot_fwd, 0)}
 
 
 def run_serving(a, device, mcells_per_s):

@@ -171,7 +171,7 @@ class FWI:
         """mode-2 forward runs of all shots on a test model; sum of the vx and vy misfits."""
         from . import api as dn
 
-        m = dn.Model(self.p.replace(store_snapshots=0), *model, device=self.device)
+        m = dn.Model(self.p.replace(store_snapshots=0, ckpt_steps=0), *model, device=self.device)
         ss = [dn.Shot(m, *sh[:5]) for sh in self.shots]
         dn.run(ss, _lib.MODE_OBJECTIVE)
         L2 = 0.0
@@ -183,7 +183,11 @@ class FWI:
         return L2
 
     def iterate(self, it):
+        import time
+
+        t0 = time.perf_counter()
         g_vp, g_vs, g_rho, L2 = self.gradient()
+        t1 = time.perf_counter()
         nx, ny = self.p.nx, self.p.ny
         # gradient with respect to the scaled model x = m / scale
         g = np.concatenate([(gc * s).ravel() for gc, s in zip((g_vp, g_vs, g_rho), self.scale)])
@@ -193,15 +197,21 @@ class FWI:
         self.prev = (x, g)
         r = self.lbfgs.direction(g)
         d = [(r[k * nx * ny:(k + 1) * nx * ny] / self.scale[k]).reshape(nx, ny).astype(np.float32) for k in range(3)]
+        t2 = time.perf_counter()
+        ntests = [0]
 
         def objective(eps):
+            ntests[0] += 1
             vp, vs, rho, _ = mat_update(self.vp, self.vs, self.rho, *d, eps, self.limits, it)
             return self.misfit((vp, vs, rho))
 
         eps, L2t, epst, found = step_length(objective, L2, self.eps_scale, self.scalefac, self.stepmax)
         if found:
             self.vp, self.vs, self.rho, _ = mat_update(self.vp, self.vs, self.rho, *d, eps, self.limits, it)
-        self.history.append({"iteration": it, "misfit": L2, "eps": eps, "L2t": L2t, "epst": epst, "found": found})
+        t3 = time.perf_counter()
+        self.history.append({"iteration": it, "misfit": L2, "eps": eps, "L2t": L2t, "epst": epst, "found": found,
+                             "gradient_s": t1 - t0, "lbfgs_s": t2 - t1, "step_search_s": t3 - t2,
+                             "test_models": ntests[0]})
         return L2
 
 
