@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "dn_internal.h"
+#include "dn_precond.h"
 #include "dn_launch.cuh"
 
 using namespace dn;
@@ -1657,10 +1658,21 @@ __global__ void k_energy_weight(int nx, int ny, int ep, float dh, const float *W
 
 // We: energy weights (or null: no preconditioning); we_add = EPSILON_WE max(We);
 // c: the C_vp, C_vs, C_rho of grad_obj_psv.c:230-236
+// Per-shot circular taper of taper_grad_shot.c: coefficient (msum - minm) / maxm
+// with msum = m inside the G x G box at grid column x0, row z0 and 1 elsewhere,
+// then the cells of zc (0-based row-major, rows zr0..zr1) set to zero.
+struct ShotTaperArgs {
+    int on, G, x0, z0;
+    const float *m;
+    float minm, maxm;
+    const int *zc;
+    int nz, zr0, zr1;
+};
+
 __global__ void k_ass_grad(int nx, int ny, int pitch, const float *rho, const float *vp, const float *vs,
                            const float *gmuss, const float *glamss, const void *wc, const void *wcu, const void *wcr,
                            int acc64, float DT, void *gsum, int out64, const float *We, const unsigned *maxbits,
-                           float cvp, float cvs, float crho)
+                           float cvp, float cvs, float crho, ShotTaperArgs tp)
 {
     const long long n = (long long)nx * ny;
     for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x) {
@@ -1710,6 +1722,23 @@ __global__ void k_ass_grad(int nx, int ny, int pitch, const float *rho, const fl
                 grho /= wr * crho * crho;
             }
         }
+        if (tp.on) {   // taper_grad_shot.c, applied to the three shot gradients alike
+            const int bi = i - tp.x0, bj = j - tp.z0;
+            const float b = (bi >= 0 && bi < tp.G && bj >= 0 && bj < tp.G) ? tp.m[bj * tp.G + bi] : 1.0f;
+            const float c = __fdiv_rn(__fsub_rn(b, tp.minm), tp.maxm);
+            if (!acc64) {
+                gvp = __fmul_rn((float)gvp, c);
+                gvs = __fmul_rn((float)gvs, c);
+                grho = __fmul_rn((float)grho, c);
+            } else {
+                gvp *= c;
+                gvs *= c;
+                grho *= c;
+            }
+            if (j >= tp.zr0 && j <= tp.zr1)
+                for (int k = 0; k < tp.nz; k++)
+                    if (tp.zc[k] == (int)w) gvp = gvs = grho = 0.0;
+        }
         if (out64) {
             double *g = (double *)gsum;
             g[w] += gvp;
@@ -1724,35 +1753,83 @@ __global__ void k_ass_grad(int nx, int ny, int pitch, const float *rho, const fl
     }
 }
 
-static int accumulate(dn_shot *s, bool precond, float cvp, float cvs, float crho)
+static int accumulate(dn_shot *s, const dn_accum_opts *o)
 {
     if (!s) return dn_fail(DN_EINVAL, "null shot");
     if (!s->correlated) return dn_fail(DN_ESTATE, "dn_shot_accumulate_gradient: no completed adjoint run");
+    const bool precond = o && o->energy;
     const int ep = s->p.eprecond;
     if (precond && ep != 1 && ep != 3)
         return dn_fail(DN_EINVAL, "energy preconditioning needs EPRECOND 1 or 3 in the shot's parameters (got %d)", ep);
+    const bool taper = o && o->circular_taper;
+    if (taper && (o->srtshape != 1 && o->srtshape != 2))
+        return dn_fail(DN_EINVAL, "circular taper: SRTSHAPE must be 1 or 2 (got %d)", o->srtshape);
+    if (taper && (!(o->srtradius >= 0.0f) || o->srtradius > 1e6f || o->filtsize < 0 || o->filtsize > 1000))
+        return dn_fail(DN_EINVAL, "circular taper: SRTRADIUS %g, FILTSIZE %d out of range", o->srtradius, o->filtsize);
     dn_model *m = s->m;
     DevState *ds;
     int st = dev_state(m->device, &ds);
     if (st) return st;
     CU(cudaSetDevice(m->device));
-    const long long n = (long long)s->p.nx * s->p.ny;
+    const int nx = s->p.nx, ny = s->p.ny;
+    const long long n = (long long)nx * ny;
     int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
     char *buf = nullptr;
     float *We = nullptr;
     unsigned *maxbits = nullptr;
+    ShotTaperArgs tp = {};
+    std::vector<char> hbuf;     // box values, then the zeroed cells
+    size_t tap_mb = 0;
+    size_t we_bytes = precond ? carve_size(n, 4) + 256 : 0, tap_off = we_bytes;
+    if (taper) {
+        dnp_shot_taper_t t;
+        if (dnp_shot_taper(nx, ny, s->p.dh, o->srtshape, o->srtradius, o->src_x, o->src_z, &t))
+            return dn_fail(DN_ENOMEM, "circular taper set-up");
+        int ci, cj, *cells = nullptr, ncells = 0;
+        dnp_source_cell(o->src_x, o->src_z, s->p.dh, &ci, &cj);
+        if (dnp_zero_cells(nx, ny, 1, &ci, &cj, o->filtsize, 1, &cells, &ncells)) {
+            free(t.m);
+            return dn_fail(DN_ENOMEM, "circular taper set-up");
+        }
+        tap_mb = carve_size((size_t)t.G * t.G, 4);
+        hbuf.assign(tap_mb + carve_size((size_t)ncells + 1, 4), 0);
+        memcpy(hbuf.data(), t.m, sizeof(float) * t.G * t.G);
+        memcpy(hbuf.data() + tap_mb, cells, sizeof(int) * ncells);
+        tp.on = 1;
+        tp.G = t.G;
+        tp.x0 = t.x0;
+        tp.z0 = t.z0;
+        tp.minm = t.minm;
+        tp.maxm = t.maxm;
+        tp.nz = ncells;
+        tp.zr0 = ny + 1;
+        tp.zr1 = 0;
+        for (int k = 0; k < ncells; k++) {
+            tp.zr0 = std::min(tp.zr0, cells[k] / nx + 1);
+            tp.zr1 = std::max(tp.zr1, cells[k] / nx + 1);
+        }
+        free(t.m);
+        free(cells);
+    }
+    const size_t total = tap_off + hbuf.size();
+    if (total) CU(cudaMalloc(&buf, total));
     if (precond) {
-        CU(cudaMalloc(&buf, carve_size(n, 4) + 256));
         We = (float *)buf;
         maxbits = (unsigned *)(buf + carve_size(n, 4));
         CU(cudaMemsetAsync(maxbits, 0, 4, ds->stream));
-        k_energy_weight<<<blocks, 256, 0, ds->stream>>>(s->p.nx, s->p.ny, ep, s->p.dh, (const float *)acc_ptr(s, 3),
+        k_energy_weight<<<blocks, 256, 0, ds->stream>>>(nx, ny, ep, s->p.dh, (const float *)acc_ptr(s, 3),
                                                         (const float *)acc_ptr(s, 4), We, maxbits);
     }
-    k_ass_grad<<<blocks, 256, 0, ds->stream>>>(s->p.nx, s->p.ny, m->lay.pitch, m->field(MF_RHO), m->field(MF_VP),
+    if (taper) {
+        CU(cudaMemcpyAsync(buf + tap_off, hbuf.data(), hbuf.size(), cudaMemcpyHostToDevice, ds->stream));
+        tp.m = (const float *)(buf + tap_off);
+        tp.zc = (const int *)(buf + tap_off + tap_mb);
+    }
+    const float cvp = precond ? o->c_vp : 0.0f, cvs = precond ? o->c_vs : 0.0f, crho = precond ? o->c_rho : 0.0f;
+    k_ass_grad<<<blocks, 256, 0, ds->stream>>>(nx, ny, m->lay.pitch, m->field(MF_RHO), m->field(MF_VP),
                                                m->field(MF_VS), m->field(MF_GMUSS), m->field(MF_GLAMSS), acc_ptr(s, 0),
                                                acc_ptr(s, 1), acc_ptr(s, 2), s->acc64, s->p.dt, m->dgrad, m->grad64,
-                                               We, maxbits, cvp, cvs, crho);
+                                               We, maxbits, cvp, cvs, crho, tp);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(ds->stream);
     cudaFree(buf);
@@ -1760,11 +1837,22 @@ static int accumulate(dn_shot *s, bool precond, float cvp, float cvs, float crho
     return DN_OK;
 }
 
-extern "C" int dn_shot_accumulate_gradient(dn_shot *s) { return accumulate(s, false, 0.0f, 0.0f, 0.0f); }
+extern "C" int dn_shot_accumulate_gradient(dn_shot *s) { return accumulate(s, nullptr); }
 
 extern "C" int dn_shot_accumulate_gradient_precond(dn_shot *s, float c_vp, float c_vs, float c_rho)
 {
-    return accumulate(s, true, c_vp, c_vs, c_rho);
+    dn_accum_opts o = {};
+    o.energy = 1;
+    o.c_vp = c_vp;
+    o.c_vs = c_vs;
+    o.c_rho = c_rho;
+    return accumulate(s, &o);
+}
+
+extern "C" int dn_shot_accumulate_gradient_ex(dn_shot *s, const dn_accum_opts *o)
+{
+    if (!o) return dn_fail(DN_EINVAL, "dn_shot_accumulate_gradient_ex: null options");
+    return accumulate(s, o);
 }
 
 extern "C" int dn_model_get_gradient(const dn_model *m, float *g_vp, float *g_vs, float *g_rho)
@@ -1792,6 +1880,43 @@ extern "C" int dn_model_zero_gradient(dn_model *m)
     if (!m) return dn_fail(DN_EINVAL, "null model");
     CU(cudaSetDevice(m->device));
     CU(cudaMemset(m->dgrad, 0, 3 * (size_t)m->p.nx * m->p.ny * (m->grad64 ? 8 : 4)));
+    return DN_OK;
+}
+
+extern "C" int dn_model_set_gradient(dn_model *m, const float *g_vp, const float *g_vs, const float *g_rho)
+{
+    if (!m) return dn_fail(DN_EINVAL, "null model");
+    const int nx = m->p.nx, ny = m->p.ny;
+    const size_t n = (size_t)nx * ny, eb = m->grad64 ? 8 : 4;
+    const float *ins[3] = {g_vp, g_vs, g_rho};
+    std::vector<char> h(n * eb);
+    CU(cudaSetDevice(m->device));
+    for (int c = 0; c < 3; c++) {
+        if (!ins[c]) continue;
+        for (int i = 1; i <= nx; i++)
+            for (int j = 1; j <= ny; j++) {
+                const float v = ins[c][(size_t)(i - 1) * ny + (j - 1)];
+                const size_t w = (size_t)(j - 1) * nx + (i - 1);
+                if (m->grad64)
+                    ((double *)h.data())[w] = v;
+                else
+                    ((float *)h.data())[w] = v;
+            }
+        CU(cudaMemcpy((char *)m->dgrad + c * n * eb, h.data(), n * eb, cudaMemcpyHostToDevice));
+    }
+    return DN_OK;
+}
+
+extern "C" int dn_model_view_get(dn_model *m, dn_model_view *v)
+{
+    if (!m || !v) return dn_fail(DN_EINVAL, "null argument");
+    v->nx = m->p.nx;
+    v->ny = m->p.ny;
+    v->pitch = m->lay.pitch;
+    v->device = m->device;
+    v->grad64 = m->grad64;
+    v->dgrad = m->dgrad;
+    v->vs = m->field(MF_VS);
     return DN_OK;
 }
 

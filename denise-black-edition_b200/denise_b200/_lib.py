@@ -85,6 +85,30 @@ class Pml(ctypes.Structure):
 
 PML_NAMES = [f[0] for f in Pml._fields_]
 
+
+class Precond(ctypes.Structure):
+    """dn_precond: smooth_grad and precond_PSV switches (the .inp keywords)."""
+    _fields_ = [
+        ("spatfilter", ctypes.c_int), ("wd_damp", ctypes.c_float), ("wd_damp1", ctypes.c_float),
+        ("fc_end", ctypes.c_float), ("c_vs", ctypes.c_float),
+        ("taper_vert", ctypes.c_int), ("taper_hor", ctypes.c_int), ("taper_sources", ctypes.c_int),
+        ("taper_file", ctypes.c_int), ("gradt", ctypes.c_int * 4), ("exp_taper_grad_hor", ctypes.c_float),
+        ("srtshape", ctypes.c_int), ("srtradius", ctypes.c_float), ("filtsize", ctypes.c_int),
+        ("taper_vp", ctypes.POINTER(ctypes.c_float)), ("taper_vs", ctypes.POINTER(ctypes.c_float)),
+        ("taper_rho", ctypes.POINTER(ctypes.c_float)),
+        ("nsrc", ctypes.c_int), ("src_x", ctypes.POINTER(ctypes.c_float)), ("src_z", ctypes.POINTER(ctypes.c_float)),
+        ("ntr", ctypes.c_int), ("rec_i", ctypes.POINTER(ctypes.c_int)), ("rec_j", ctypes.POINTER(ctypes.c_int)),
+    ]
+
+
+class AccumOpts(ctypes.Structure):
+    """dn_accum_opts: per-shot energy scaling and circular taper of the gradient assembly."""
+    _fields_ = [
+        ("energy", ctypes.c_int), ("c_vp", ctypes.c_float), ("c_vs", ctypes.c_float), ("c_rho", ctypes.c_float),
+        ("circular_taper", ctypes.c_int), ("srtshape", ctypes.c_int), ("srtradius", ctypes.c_float),
+        ("filtsize", ctypes.c_int), ("src_x", ctypes.c_float), ("src_z", ctypes.c_float),
+    ]
+
 # every function the header declares, with its argument types
 _P = ctypes.POINTER
 _c_int_p = _P(ctypes.c_int)
@@ -119,6 +143,14 @@ SIGNATURES = {
     "dn_shot_accumulate_gradient_precond": (ctypes.c_int, [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float]),
     "dn_model_get_gradient": (ctypes.c_int, [_vp, _c_float_p, _c_float_p, _c_float_p]),
     "dn_model_zero_gradient": (ctypes.c_int, [_vp]),
+    "dn_model_set_gradient": (ctypes.c_int, [_vp, _c_float_p, _c_float_p, _c_float_p]),
+    "dn_precond_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_float, _P(Precond), ctypes.c_int,
+                                         _P(_vp)]),
+    "dn_precond_destroy": (ctypes.c_int, [_vp]),
+    "dn_precond_apply": (ctypes.c_int, [_vp, _vp]),
+    "dn_taper_coefficients": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_float, _P(Precond), ctypes.c_int,
+                                             _c_float_p]),
+    "dn_shot_accumulate_gradient_ex": (ctypes.c_int, [_vp, _P(AccumOpts)]),
     "dn_shot_get_field": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p]),
     "dn_run_steps": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "dn_shot_get_snapshot": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_float_p]),

@@ -186,6 +186,11 @@ class Model:
     def zero_gradient(self):
         check(lib.dn_model_zero_gradient(self.handle))
 
+    def set_gradient(self, g_vp=None, g_vs=None, g_rho=None):
+        """Replaces the stacked gradients (file order (nx, ny) arrays; None keeps a class)."""
+        arrs = [None if g is None else np.ascontiguousarray(g, np.float32) for g in (g_vp, g_vs, g_rho)]
+        check(lib.dn_model_set_gradient(self.handle, *[fptr(a) for a in arrs]))
+
 
 class Shot:
     """Wavefield state + acquisition of one shot on a model's device."""
@@ -249,6 +254,20 @@ class Shot:
     def accumulate_gradient_precond(self, c_vp, c_vs, c_rho):
         """ass_gradPSV with the per-shot energy preconditioning (EPRECOND 1 or 3)."""
         check(lib.dn_shot_accumulate_gradient_precond(self.handle, float(c_vp), float(c_vs), float(c_rho)))
+
+    def accumulate_gradient_ex(self, energy=None, circular_taper=None):
+        """Gradient assembly with the per-shot options of grad_obj_psv.c:214-250.
+        energy = (c_vp, c_vs, c_rho) for EPRECOND 1/3 scaling; circular_taper =
+        (srtshape, srtradius, filtsize, src_x, src_z) for taper_grad_shot around
+        this shot's source (metres)."""
+        o = _lib.AccumOpts()
+        if energy is not None:
+            o.energy = 1
+            o.c_vp, o.c_vs, o.c_rho = (float(x) for x in energy)
+        if circular_taper is not None:
+            o.circular_taper = 1
+            o.srtshape, o.srtradius, o.filtsize, o.src_x, o.src_z = circular_taper
+        check(lib.dn_shot_accumulate_gradient_ex(self.handle, ctypes.byref(o)))
 
     def field(self, fid):
         out = np.zeros((self.model.params.nx, self.model.params.ny), np.float32)

@@ -145,7 +145,7 @@ class FWI:
     snapshots.  limits: (vp_lo, vp_hi, vs_lo, vs_hi, rho_lo, rho_hi)."""
 
     def __init__(self, params, model, shots, obs, limits, device=0, nlbfgs=20, eps_scale=0.01, scalefac=2.0,
-                 stepmax=4, dist=None):
+                 stepmax=4, dist=None, precond=None, shot_taper=None):
         self.p = params
         self.vp, self.vs, self.rho = [np.ascontiguousarray(a, np.float32) for a in model[:3]]
         self.shots, self.obs, self.limits = shots, obs, limits
@@ -154,6 +154,13 @@ class FWI:
         self.scale = np.array([self.vp.max(), self.vs.max(), self.rho.max()], np.float64)
         n = 3 * params.nx * params.ny
         self.lbfgs = LBFGS(n, nlbfgs, device)
+        # gradient conditioning after stacking (FWI_PSV.c:628-634) and per shot
+        self.shot_taper = shot_taper
+        self.precond = None
+        if precond is not None:
+            from .precond import PrecondPlan
+
+            self.precond = PrecondPlan(params.nx, params.ny, params.dh, precond, device)
         self.prev = None          # (x, g) of the previous iteration, scaled
         self.history = []
 
@@ -165,7 +172,17 @@ class FWI:
         from .shard import sharded_gradient
 
         m = model or (self.vp, self.vs, self.rho)
-        return sharded_gradient(self.p, m, self.shots, self.obs, self.dist, self.device)
+        g_vp, g_vs, g_rho, L2 = sharded_gradient(self.p, m, self.shots, self.obs, self.dist, self.device,
+                                                 self.shot_taper)
+        if self.precond is not None:
+            from . import api as dn
+
+            dm = dn.Model(self.p.replace(store_snapshots=0, ckpt_steps=0, L=0, fl=()), *m[:3], device=self.device)
+            dm.set_gradient(g_vp.astype(np.float32), g_vs.astype(np.float32), g_rho.astype(np.float32))
+            self.precond.apply(dm)
+            g_vp, g_vs, g_rho = [x.astype(np.float64) for x in dm.gradient()]
+            dm.close()
+        return g_vp, g_vs, g_rho, L2
 
     def misfit(self, model):
         """mode-2 forward runs of all shots on a test model; sum of the vx and vy misfits."""

@@ -48,13 +48,15 @@ def allreduce_sum(arrays, dist=None, device=None):
     return out
 
 
-def sharded_gradient(params, model, shots, obs, dist=None, device_index=0):
+def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_taper=None):
     """FWI gradient of `shots` sharded over the ranks of `dist` (all ranks pass
     the same arguments).  Each rank runs its share as one batch on its GPU:
     forward with snapshots, device residuals against `obs`, adjoint, and stacks
     its shots' gradients in shot order; the partial gradients and misfits are
     then summed over ranks.  Returns (g_vp, g_vs, g_rho, misfit), float64, on
-    every rank."""
+    every rank.  shot_taper = (srtshape, srtradius, filtsize) applies the
+    per-shot circular taper (taper_grad_shot.c) around each shot's first source
+    before stacking."""
     from . import api as dn
     from ._lib import MODE_ADJOINT, MODE_FORWARD, SEC_VX, SEC_VY
 
@@ -72,8 +74,12 @@ def sharded_gradient(params, model, shots, obs, dist=None, device_index=0):
         for s, k in zip(ss, mine):
             misfit += s.residual(obs[k][0], SEC_VX) + s.residual(obs[k][1], SEC_VY)
         dn.run(ss, MODE_ADJOINT)
-        for s in ss:
-            s.accumulate_gradient()
+        for s, k in zip(ss, mine):
+            if shot_taper is None:
+                s.accumulate_gradient()
+            else:
+                sx, sz = float(shots[k][0][0]) * params.dh, float(shots[k][1][0]) * params.dh
+                s.accumulate_gradient_ex(circular_taper=tuple(shot_taper) + (sx, sz))
         g = [x.astype(np.float64) for x in m.gradient()]
         for s in ss:
             s.close()

@@ -221,6 +221,67 @@ int dn_shot_accumulate_gradient_precond(dn_shot *s, float c_vp, float c_vs, floa
 /* The model's stacked gradients (waveconv, waveconv_u, waveconv_rho) in file order. */
 int dn_model_get_gradient(const dn_model *m, float *g_vp, float *g_vs, float *g_rho);
 int dn_model_zero_gradient(dn_model *m);
+/* Replaces the model's stacked gradients (file order; NULL leaves a class as it
+ * is), e.g. with the sum over ranks before the conditioning below. */
+int dn_model_set_gradient(dn_model *m, const float *g_vp, const float *g_vs, const float *g_rho);
+
+/* ---- gradient conditioning ------------------------------------------------
+ * smooth_grad (src/smooth_grad.c) of the three stacked gradients followed by
+ * precond_PSV (src/PSV/precond_PSV.c), FWI_PSV.c:628-634, and the per-shot
+ * circular taper taper_grad_shot (src/taper_grad_shot.c) that
+ * grad_obj_psv.c:242-250 applies before stacking.  Field names are the .inp
+ * keywords of the reference. */
+typedef struct dn_precond {
+    /* smooth_grad: 0 none, 2 smooth2 (tridiagonal smoothing, WD_DAMP along z,
+     * WD_DAMP1 along x), 3 gauss_filt (Gaussian of WD_DAMP * C_vs / FC_END),
+     * 4 gauss_filt_var (Gaussian of WD_DAMP, WD_DAMP1 times the local S
+     * wavelength vs / FC_END).  1 (wavenumber filter) needs FFTW: DN_ENOTSUP. */
+    int spatfilter;
+    float wd_damp, wd_damp1, fc_end, c_vs;
+    /* precond_PSV tapers, applied in this order to each class */
+    int taper_vert;                     /* SWS_TAPER_GRAD_VERT (taper_grad sws 1) */
+    int taper_hor;                      /* SWS_TAPER_GRAD_HOR (sws 2) */
+    int taper_sources;                  /* SWS_TAPER_GRAD_SOURCES (sws 3) */
+    int taper_file;                     /* SWS_TAPER_FILE (sws 4-6) */
+    int gradt[4];                       /* GRADT1..GRADT4 */
+    float exp_taper_grad_hor;           /* EXP_TAPER_GRAD_HOR */
+    int srtshape;                       /* SRTSHAPE: 1 erf, 2 log */
+    float srtradius;                    /* SRTRADIUS (m) */
+    int filtsize;                       /* FILTSIZE: half-width of the zeroed box at each source */
+    /* taper_file: coefficients of TFILE.bin, TFILE_u.bin, TFILE_rho.bin (file order) */
+    const float *taper_vp, *taper_vs, *taper_rho;
+    /* acquisition: all sources of the survey (metres, srcpos[1..2]) and receivers (grid indices) */
+    int nsrc;
+    const float *src_x, *src_z;
+    int ntr;
+    const int *rec_i, *rec_j;
+} dn_precond;
+
+typedef struct dn_precond_plan dn_precond_plan;
+/* Validates `c` and computes, on the host, everything that depends on the
+ * geometry only (taper coefficients, zeroed cells, smoothing factorisations,
+ * Gaussian weights), stored on `device` for dn_precond_apply. */
+int dn_precond_create(int nx, int ny, float dh, const dn_precond *c, int device, dn_precond_plan **out);
+int dn_precond_destroy(dn_precond_plan *p);
+/* Conditions the model's stacked gradients in place on the device (smoothing,
+ * then the tapers).  SPATFILTER 4 reads the model's vs. */
+int dn_precond_apply(const dn_precond_plan *p, dn_model *m);
+/* The taper coefficients of one taper_grad switch (sws 1 vertical, 2
+ * horizontal, 3 sources; before the zeroed source boxes) in file order: the
+ * TFILE_coeff_*.bin the reference writes. */
+int dn_taper_coefficients(int nx, int ny, float dh, const dn_precond *c, int sws, float *coeff);
+
+/* Per-shot options of the gradient assembly (grad_obj_psv.c:214-250). */
+typedef struct dn_accum_opts {
+    int energy;                         /* 1: EPRECOND 1/3 scaling (as dn_shot_accumulate_gradient_precond) */
+    float c_vp, c_vs, c_rho;
+    int circular_taper;                 /* SWS_TAPER_CIRCULAR_PER_SHOT: taper_grad_shot around this shot's source */
+    int srtshape;
+    float srtradius;
+    int filtsize;
+    float src_x, src_z;                 /* this shot's source position (m) */
+} dn_accum_opts;
+int dn_shot_accumulate_gradient_ex(dn_shot *s, const dn_accum_opts *o);
 
 /* Unit-level access for parity tests: full-grid interior copies in file order.
  * field ids: 0 vx, 1 vy, 2 sxx, 3 syy, 4 sxy, 5 vxp1, 6 vyp1,

@@ -535,3 +535,138 @@ int refh_ass_grad_ep(const float *c3, float *gvp, float *gvs, float *grho)
     to_file(FWI.waveconv_rho_shot, grho);
     return 0;
 }
+
+/* ---- gradient conditioning of the reference --------------------------------- */
+/* Globals of taper_grad.c, taper_grad_shot.c, smooth_grad.c and the filters it calls. */
+extern int NXG, NYG, GRADT1, GRADT2, GRADT3, GRADT4, SWS_TAPER_GRAD_VERT, SWS_TAPER_GRAD_HOR;
+extern int SWS_TAPER_GRAD_SOURCES, SWS_TAPER_FILE, SRTSHAPE, FILTSIZE, SPATFILTER;
+extern float SRTRADIUS, EXP_TAPER_GRAD_HOR, WD_DAMP, WD_DAMP1, FC_END;
+extern char TFILE[STRING_SIZE], JACOBIAN[STRING_SIZE];
+
+/* Gradient arrays padded like the reference's waveconv (FWI_PSV.c allocates them with
+ * the wavefield halo); taper_coeff gets a generous pad so that the source-box loops,
+ * which may index a few cells left of column 1, stay inside the allocation. */
+#define REFH_PAD 64
+static float **grad_in(int nx, int ny, const float *a)
+{
+    float **m = matrix(-REFH_PAD, ny + REFH_PAD, -REFH_PAD, nx + REFH_PAD);
+    for (int i = 1; i <= nx; i++)
+        for (int j = 1; j <= ny; j++) m[j][i] = a[(size_t)(i - 1) * ny + (j - 1)];
+    return m;
+}
+static void grad_out(int nx, int ny, float **m, float *a)
+{
+    for (int i = 1; i <= nx; i++)
+        for (int j = 1; j <= ny; j++) a[(size_t)(i - 1) * ny + (j - 1)] = m[j][i];
+    free_matrix(m, -REFH_PAD, ny + REFH_PAD, -REFH_PAD, nx + REFH_PAD);
+}
+static void precond_globals(int nx, int ny, float dh)
+{
+    NX = NXG = nx;
+    NY = NYG = ny;
+    DH = dh;
+    MYID = 0;
+    MYID_SHOT = 0;
+    POS[1] = POS[2] = 0;
+    NPROCX = NPROCY = 1;
+    IDX = IDY = 1;
+    FP = null_log();
+}
+
+/* precond_PSV (src/PSV/precond_PSV.c) on three gradients in file order.
+ * sw = {vert, hor, sources, file}; srcxz = [nsrc][2] source x, z in metres;
+ * tfile = the TFILE prefix (files tfile.bin, tfile_u.bin, tfile_rho.bin for sw[3]),
+ * relative to the working directory, which must be writable (taper_grad writes
+ * its coefficient files there). */
+int refh_precond(int nx, int ny, float dh, const int *sw, const int *gradt, float exp_hor, int srtshape,
+                 float srtradius, int filtsize, const char *tfile, int nsrc, const float *srcxz, int ntr,
+                 const int *rec_i, const int *rec_j, float *g_vp, float *g_vs, float *g_rho)
+{
+    precond_globals(nx, ny, dh);
+    SWS_TAPER_GRAD_VERT = sw[0];
+    SWS_TAPER_GRAD_HOR = sw[1];
+    SWS_TAPER_GRAD_SOURCES = sw[2];
+    SWS_TAPER_FILE = sw[3];
+    GRADT1 = gradt[0];
+    GRADT2 = gradt[1];
+    GRADT3 = gradt[2];
+    GRADT4 = gradt[3];
+    EXP_TAPER_GRAD_HOR = exp_hor;
+    SRTSHAPE = srtshape;
+    SRTRADIUS = srtradius;
+    FILTSIZE = filtsize;
+    snprintf(TFILE, STRING_SIZE, "%s", tfile);
+    struct fwiPSV F;
+    struct acq Q;
+    memset(&F, 0, sizeof F);
+    memset(&Q, 0, sizeof Q);
+    F.waveconv = grad_in(nx, ny, g_vp);
+    F.waveconv_u = grad_in(nx, ny, g_vs);
+    F.waveconv_rho = grad_in(nx, ny, g_rho);
+    Q.srcpos = matrix(1, 8, 1, nsrc > 0 ? nsrc : 1);
+    for (int n = 1; n <= nsrc; n++) {
+        Q.srcpos[1][n] = srcxz[2 * (n - 1)];
+        Q.srcpos[2][n] = srcxz[2 * (n - 1) + 1];
+    }
+    Q.recpos = imatrix(1, 3, 1, ntr > 0 ? ntr : 1);
+    for (int n = 1; n <= ntr; n++) {
+        Q.recpos[1][n] = rec_i[n - 1];
+        Q.recpos[2][n] = rec_j[n - 1];
+    }
+    float **tc = matrix(-REFH_PAD, ny + REFH_PAD, -REFH_PAD, nx + REFH_PAD);
+    precond_PSV(&F, &Q, nsrc, ntr, tc, NULL);
+    grad_out(nx, ny, F.waveconv, g_vp);
+    grad_out(nx, ny, F.waveconv_u, g_vs);
+    grad_out(nx, ny, F.waveconv_rho, g_rho);
+    free_matrix(tc, -REFH_PAD, ny + REFH_PAD, -REFH_PAD, nx + REFH_PAD);
+    free_matrix(Q.srcpos, 1, 8, 1, nsrc > 0 ? nsrc : 1);
+    free_imatrix(Q.recpos, 1, 3, 1, ntr > 0 ? ntr : 1);
+    return 0;
+}
+
+/* taper_grad_shot (src/taper_grad_shot.c) of shot ishot (1-based) on one gradient. */
+int refh_taper_shot(int nx, int ny, float dh, int srtshape, float srtradius, int filtsize, const char *tfile,
+                    int nsrc, const float *srcxz, int ishot, float *g)
+{
+    precond_globals(nx, ny, dh);
+    SRTSHAPE = srtshape;
+    SRTRADIUS = srtradius;
+    FILTSIZE = filtsize;
+    COLOR = 0;
+    snprintf(TFILE, STRING_SIZE, "%s", tfile);
+    float **srcpos = matrix(1, 8, 1, nsrc);
+    for (int n = 1; n <= nsrc; n++) {
+        srcpos[1][n] = srcxz[2 * (n - 1)];
+        srcpos[2][n] = srcxz[2 * (n - 1) + 1];
+    }
+    int **recpos = imatrix(1, 3, 1, 1);
+    float **w = grad_in(nx, ny, g);
+    float **tc = matrix(-REFH_PAD, ny + REFH_PAD, -REFH_PAD, nx + REFH_PAD);
+    taper_grad_shot(w, tc, srcpos, nsrc, recpos, 0, ishot);
+    grad_out(nx, ny, w, g);
+    free_matrix(tc, -REFH_PAD, ny + REFH_PAD, -REFH_PAD, nx + REFH_PAD);
+    free_matrix(srcpos, 1, 8, 1, nsrc);
+    free_imatrix(recpos, 1, 3, 1, 1);
+    return 0;
+}
+
+/* smooth_grad (src/smooth_grad.c) on one gradient; vel = the S-velocity model
+ * (file order) for SPATFILTER 4.  jacobian = the JACOBIAN prefix of the
+ * temporary files, relative to the (writable) working directory. */
+int refh_smooth_grad(int nx, int ny, float dh, int spatfilter, float wd_damp, float wd_damp1, float fc_end,
+                     float c_vs, const char *jacobian, const float *vel, float *g)
+{
+    precond_globals(nx, ny, dh);
+    SPATFILTER = spatfilter;
+    WD_DAMP = wd_damp;
+    WD_DAMP1 = wd_damp1;
+    FC_END = fc_end;
+    C_vs = c_vs;
+    snprintf(JACOBIAN, STRING_SIZE, "%s", jacobian);
+    float **w = grad_in(nx, ny, g);
+    float **v = grad_in(nx, ny, vel);
+    smooth_grad(w, v);
+    grad_out(nx, ny, w, g);
+    free_matrix(v, -REFH_PAD, ny + REFH_PAD, -REFH_PAD, nx + REFH_PAD);
+    return 0;
+}

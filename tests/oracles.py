@@ -243,3 +243,49 @@ def reference_forward_sections(p, model, src, rec):
     r = Reference(p, model, src, rec, mode_global=0)
     r.run(0)
     return r.sections(0), r.sections(1)
+
+
+# ---------------------------------------------------------------------------
+# the reference's gradient conditioning (precond_PSV, taper_grad_shot,
+# smooth_grad) through oracle/ref_harness.c; call each in run_isolated().
+# Gradients are [NY][NX] float32 (row j, column i); the harness takes file order.
+# ---------------------------------------------------------------------------
+def _ref_lib():
+    return ctypes.CDLL(REF_SO)
+
+
+def ref_precond(workdir, nx, ny, dh, sw, gradt, exp_hor, srtshape, srtradius, filtsize, srcs, recs, grads,
+                tfile="tp"):
+    os.chdir(workdir)
+    lib = _ref_lib()
+    gs = [np.ascontiguousarray(np.asarray(g, np.float32).T) for g in grads]
+    sxz = np.asarray(srcs, np.float32).reshape(-1, 2) if len(srcs) else np.zeros((1, 2), np.float32)
+    ri = np.array([r[0] for r in recs] or [0], np.int32)
+    rj = np.array([r[1] for r in recs] or [0], np.int32)
+    lib.refh_precond(ctypes.c_int(nx), ctypes.c_int(ny), ctypes.c_float(dh), _ip(sw), _ip(gradt),
+                     ctypes.c_float(exp_hor), ctypes.c_int(srtshape), ctypes.c_float(srtradius), ctypes.c_int(filtsize),
+                     tfile.encode(), ctypes.c_int(len(srcs)), _fp(sxz), ctypes.c_int(len(recs)), _ip(ri), _ip(rj),
+                     *[g.ctypes.data_as(_f) for g in gs])
+    return [g.T.copy() for g in gs]
+
+
+def ref_taper_shot(workdir, nx, ny, dh, srtshape, srtradius, filtsize, srcs, ishot, grad, tfile="tp"):
+    os.chdir(workdir)
+    lib = _ref_lib()
+    g = np.ascontiguousarray(np.asarray(grad, np.float32).T)
+    sxz = np.asarray(srcs, np.float32).reshape(-1, 2)
+    lib.refh_taper_shot(ctypes.c_int(nx), ctypes.c_int(ny), ctypes.c_float(dh), ctypes.c_int(srtshape),
+                        ctypes.c_float(srtradius), ctypes.c_int(filtsize), tfile.encode(), ctypes.c_int(len(srcs)),
+                        _fp(sxz), ctypes.c_int(ishot), g.ctypes.data_as(_f))
+    return g.T.copy()
+
+
+def ref_smooth_grad(workdir, nx, ny, dh, spatfilter, wd_damp, wd_damp1, fc_end, c_vs, vel, grad, jac="jac"):
+    os.chdir(workdir)
+    lib = _ref_lib()
+    g = np.ascontiguousarray(np.asarray(grad, np.float32).T)
+    v = np.ascontiguousarray(np.asarray(vel, np.float32).T)
+    lib.refh_smooth_grad(ctypes.c_int(nx), ctypes.c_int(ny), ctypes.c_float(dh), ctypes.c_int(spatfilter),
+                         ctypes.c_float(wd_damp), ctypes.c_float(wd_damp1), ctypes.c_float(fc_end), ctypes.c_float(c_vs),
+                         jac.encode(), v.ctypes.data_as(_f), g.ctypes.data_as(_f))
+    return g.T.copy()
