@@ -241,11 +241,8 @@ static int validate(int nx, int ny, float dh, const dn_precond *c)
         return dn_fail(DN_EINVAL, "gauss_filt needs FC_END > 0 (got %g)", c->fc_end);
     if (c->spatfilter == 4 && (c->wd_damp < 0.0f || c->wd_damp1 < 0.0f))
         return dn_fail(DN_EINVAL, "gauss_filt_var needs WD_DAMP, WD_DAMP1 >= 0");
-    if (c->taper_vert || c->taper_hor) {
-        if (c->gradt[0] > c->gradt[1] || c->gradt[2] > c->gradt[3] || c->gradt[1] > c->gradt[3])
-            return dn_fail(DN_EINVAL, "GRADT1..GRADT4 = %d %d %d %d are not in order", c->gradt[0], c->gradt[1],
-                           c->gradt[2], c->gradt[3]);
-    }
+    // GRADT1..4 need no check: the taper windows are only read at indices the
+    // loops of taper_grad.c reach for any values (an empty ramp reads nothing)
     if (c->taper_sources && c->srtshape != 1 && c->srtshape != 2)
         return dn_fail(DN_EINVAL, "SRTSHAPE must be 1 or 2 (got %d)", c->srtshape);
     if (c->taper_sources && (!(c->srtradius >= 0.0f) || c->srtradius > 1e6f || c->filtsize < 0 || c->filtsize > 1000))

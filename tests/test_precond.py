@@ -103,9 +103,11 @@ def config(sw, shape=1, **kw):
 
 
 @pytest.mark.parametrize("shape", [1, 2])
-def test_host_taper_coefficients_match_oracle(shape):
+@pytest.mark.parametrize("gradt", [GRADT, (5, 9, 0, 0), (0, 0, 30, 30), (9, 3, 45, 55)])
+def test_host_taper_coefficients_match_oracle(shape, gradt):
     c = config((1, 1, 1, 0), shape)
-    want = {1: po.taper_vertical(NX, NY, GRADT), 2: po.taper_horizontal(NX, NY, DH, GRADT, 1.5),
+    c.gradt = gradt
+    want = {1: po.taper_vertical(NX, NY, gradt), 2: po.taper_horizontal(NX, NY, DH, gradt, 1.5),
             3: po.taper_sources(NX, NY, DH, SRCS, shape, 12.0)}
     for sws, w in want.items():
         got = taper_coefficients(NX, NY, DH, c, sws)
@@ -116,7 +118,7 @@ def test_argument_errors():
     with pytest.raises(DeniseError, match="DN_ENOTSUP"):
         PrecondPlan(NX, NY, DH, PrecondConfig(spatfilter=1))
     with pytest.raises(DeniseError, match="DN_EINVAL"):
-        PrecondPlan(NX, NY, DH, PrecondConfig(taper_vert=1, gradt=(9, 3, 45, 55)))
+        PrecondPlan(1, NY, DH, PrecondConfig(taper_vert=1, gradt=(9, 3, 45, 55)))
     with pytest.raises(DeniseError, match="DN_EINVAL"):
         PrecondPlan(NX, NY, DH, PrecondConfig(taper_sources=1, srtshape=3, srtradius=10.0, sources=SRCS))
     with pytest.raises(DeniseError, match="DN_EINVAL"):
