@@ -1985,12 +1985,15 @@ extern "C" int dn_profile_steps(dn_shot *const *shots, int n, int mode, int nste
 // data residual of a forward-run shot into its adjoint sources (calc_res_PSV +
 // calc_res, LNORM 2): obs [ntr][nt] host, comp DN_SEC_VX / VY / P
 // ---------------------------------------------------------------------------
-extern "C" int dn_adjoint_source_launch(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt,
-                                        int grad_form, int rtm, double *scratch, cudaStream_t stream);
+extern "C" int dn_residual_run_ex(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt,
+                                  float dh, const int *rec_i, const int *rec_j, const dn_residual_opts *o,
+                                  double *misfit, cudaStream_t st);
 
-static int shot_source(dn_shot *s, int comp, const float *obs, double *l2, int rtm)
+// calc_res of one recorded component against host observed data; the residual
+// becomes the shot's adjoint source of that component
+static int shot_source(dn_shot *s, int comp, const float *obs, double *l2, const dn_residual_opts *o)
 {
-    if (!s || !obs) return dn_fail(DN_EINVAL, "dn_shot_residual: null argument");
+    if (!s || !obs || !o) return dn_fail(DN_EINVAL, "dn_shot_residual: null argument");
     if (comp != DN_SEC_VX && comp != DN_SEC_VY && comp != DN_SEC_P)
         return dn_fail(DN_EINVAL, "dn_shot_residual: component must be vx, vy or p");
     if (s->ntr < 1) return dn_fail(DN_EINVAL, "dn_shot_residual: shot has no receivers");
@@ -2001,9 +2004,7 @@ static int shot_source(dn_shot *s, int comp, const float *obs, double *l2, int r
     const int nt = s->p.nt, ntr = s->ntr;
     const size_t n = (size_t)ntr * nt;
     float *dobs = nullptr;
-    double *scratch = nullptr;
-    if (cudaMalloc(&dobs, n * 4) != cudaSuccess || cudaMalloc(&scratch, sizeof(double) * (ntr + 1)) != cudaSuccess) {
-        cudaFree(dobs);
+    if (cudaMalloc(&dobs, n * 4) != cudaSuccess) {
         cudaGetLastError();
         return dn_fail(DN_ENOMEM, "dn_shot_residual: device allocation failed");
     }
@@ -2012,28 +2013,39 @@ static int shot_source(dn_shot *s, int comp, const float *obs, double *l2, int r
     double h = 0.0;
     cudaError_t e = cudaMemcpyAsync(dobs, obs, n * 4, cudaMemcpyHostToDevice, ds->stream);
     if (e == cudaSuccess)
-        st = dn_adjoint_source_launch(s->d_sec + (size_t)comp * nt * ntr, dobs, s->d_res + k * rs, ntr, nt, s->p.dt,
-                                      s->p.grad_form, rtm, scratch, ds->stream);
-    else st = dn_fail(DN_EDEVICE, "dn_shot_residual: %s", cudaGetErrorString(e));
-    if (!st) {
-        e = cudaMemcpyAsync(&h, scratch + ntr, sizeof(double), cudaMemcpyDeviceToHost, ds->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(ds->stream);
-        if (e != cudaSuccess) st = dn_fail(DN_EDEVICE, "dn_shot_residual: %s", cudaGetErrorString(e));
-    }
+        st = dn_residual_run_ex(s->d_sec + (size_t)comp * nt * ntr, dobs, s->d_res + k * rs, ntr, nt, s->p.dt, s->p.dh,
+                                s->rec_i.data(), s->rec_j.data(), o, &h, ds->stream);
+    else
+        st = dn_fail(DN_EDEVICE, "dn_shot_residual: %s", cudaGetErrorString(e));
     cudaFree(dobs);
-    cudaFree(scratch);
     if (st) return st;
     s->has_res[k] = 1;
     if (l2) *l2 = h;
     return DN_OK;
 }
 
+static dn_residual_opts l2_opts(const dn_shot *s, int rtm)
+{
+    dn_residual_opts o = {};
+    o.lnorm = 2;
+    o.grad_form = s ? s->p.grad_form : 1;
+    o.mode = rtm ? 2 : 1;
+    return o;
+}
+
 extern "C" int dn_shot_residual(dn_shot *s, int comp, const float *obs, double *l2)
 {
-    return shot_source(s, comp, obs, l2, 0);
+    const dn_residual_opts o = l2_opts(s, 0);
+    return shot_source(s, comp, obs, l2, &o);
 }
 
 extern "C" int dn_shot_rtm_source(dn_shot *s, int comp, const float *obs)
 {
-    return shot_source(s, comp, obs, nullptr, 1);
+    const dn_residual_opts o = l2_opts(s, 1);
+    return shot_source(s, comp, obs, nullptr, &o);
+}
+
+extern "C" int dn_shot_residual_ex(dn_shot *s, int comp, const float *obs, const dn_residual_opts *o, double *misfit)
+{
+    return shot_source(s, comp, obs, misfit, o);
 }

@@ -101,6 +101,18 @@ class Precond(ctypes.Structure):
     ]
 
 
+class ResidualOpts(ctypes.Structure):
+    """dn_residual_opts: the calc_res options (LNORM, GRAD_FORM, MODE, N_ORDER, ...)."""
+    _fields_ = [
+        ("lnorm", ctypes.c_int), ("grad_form", ctypes.c_int), ("mode", ctypes.c_int), ("n_order", ctypes.c_int),
+        ("comp_weight", ctypes.c_int), ("c_vp", ctypes.c_float), ("c_rho", ctypes.c_float),
+        ("fc_start", ctypes.c_float), ("fc_end", ctypes.c_float), ("kill", ctypes.POINTER(ctypes.c_int)),
+        ("offset_mute", ctypes.c_int), ("offsetc", ctypes.c_float), ("timewin", ctypes.c_int),
+        ("gamma", ctypes.c_float), ("twlength_minus", ctypes.c_float), ("src_x", ctypes.c_float),
+        ("src_z", ctypes.c_float),
+    ]
+
+
 class AccumOpts(ctypes.Structure):
     """dn_accum_opts: per-shot energy scaling and circular taper of the gradient assembly."""
     _fields_ = [
@@ -160,6 +172,9 @@ SIGNATURES = {
                                       _c_double_p]),
     "dn_shot_residual": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p, _c_double_p]),
     "dn_shot_rtm_source": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p]),
+    "dn_shot_residual_ex": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p, _P(ResidualOpts), _c_double_p]),
+    "dn_residual_ex": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                      _c_int_p, _c_int_p, _P(ResidualOpts), _c_double_p]),
     "dn_queue_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _P(_vp)]),
     "dn_queue_destroy": (ctypes.c_int, [_vp]),
     "dn_queue_add": (ctypes.c_int, [_vp, _vp, ctypes.c_int]),

@@ -242,6 +242,17 @@ class Shot:
         check(lib.dn_shot_residual(self.handle, comp, fptr(o), ctypes.byref(l2)))
         return l2.value
 
+    def residual_ex(self, obs, comp=_lib.SEC_VX, **opts):
+        """calc_res with the options of dn_residual_opts (lnorm, grad_form, mode, n_order,
+        comp_weight, c_vp, c_rho, fc_start, fc_end, kill, offset_mute, offsetc, timewin,
+        gamma, twlength_minus, src_x, src_z); stores the residual as this component's
+        adjoint source and returns the misfit."""
+        o, keep = residual_opts(**opts)
+        obs = np.ascontiguousarray(obs, np.float32)
+        out = ctypes.c_double()
+        check(lib.dn_shot_residual_ex(self.handle, comp, fptr(obs), ctypes.byref(o), ctypes.byref(out)))
+        return out.value
+
     def rtm_source(self, obs, comp=_lib.SEC_VX):
         """Reverse-time-migration source (calc_res MODE 2): the observed data
         itself, time-reversed and integrated, as this shot's adjoint source."""
@@ -281,6 +292,21 @@ class Shot:
 
     def run_steps(self, mode, nt0, nt1):
         check(lib.dn_run_steps(self.handle, mode, nt0, nt1))
+
+
+def residual_opts(lnorm=2, grad_form=1, mode=1, n_order=0, comp_weight=0, c_vp=0.0, c_rho=0.0, fc_start=0.0,
+                  fc_end=0.0, kill=None, offset_mute=0, offsetc=0.0, timewin=0, gamma=0.0, twlength_minus=1.0,
+                  src_x=0.0, src_z=0.0):
+    """dn_residual_opts and the arrays it points to (keep both alive)."""
+    o = _lib.ResidualOpts(lnorm=lnorm, grad_form=grad_form, mode=mode, n_order=n_order, comp_weight=comp_weight,
+                          c_vp=c_vp, c_rho=c_rho, fc_start=fc_start, fc_end=fc_end, offset_mute=offset_mute,
+                          offsetc=offsetc, timewin=timewin, gamma=gamma, twlength_minus=twlength_minus, src_x=src_x,
+                          src_z=src_z)
+    keep = None
+    if kill is not None:
+        keep = np.ascontiguousarray(kill, np.int32)
+        o.kill = iptr(keep)
+    return o, keep
 
 
 FIELDS = {"vx": 0, "vy": 1, "sxx": 2, "syy": 3, "sxy": 4, "vxp1": 5, "vyp1": 6,

@@ -327,6 +327,34 @@ int dn_shot_residual(dn_shot *s, int comp, const float *obs, double *l2);
  * vs gradient of dn_model_get_gradient). */
 int dn_shot_rtm_source(dn_shot *s, int comp, const float *obs);
 
+/* calc_res (src/calc_res.c) with the objective functions that need no Fourier
+ * transform and its trace selections.  LNORM 6 (envelope, Hilbert transform)
+ * and TIMEWIN 1-4 (picked or STA/LTA windows) are DN_ENOTSUP; LNORM 8 needs
+ * GRAD_FORM 2 (the reference has no AGC array otherwise). */
+typedef struct dn_residual_opts {
+    int lnorm;                /* LNORM: 1 L1 sign, 2 L2, 3 Cauchy, 4 sech, 5 global correlation,
+                                 7 normalised integration, 8 AGC-weighted L2 */
+    int grad_form;            /* GRAD_FORM 1 (time-integrated) or 2 */
+    int mode;                 /* MODE 1 or 3: residual; 2: the RTM source (LNORM 2) */
+    int n_order;              /* N_ORDER time integrations of both sections */
+    int comp_weight;          /* COMP_WEIGHT > 0: both sections times c_vp * c_rho */
+    float c_vp, c_rho;
+    float fc_start, fc_end;   /* LNORM 8: AGC half window iround(2 / ((FC_START + FC_END) DT)) samples */
+    const int *kill;          /* TRKILL: per-trace flags (host array of ntr), 1 = killed; NULL: none */
+    int offset_mute;          /* OFFSET_MUTE 1: mute offsets >= offsetc; 2: offsets <= offsetc */
+    float offsetc;
+    int timewin;              /* TIMEWIN 0, or 5: surface-wave damping of the L2 residual */
+    float gamma, twlength_minus;
+    float src_x, src_z;       /* source position (m), for the offsets */
+} dn_residual_opts;
+/* The residual of one shot's recorded component against obs [ntr][nt] (host),
+ * stored as the shot's adjoint source; *misfit = the objective's value. */
+int dn_shot_residual_ex(dn_shot *s, int comp, const float *obs, const dn_residual_opts *o, double *misfit);
+/* The same on device buffers: syn_tm [nt][ntr], obs and res [ntr][nt];
+ * rec_i/rec_j (host) are the receivers' grid indices for the offsets. */
+int dn_residual_ex(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt, float dh,
+                   const int *rec_i, const int *rec_j, const dn_residual_opts *o, double *misfit);
+
 /* Per-kernel device time of `nsteps` time steps of a batch (direct launches with
  * CUDA events between kernels, for measurement only; leaves the shots' results
  * undefined).  ms_out[8] = average ms per launch of: velocity update, velocity

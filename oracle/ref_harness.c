@@ -670,3 +670,63 @@ int refh_smooth_grad(int nx, int ny, float dh, int spatfilter, float wd_damp, fl
     free_matrix(v, -REFH_PAD, ny + REFH_PAD, -REFH_PAD, nx + REFH_PAD);
     return 0;
 }
+
+/* calc_res (src/calc_res.c) with the options of the objective functions that
+ * need no FFT.  iopt = {lnorm, grad_form, mode, n_order, comp_weight, trkill,
+ * offset_mute, timewin}; fopt = {c_vp, c_rho, offsetc, gamma, twlength_minus,
+ * fc_start, fc_end}; rec_i/rec_j grid indices, (src_x, src_z) metres;
+ * killfile = the TRKILL_FILE (one row of ntr 0/1 flags) relative to the working
+ * directory.  data/syn [ntr][ns] in, residual [ntr][ns] out; returns the misfit. */
+extern int N_ORDER, OFFSET_MUTE, TIMEWIN, TRKILL;
+extern float OFFSETC, GAMMA, TWLENGTH_MINUS, FC_START;
+extern char TRKILL_FILE[STRING_SIZE];
+double refh_calc_res_ex(int ntr, int ns, float dt, float dh, const int *iopt, const float *fopt, const int *rec_i,
+                        const int *rec_j, float src_x, float src_z, const char *killfile, const float *data,
+                        const float *syn, float *diff)
+{
+    MYID = 0;
+    MYID_SHOT = 0;
+    DT = dt;
+    DH = dh;
+    FP = null_log();
+    GRAD_FORM = iopt[1];
+    MODE = iopt[2];
+    N_ORDER = iopt[3];
+    COMP_WEIGHT = iopt[4];
+    TRKILL = iopt[5];
+    OFFSET_MUTE = iopt[6];
+    TIMEWIN = iopt[7];
+    C_vp = fopt[0];
+    C_rho = fopt[1];
+    OFFSETC = fopt[2];
+    GAMMA = fopt[3];
+    TWLENGTH_MINUS = fopt[4];
+    FC_START = fopt[5];
+    FC_END = fopt[6];
+    snprintf(TRKILL_FILE, STRING_SIZE, "%s", killfile ? killfile : "");
+    float **d = matrix(1, ntr, 1, ns), **s = matrix(1, ntr, 1, ns);
+    float **df = matrix(1, ntr, 1, ns), **dfo = matrix(1, ntr, 1, ns);
+    int **recpos = imatrix(1, 3, 1, ntr);
+    float **srcpos = matrix(1, 8, 1, 1);
+    srcpos[1][1] = src_x;
+    srcpos[2][1] = src_z;
+    for (int r = 1; r <= ntr; r++) {
+        recpos[1][r] = rec_i[r - 1];
+        recpos[2][r] = rec_j[r - 1];
+        recpos[3][r] = r;
+        for (int t = 1; t <= ns; t++) {
+            d[r][t] = data[(size_t)(r - 1) * ns + (t - 1)];
+            s[r][t] = syn[(size_t)(r - 1) * ns + (t - 1)];
+        }
+    }
+    double l2 = calc_res(d, s, df, dfo, ntr, ns, iopt[0], 0.0, 0, 1, 1, ntr, recpos, recpos, srcpos, 1, 1, 1);
+    for (int r = 1; r <= ntr; r++)
+        for (int t = 1; t <= ns; t++) diff[(size_t)(r - 1) * ns + (t - 1)] = df[r][t];
+    free_matrix(d, 1, ntr, 1, ns);
+    free_matrix(s, 1, ntr, 1, ns);
+    free_matrix(df, 1, ntr, 1, ns);
+    free_matrix(dfo, 1, ntr, 1, ns);
+    free_imatrix(recpos, 1, 3, 1, ntr);
+    free_matrix(srcpos, 1, 8, 1, 1);
+    return l2;
+}

@@ -289,3 +289,24 @@ def ref_smooth_grad(workdir, nx, ny, dh, spatfilter, wd_damp, wd_damp1, fc_end, 
                          ctypes.c_float(wd_damp), ctypes.c_float(wd_damp1), ctypes.c_float(fc_end), ctypes.c_float(c_vs),
                          jac.encode(), v.ctypes.data_as(_f), g.ctypes.data_as(_f))
     return g.T.copy()
+
+
+def ref_calc_res_ex(workdir, data, syn, dt, dh, iopt, fopt, rec_i, rec_j, src, kill=None):
+    """The reference's calc_res with the options of refh_calc_res_ex; run it in run_isolated()."""
+    os.chdir(workdir)
+    lib = _ref_lib()
+    lib.refh_calc_res_ex.restype = ctypes.c_double
+    d = np.ascontiguousarray(data, np.float32)
+    s = np.ascontiguousarray(syn, np.float32)
+    ntr, ns = d.shape
+    out = np.zeros_like(d)
+    killfile = None
+    if kill is not None:
+        with open("kill.dat", "w") as f:
+            f.write(" ".join(str(int(k)) for k in kill) + "\n")
+        killfile = b"kill.dat"
+    l2 = lib.refh_calc_res_ex(ctypes.c_int(ntr), ctypes.c_int(ns), ctypes.c_float(dt), ctypes.c_float(dh),
+                              _ip(np.asarray(iopt, np.int32)), _fp(np.asarray(fopt, np.float32)), _ip(rec_i),
+                              _ip(rec_j), ctypes.c_float(src[0]), ctypes.c_float(src[1]), killfile,
+                              d.ctypes.data_as(_f), s.ctypes.data_as(_f), out.ctypes.data_as(_f))
+    return out, l2

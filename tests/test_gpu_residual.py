@@ -127,3 +127,66 @@ def test_rtm_source_matches_calc_res_mode2():
     ref.adjoint(want, want_y, None)
     for fid in (7, 8, 9):
         np.testing.assert_array_equal(s.field(fid), ref.field(fid), err_msg=f"accumulator {fid}")
+
+
+# ---------------------------------------------------------------------------
+# the objective functions of calc_res without FFT, on device buffers, against
+# the oracle restatement (pinned to the reference in test_residual_norms.py)
+# ---------------------------------------------------------------------------
+from test_residual_norms import CASES, DH, DT, FOPT, KILL, REC, SRC, oracle_call, sections  # noqa: E402
+
+
+def _ulps(a, b):
+    a = a.view(np.int32).astype(np.int64)
+    b = b.view(np.int32).astype(np.int64)
+    return np.abs(a - b).max() if a.size else 0
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"L{c[0]}gf{c[1]}m{c[2]}n{c[3]}cw{c[4]}k{c[5]}om{c[6]}tw{c[7]}"
+                                            for c in CASES])
+def test_residual_norms_match_oracle(case):
+    import ctypes
+
+    import torch
+
+    from denise_b200 import _lib
+    from denise_b200.api import residual_opts
+
+    obs, syn = sections(case[0])
+    want, wl2 = oracle_call(case, obs, syn)
+    ln, gf, mode, no, cw, tk, om, tw = case
+    o, keep = residual_opts(lnorm=ln, grad_form=gf, mode=mode, n_order=no, comp_weight=cw, c_vp=FOPT[0],
+                            c_rho=FOPT[1], kill=KILL if tk else None, offset_mute=om, offsetc=FOPT[2], timewin=tw,
+                            gamma=FOPT[3], twlength_minus=FOPT[4], fc_start=FOPT[5], fc_end=FOPT[6], src_x=SRC[0],
+                            src_z=SRC[1])
+    d_syn = torch.as_tensor(np.ascontiguousarray(syn.T)).cuda()     # time-major
+    d_obs = torch.as_tensor(obs).cuda()
+    d_res = torch.full_like(d_obs, 7.0)                             # every element must be written
+    l2 = ctypes.c_double()
+    ri, rj = [np.ascontiguousarray(x, np.int32) for x in REC]
+    _lib.check(_lib.lib.dn_residual_ex(d_syn.data_ptr(), d_obs.data_ptr(), d_res.data_ptr(), obs.shape[0],
+                                       obs.shape[1], ctypes.c_float(DT), ctypes.c_float(DH), _lib.iptr(ri),
+                                       _lib.iptr(rj), ctypes.byref(o), ctypes.byref(l2)))
+    got = d_res.cpu().numpy()
+    if ln == 4 or tw == 5:
+        # tanh / exp in double: CUDA's and the C library's may differ in the last bit of the double
+        assert _ulps(got, want) <= 1
+    else:
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert abs(l2.value - wl2) <= 1e-12 * max(abs(wl2), 1e-300)
+
+
+def test_residual_ex_on_a_shot_and_unsupported_options():
+    p, model, src, rec = small_case(store_snapshots=1)
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run([s], dn.MODE_FORWARD)
+    syn = s.sections(dn.SEC_VY)
+    obs = (0.8 * syn).astype(np.float32)
+    a = s.residual(obs, dn.SEC_VY)
+    b = s.residual_ex(obs, dn.SEC_VY, lnorm=2, grad_form=p.grad_form)
+    assert a == b
+    for bad, code in ((dict(lnorm=6), "DN_ENOTSUP"), (dict(lnorm=8, grad_form=1), "DN_EINVAL"),
+                      (dict(timewin=3), "DN_ENOTSUP"), (dict(lnorm=9), "DN_EINVAL")):
+        with pytest.raises(dn.DeniseError, match=code):
+            s.residual_ex(obs, dn.SEC_VY, **bad)
+    m.close()
