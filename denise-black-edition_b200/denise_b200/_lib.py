@@ -172,6 +172,10 @@ SIGNATURES = {
                                       _c_double_p]),
     "dn_shot_residual": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p, _c_double_p]),
     "dn_shot_rtm_source": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p]),
+    "dn_tdfilt": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_float,
+                                 ctypes.c_float]),
+    "dn_tdfilt_host": (ctypes.c_int, [_c_float_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                      ctypes.c_float, ctypes.c_float, ctypes.c_int]),
     "dn_shot_residual_ex": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p, _P(ResidualOpts), _c_double_p]),
     "dn_residual_ex": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                       _c_int_p, _c_int_p, _P(ResidualOpts), _c_double_p]),

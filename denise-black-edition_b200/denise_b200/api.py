@@ -294,6 +294,17 @@ class Shot:
         check(lib.dn_run_steps(self.handle, mode, nt0, nt1))
 
 
+def tdfilt(traces, dt, order, fc_low, fc_high=0.0, device=0):
+    """apply_tdfilt: Butterworth low-pass at fc_low, then high-pass at fc_high if > 0, of
+    [ntr][ns] traces (host array; a filtered copy is returned)."""
+    a = np.array(traces, np.float32, copy=True, order="C")
+    two_d = a.ndim == 2
+    a = a.reshape(-1, a.shape[-1])
+    check(lib.dn_tdfilt_host(fptr(a), a.shape[0], a.shape[1], ctypes.c_float(dt), int(order),
+                             ctypes.c_float(fc_low), ctypes.c_float(fc_high), int(device)))
+    return a if two_d else a.reshape(-1)
+
+
 def residual_opts(lnorm=2, grad_form=1, mode=1, n_order=0, comp_weight=0, c_vp=0.0, c_rho=0.0, fc_start=0.0,
                   fc_end=0.0, kill=None, offset_mute=0, offsetc=0.0, timewin=0, gamma=0.0, twlength_minus=1.0,
                   src_x=0.0, src_z=0.0):

@@ -142,12 +142,24 @@ def dot(a, b):
 class FWI:
     """FWI iterations for one grid: shots (src_i, src_j, signals, rec_i, rec_j)
     with observed data obs[k] = (vx, vy) [ntr][nt]; `params` must store
-    snapshots.  limits: (vp_lo, vp_hi, vs_lo, vs_hi, rho_lo, rho_hi)."""
+    snapshots.  limits: (vp_lo, vp_hi, vs_lo, vs_hi, rho_lo, rho_hi).
+    precond: a precond.PrecondConfig applied to every stacked gradient;
+    shot_taper: (srtshape, srtradius, filtsize) of the per-shot circular taper;
+    time_filter: (order, fc, fc_start) band-limiting sources and data."""
 
     def __init__(self, params, model, shots, obs, limits, device=0, nlbfgs=20, eps_scale=0.01, scalefac=2.0,
-                 stepmax=4, dist=None, precond=None, shot_taper=None):
+                 stepmax=4, dist=None, precond=None, shot_taper=None, time_filter=None):
         self.p = params
         self.vp, self.vs, self.rho = [np.ascontiguousarray(a, np.float32) for a in model[:3]]
+        if time_filter is not None:
+            # TIME_FILT (grad_obj_psv.c:151-155, calc_res_PSV.c): the source signals and the
+            # observed data are band-limited by apply_tdfilt(ORDER, FC, FC_START)
+            from .api import tdfilt
+
+            order, fc, fc_start = time_filter
+            shots = [tuple(sh[:2]) + (tdfilt(sh[2], params.dt, order, fc, fc_start, device),) + tuple(sh[3:])
+                     for sh in shots]
+            obs = [tuple(tdfilt(o, params.dt, order, fc, fc_start, device) for o in ob) for ob in obs]
         self.shots, self.obs, self.limits = shots, obs, limits
         self.device, self.dist = device, dist
         self.eps_scale, self.scalefac, self.stepmax = eps_scale, scalefac, stepmax

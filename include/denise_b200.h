@@ -355,6 +355,16 @@ int dn_shot_residual_ex(dn_shot *s, int comp, const float *obs, const dn_residua
 int dn_residual_ex(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt, float dh,
                    const int *rec_i, const int *rec_j, const dn_residual_opts *o, double *misfit);
 
+/* apply_tdfilt (src/apply_tdfilt.c, TIME_FILT and the QUELLART 6 spike band):
+ * Butterworth low-pass of `order` (1..16) at corner fc_low, then, if
+ * fc_high > 0, high-pass at fc_high - the recursive filters of libcseife's
+ * seife_lpb/seife_hpb that timedomain_filt.c calls, in double, with the
+ * reference's float conversions around each and its last sample of every
+ * trace left unfiltered.  traces [ntr][ns], in place: device memory
+ * (dn_tdfilt) or host memory (dn_tdfilt_host, filtered on `device`). */
+int dn_tdfilt(float *traces, int ntr, int ns, float dt, int order, float fc_low, float fc_high);
+int dn_tdfilt_host(float *traces, int ntr, int ns, float dt, int order, float fc_low, float fc_high, int device);
+
 /* Per-kernel device time of `nsteps` time steps of a batch (direct launches with
  * CUDA events between kernels, for measurement only; leaves the shots' results
  * undefined).  ms_out[8] = average ms per launch of: velocity update, velocity

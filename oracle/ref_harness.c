@@ -730,3 +730,17 @@ double refh_calc_res_ex(int ntr, int ns, float dt, float dh, const int *iopt, co
     free_matrix(srcpos, 1, 8, 1, 1);
     return l2;
 }
+
+/* apply_tdfilt (src/apply_tdfilt.c) on [ntr][ns] traces in place. */
+int refh_apply_tdfilt(int ntr, int ns, float dt, int order, float fc2, float fc1, float *data)
+{
+    DT = dt;
+    float **s = matrix(1, ntr, 1, ns);
+    for (int r = 1; r <= ntr; r++)
+        for (int t = 1; t <= ns; t++) s[r][t] = data[(size_t)(r - 1) * ns + (t - 1)];
+    apply_tdfilt(s, ntr, ns, order, fc2, fc1);
+    for (int r = 1; r <= ntr; r++)
+        for (int t = 1; t <= ns; t++) data[(size_t)(r - 1) * ns + (t - 1)] = s[r][t];
+    free_matrix(s, 1, ntr, 1, ns);
+    return 0;
+}

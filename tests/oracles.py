@@ -310,3 +310,12 @@ def ref_calc_res_ex(workdir, data, syn, dt, dh, iopt, fopt, rec_i, rec_j, src, k
                               _ip(rec_j), ctypes.c_float(src[0]), ctypes.c_float(src[1]), killfile,
                               d.ctypes.data_as(_f), s.ctypes.data_as(_f), out.ctypes.data_as(_f))
     return out, l2
+
+
+def ref_apply_tdfilt(data, dt, order, fc2, fc1):
+    """The reference's apply_tdfilt on [ntr][ns] float32 traces; run it in run_isolated()."""
+    lib = _ref_lib()
+    d = np.ascontiguousarray(data, np.float32).copy()
+    lib.refh_apply_tdfilt(ctypes.c_int(d.shape[0]), ctypes.c_int(d.shape[1]), ctypes.c_float(dt), ctypes.c_int(order),
+                          ctypes.c_float(fc2), ctypes.c_float(fc1), d.ctypes.data_as(_f))
+    return d

@@ -124,3 +124,28 @@ def test_fwi_with_gradient_conditioning():
     assert all(h["found"] for h in f.history), f.history
     assert L1 < L0, (L0, L1)
     f.lbfgs.close()
+
+
+def test_fwi_with_time_filter():
+    """TIME_FILT: sources and observed data are band-limited before the iteration."""
+    import denise_b200 as dn
+
+    req = _request(0, "gradient", 90, 60, 500, 8, 0, 4, 11)
+    p = req.params
+    vp, vs, rho = req.model
+    vpt, vst, rhot = synth.add_ellipse(vp, vs, rho, p.dh, 3, v=3600.0)
+    m = dn.Model(p.replace(store_snapshots=0), vpt, vst, rhot)
+    ss = [dn.Shot(m, *sh[:5]) for sh in req.shots]
+    dn.run(ss)
+    obs = [(s.sections(dn.SEC_VX), s.sections(dn.SEC_VY)) for s in ss]
+    for s in ss:
+        s.close()
+    m.close()
+    start = tuple(synth.smoothed(a, 3.0) for a in (vp, vs, rho))
+    lim = (1000.0, 6000.0, 500.0, 3500.0, 1000.0, 3500.0)
+    f = fwi.FWI(p, start, req.shots, obs, lim, device=0, nlbfgs=5, eps_scale=0.01, time_filter=(4, 30.0, 2.0))
+    np.testing.assert_array_equal(f.shots[0][2], dn.tdfilt(req.shots[0][2], p.dt, 4, 30.0, 2.0))
+    np.testing.assert_array_equal(f.obs[1][0], dn.tdfilt(obs[1][0], p.dt, 4, 30.0, 2.0))
+    L0 = f.iterate(1)
+    assert np.isfinite(L0) and f.history[0]["found"]
+    f.lbfgs.close()
