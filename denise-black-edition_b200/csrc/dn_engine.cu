@@ -989,6 +989,9 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c, con
     // DN_KERNEL=tma, the bulk-copy row pipeline of dn_kernels_tma.cuh
     const char *kern = getenv("DN_KERNEL");
     c.tma = c.bx == TMA_W && kern && strcmp(kern, "tma") == 0;
+    // paired-column FP32x2 kernels (default; DN_PACK=0 selects the one-column kernels)
+    const char *pk = getenv("DN_PACK");
+    c.pack = !c.tma && !(pk && strcmp(pk, "0") == 0);
     c.any_surf = c.any_src_s = c.any_store = c.any_adj = c.any_rec = false;
     int maxtiles = 0, maxsrc = 1, maxnx = 1, maxtr = 1;
     for (int k = 0; k < n; k++) {

@@ -294,6 +294,209 @@ __global__ void __maxnreg__(40) k_update_v(const Inst *__restrict__ insts, const
 }
 
 // ===========================================================================
+// Paired-column kernels: each thread owns two adjacent columns (i0, i0 + 1),
+// i0 odd, and computes both with the packed FP32x2 instructions of sm_100
+// (__fadd2_rn, __fmul2_rn, __ffma2_rn: per lane the same IEEE operation as
+// the scalar intrinsic, so results stay bit-identical).  Fields are read as
+// float2 (column i0 of the padded layout sits at an even element, so the pair
+// is 8-byte aligned); an x stencil needs one pair per offset, half of which
+// straddle two loaded pairs and are assembled from them.  z neighbours are
+// read from L1 row by row (no register window), which keeps the kernels at
+// 64 registers or fewer.  Per cell this issues roughly a third of the
+// instructions of the one-column kernels above, which were bound by
+// instruction issue, not by DRAM.
+// ===========================================================================
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+// The compiler contracts a packed product feeding a packed sum into one fused
+// multiply-add (one rounding instead of two) although both are _rn intrinsics
+// (measured on sm_100a: 1-ulp differences in the stencil sums; the scalar
+// _rn intrinsics are never contracted).  An empty asm statement that takes the
+// product as a 64-bit register hides it from that rewrite.
+__device__ __forceinline__ float2 opaque2(float2 a)
+{
+    unsigned long long u = ((unsigned long long)__float_as_uint(a.y) << 32) | __float_as_uint(a.x);
+    asm volatile("" : "+l"(u));
+    return make_float2(__uint_as_float((unsigned)u), __uint_as_float((unsigned)(u >> 32)));
+}
+template <bool X> __device__ __forceinline__ float2 MUL2(float2 a, float2 b) { return opaque2(__fmul2_rn(a, b)); }
+template <bool X> __device__ __forceinline__ float2 ADD2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b as a + (-b): IEEE defines subtraction as addition of the negation (same bits, signed zeros included)
+template <bool X> __device__ __forceinline__ float2 SUB2(float2 a, float2 b) { return __fadd2_rn(a, neg2(b)); }
+__device__ __forceinline__ float2 ld2(const float *p) { return __ldg(reinterpret_cast<const float2 *>(p)); }
+__device__ __forceinline__ void pf_l1(const float *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+#ifndef DN_PF_ROWS
+#define DN_PF_ROWS 1
+#endif
+__device__ __forceinline__ float2 ldw2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+
+// division by DH of both lanes, as DIVH per lane
+template <bool X>
+__device__ __forceinline__ float2 DIVH2(float2 a, bool fd, float DH, float rdh)
+{
+    if (!X) return __fmul2_rn(a, bc2(rdh));
+    if (!fd) return make_float2(__fdiv_rn(a.x, DH), __fdiv_rn(a.y, DH));
+    const float2 q = __fmul2_rn(a, bc2(rdh));
+    const float2 r = __ffma2_rn(neg2(q), bc2(DH), a);
+    float2 q1 = __ffma2_rn(r, bc2(rdh), q);
+    const float ax = fabsf(a.x), ay = fabsf(a.y);
+    if (!(ax >= 0x1p-100f && ax <= 0x1p100f)) q1.x = a.x == 0.0f ? q.x : __fdiv_rn(a.x, DH);
+    if (!(ay >= 0x1p-100f && ay <= 0x1p100f)) q1.y = a.y == 0.0f ? q.y : __fdiv_rn(a.y, DH);
+    return q1;
+}
+
+template <int R, bool X>
+__global__ void __launch_bounds__(128, 8) k_update_v2(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+{
+    const Inst &I = insts[blockIdx.y];
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt) return;
+    const int b = blockIdx.x;
+    if (b >= I.tiles) return;
+    const int bxw = 2 * blockDim.x;
+    const int tx = b % I.tiles_x, tz = b / I.tiles_x;
+    const int i0 = tx * bxw + 2 * threadIdx.x + 1;
+    if (i0 > I.nx) return;
+    const int j0 = tz * I.zch + 1, j1 = min(j0 + I.zch - 1, I.ny);
+    const bool two = i0 + 1 <= I.nx;
+    const long long P = I.pitch;
+    float hc[R + 1];
+#pragma unroll
+    for (int m = 1; m <= R; m++) hc[m] = I.hc[m];
+    const float DT = I.DT, DH = I.DH, rdh = I.rdh;
+    const bool fd = I.fastdiv;
+    const int mode = I.mode;
+    const bool snapstep = (mode == 0) && I.store && ((nt - 1) % I.dtinv == 0);
+    const int fw = I.fw, nx = I.nx, ny = I.ny, free_surf = I.free_surf;
+    const bool xframe = fw > 0 && (i0 <= fw || i0 + 1 >= nx - fw + 1);
+    for (int j = j0; j <= j1; j++) {
+        const long long o = (long long)j * P + i0;
+        // the lines row j + 1 reads first (its new z-stencil rows and its own-row operands) are
+        // requested into L1 now; every address stays inside the padded planes (rows up to ny + R + 1)
+        {
+            constexpr int D = DN_PF_ROWS;   // rows ahead; D <= HZ - R keeps the addresses inside the planes
+            pf_l1(I.syy + o + (R + D) * P);
+            pf_l1(I.sxy + o + (R - 1 + D) * P);
+            pf_l1(I.sxx + o + D * P);
+            pf_l1(I.rip + o + D * P);
+            pf_l1(I.rjp + o + D * P);
+            pf_l1(I.vx + o + D * P);
+            pf_l1(I.vy + o + D * P);
+        }
+        // sxx x stencil of lane 0: columns i0-R+1 .. i0+R (A[k], k = 0..2R); pairs (A[k], A[k+1]);
+        // column i0-R+1+k is odd when k - R is odd
+        float2 ax[2 * R];
+        {
+            const float *row = I.sxx + o - R + 1;   // A[0]
+            constexpr int kb = (R % 2 == 0) ? -1 : 0;   // first aligned k
+            float2 L[R + 1];
+#pragma unroll
+            for (int q = 0; q <= R; q++) L[q] = ld2(row + kb + 2 * q);
+#pragma unroll
+            for (int k = 0; k < 2 * R; k++) {
+                if (((k - kb) & 1) == 0) ax[k] = L[(k - kb) / 2];
+                else ax[k] = make_float2(L[(k - 1 - kb) / 2].y, L[(k + 1 - kb) / 2].x);
+            }
+        }
+        // sxy x stencil of lane 0: columns i0-R .. i0+R-1 (B[k], k = 0..2R); column i0-R+k odd when k - R even
+        float2 bx[2 * R];
+        {
+            const float *row = I.sxy + o - R;       // B[0]
+            constexpr int kb = (R % 2 == 0) ? 0 : -1;
+            float2 L[R + 1];
+#pragma unroll
+            for (int q = 0; q <= R; q++) L[q] = ld2(row + kb + 2 * q);
+#pragma unroll
+            for (int k = 0; k < 2 * R; k++) {
+                if (((k - kb) & 1) == 0) bx[k] = L[(k - kb) / 2];
+                else bx[k] = make_float2(L[(k - 1 - kb) / 2].y, L[(k + 1 - kb) / 2].x);
+            }
+        }
+        // derivatives, in the reference's term order (update_v_PML_PSV.c case 8 :366-480)
+        float2 sxx_x = MUL2<X>(bc2(hc[1]), SUB2<X>(ax[R], ax[R - 1]));
+        float2 sxy_x = MUL2<X>(bc2(hc[1]), SUB2<X>(bx[R], bx[R - 1]));
+        float2 sxy_y = MUL2<X>(bc2(hc[1]), SUB2<X>(ld2(I.sxy + o), ld2(I.sxy + o - P)));
+        float2 syy_y = MUL2<X>(bc2(hc[1]), SUB2<X>(ld2(I.syy + o + P), ld2(I.syy + o)));
+#pragma unroll
+        for (int m = 2; m <= R; m++) {
+            sxx_x = ADD2<X>(sxx_x, MUL2<X>(bc2(hc[m]), SUB2<X>(ax[R - 1 + m], ax[R - m])));
+            sxy_x = ADD2<X>(sxy_x, MUL2<X>(bc2(hc[m]), SUB2<X>(bx[R + m - 1], bx[R - m])));
+            sxy_y = ADD2<X>(sxy_y, MUL2<X>(bc2(hc[m]), SUB2<X>(ld2(I.sxy + o + (m - 1) * P), ld2(I.sxy + o - m * P))));
+            syy_y = ADD2<X>(syy_y, MUL2<X>(bc2(hc[m]), SUB2<X>(ld2(I.syy + o + m * P), ld2(I.syy + o - (m - 1) * P))));
+        }
+        if (xframe) {
+            // per lane: left frame h = i, right frame h1 = i - nx + 2 fw (both when they overlap)
+            float *sx = &sxx_x.x, *sy = &sxy_x.x;
+            for (int lane = 0; lane < 2; lane++) {
+                const int i = i0 + lane;
+                if (i > nx || !(i <= fw || i >= nx - fw + 1)) continue;
+                for (int side = 0; side < 2; side++) {
+                    if (side == 0 ? (i > fw) : (i < nx - fw + 1)) continue;
+                    const int h = side == 0 ? i - 1 : i - nx + 2 * fw - 1;
+                    float *ps = I.psi_sxx_x + (long long)(j - 1) * 2 * fw + h;
+                    float v = ADD<X>(MUL<X>(I.b_xh[h], *ps), MUL<X>(I.a_xh[h], sx[lane]));
+                    *ps = v;
+                    sx[lane] = ADD<X>(DIVK<X>(sx[lane], I.K_xh[h]), v);
+                    float *pq = I.psi_sxy_x + (long long)(j - 1) * 2 * fw + h;
+                    float w = ADD<X>(MUL<X>(I.b_x[h], *pq), MUL<X>(I.a_x[h], sy[lane]));
+                    *pq = w;
+                    sy[lane] = ADD<X>(DIVK<X>(sy[lane], I.K_x[h]), w);
+                }
+            }
+        }
+        if (fw > 0 && ((!free_surf && j <= fw) || j >= ny - fw + 1)) {
+            float *sy = &syy_y.x, *sx = &sxy_y.x;
+            for (int lane = 0; lane < 2; lane++) {
+                const int i = i0 + lane;
+                if (i > nx) continue;
+                for (int side = 0; side < 2; side++) {
+                    if (side == 0 ? (free_surf || j > fw) : (j < ny - fw + 1)) continue;
+                    const int h = side == 0 ? j - 1 : j - ny + 2 * fw - 1;
+                    float *ps = I.psi_syy_y + (long long)h * nx + (i - 1);
+                    float v = ADD<X>(MUL<X>(I.b_yh[h], *ps), MUL<X>(I.a_yh[h], sy[lane]));
+                    *ps = v;
+                    sy[lane] = ADD<X>(DIVK<X>(sy[lane], I.K_yh[h]), v);
+                    float *pq = I.psi_sxy_y + (long long)h * nx + (i - 1);
+                    float w = ADD<X>(MUL<X>(I.b_y[h], *pq), MUL<X>(I.a_y[h], sx[lane]));
+                    *pq = w;
+                    sx[lane] = ADD<X>(DIVK<X>(sx[lane], I.K_y[h]), w);
+                }
+            }
+        }
+        const float2 ripv = ld2(I.rip + o), rjpv = ld2(I.rjp + o);
+        const float2 vxo = ldw2(I.vx + o), vyo = ldw2(I.vy + o);
+        const float2 s1 = ADD2<X>(sxx_x, sxy_y);
+        const float2 s2 = ADD2<X>(sxy_x, syy_y);
+        const float2 nvx = ADD2<X>(vxo, DIVH2<X>(MUL2<X>(MUL2<X>(bc2(DT), ripv), s1), fd, DH, rdh));
+        const float2 nvy = ADD2<X>(vyo, DIVH2<X>(MUL2<X>(MUL2<X>(bc2(DT), rjpv), s2), fd, DH, rdh));
+        float2 p1x, p1y;
+        const bool wp = snapstep || mode == 1;
+        if (snapstep) {
+            p1x = DIVH2<X>(MUL2<X>(ripv, s1), fd, DH, rdh);
+            p1y = DIVH2<X>(MUL2<X>(rjpv, s2), fd, DH, rdh);
+        } else if (mode == 1) {
+            p1x = ADD2<X>(ldw2(I.vxp1 + o), MUL2<X>(bc2(DT), vxo));
+            p1y = ADD2<X>(ldw2(I.vyp1 + o), MUL2<X>(bc2(DT), vyo));
+        }
+        if (two) {
+            *reinterpret_cast<float2 *>(I.vx + o) = nvx;
+            *reinterpret_cast<float2 *>(I.vy + o) = nvy;
+            if (wp) {
+                *reinterpret_cast<float2 *>(I.vxp1 + o) = p1x;
+                *reinterpret_cast<float2 *>(I.vyp1 + o) = p1y;
+            }
+        } else {   // the last column of an odd nx: column nx + 1 is halo and stays zero
+            I.vx[o] = nvx.x;
+            I.vy[o] = nvy.x;
+            if (wp) {
+                I.vxp1[o] = p1x.x;
+                I.vyp1[o] = p1y.x;
+            }
+        }
+    }
+}
+
+// ===========================================================================
 // Force sources (update_v_PML_PSV.c:738-752) and adjoint residual forces
 // (:755-768).  One thread per unique source cell; sources sharing a cell are
 // added in their list order, as the reference's sequential loop does.
@@ -497,6 +700,159 @@ __global__ void __launch_bounds__(256, 4) k_update_s_el(const Inst *__restrict__
         sxx[o] = F(DADD((double)s_xx, DADD((double)gdiv, DMUL(f2, (double)vxx))));
         syy[o] = F(DADD((double)s_yy, DADD((double)gdiv, DMUL(f2, (double)vyy))));
         D.shift();
+    }
+}
+
+// ===========================================================================
+// Paired-column stress derivatives: vxx, vyx, vxy, vyy of update_s_*_PML_PSV.c
+// for columns (i0, i0 + 1), times dhi, then the CPML correction per lane
+// (the scalar VDeriv::compute, two lanes at a time).
+// ===========================================================================
+template <int R, bool X>
+__device__ __forceinline__ void vderiv2(const Inst &I, const float *hc, int i0, int j, long long o, long long P,
+                                        float dhi, float2 &vxx, float2 &vyx, float2 &vxy, float2 &vyy)
+{
+    // vx x stencil of lane 0: columns i0-R .. i0+R-1 (C[k]); column i0-R+k odd when k - R is even
+    float2 cx[2 * R], dx[2 * R];
+    {
+        const float *row = I.vx + o - R;
+        constexpr int kb = (R % 2 == 0) ? 0 : -1;
+        float2 L[R + 1];
+#pragma unroll
+        for (int q = 0; q <= R; q++) L[q] = ldw2(row + kb + 2 * q);
+#pragma unroll
+        for (int k = 0; k < 2 * R; k++) {
+            if (((k - kb) & 1) == 0) cx[k] = L[(k - kb) / 2];
+            else cx[k] = make_float2(L[(k - 1 - kb) / 2].y, L[(k + 1 - kb) / 2].x);
+        }
+    }
+    // vy x stencil of lane 0: columns i0-R+1 .. i0+R (D[k]); column i0-R+1+k odd when k - R is odd
+    {
+        const float *row = I.vy + o - R + 1;
+        constexpr int kb = (R % 2 == 0) ? -1 : 0;
+        float2 L[R + 1];
+#pragma unroll
+        for (int q = 0; q <= R; q++) L[q] = ldw2(row + kb + 2 * q);
+#pragma unroll
+        for (int k = 0; k < 2 * R; k++) {
+            if (((k - kb) & 1) == 0) dx[k] = L[(k - kb) / 2];
+            else dx[k] = make_float2(L[(k - 1 - kb) / 2].y, L[(k + 1 - kb) / 2].x);
+        }
+    }
+    float2 a = MUL2<X>(bc2(hc[1]), SUB2<X>(cx[R], cx[R - 1]));
+    float2 b = MUL2<X>(bc2(hc[1]), SUB2<X>(dx[R], dx[R - 1]));
+    float2 c = MUL2<X>(bc2(hc[1]), SUB2<X>(ldw2(I.vx + o + P), ldw2(I.vx + o)));
+    float2 d = MUL2<X>(bc2(hc[1]), SUB2<X>(ldw2(I.vy + o), ldw2(I.vy + o - P)));
+#pragma unroll
+    for (int m = 2; m <= R; m++) {
+        a = ADD2<X>(a, MUL2<X>(bc2(hc[m]), SUB2<X>(cx[R + m - 1], cx[R - m])));
+        b = ADD2<X>(b, MUL2<X>(bc2(hc[m]), SUB2<X>(dx[R - 1 + m], dx[R - m])));
+        c = ADD2<X>(c, MUL2<X>(bc2(hc[m]), SUB2<X>(ldw2(I.vx + o + m * P), ldw2(I.vx + o - (m - 1) * P))));
+        d = ADD2<X>(d, MUL2<X>(bc2(hc[m]), SUB2<X>(ldw2(I.vy + o + (m - 1) * P), ldw2(I.vy + o - m * P))));
+    }
+    vxx = MUL2<X>(a, bc2(dhi));
+    vyx = MUL2<X>(b, bc2(dhi));
+    vxy = MUL2<X>(c, bc2(dhi));
+    vyy = MUL2<X>(d, bc2(dhi));
+    const int fw = I.fw, nx = I.nx, ny = I.ny;
+    if (fw > 0 && (i0 <= fw || i0 + 1 >= nx - fw + 1)) {
+        float *px = &vxx.x, *py = &vyx.x;
+        for (int lane = 0; lane < 2; lane++) {
+            const int i = i0 + lane;
+            if (i > nx || !(i <= fw || i >= nx - fw + 1)) continue;
+            for (int side = 0; side < 2; side++) {
+                if (side == 0 ? (i > fw) : (i < nx - fw + 1)) continue;
+                const int h = side == 0 ? i - 1 : i - nx + 2 * fw - 1;
+                float *p1 = I.psi_vxx + (long long)(j - 1) * 2 * fw + h;
+                float v = ADD<X>(MUL<X>(I.b_x[h], *p1), MUL<X>(I.a_x[h], px[lane]));
+                *p1 = v;
+                px[lane] = ADD<X>(DIVK<X>(px[lane], I.K_x[h]), v);
+                float *p2 = I.psi_vyx + (long long)(j - 1) * 2 * fw + h;
+                float w = ADD<X>(MUL<X>(I.b_xh[h], *p2), MUL<X>(I.a_xh[h], py[lane]));
+                *p2 = w;
+                py[lane] = ADD<X>(DIVK<X>(py[lane], I.K_xh[h]), w);
+            }
+        }
+    }
+    if (fw > 0 && ((!I.free_surf && j <= fw) || j >= ny - fw + 1)) {
+        float *pyy = &vyy.x, *pxy = &vxy.x;
+        for (int lane = 0; lane < 2; lane++) {
+            const int i = i0 + lane;
+            if (i > nx) continue;
+            for (int side = 0; side < 2; side++) {
+                if (side == 0 ? (I.free_surf || j > fw) : (j < ny - fw + 1)) continue;
+                const int h = side == 0 ? j - 1 : j - ny + 2 * fw - 1;
+                float *p1 = I.psi_vyy + (long long)h * nx + (i - 1);
+                float *p2 = I.psi_vxy + (long long)h * nx + (i - 1);
+                float v = ADD<X>(MUL<X>(I.b_y[h], *p1), MUL<X>(I.a_y[h], pyy[lane]));
+                float w = ADD<X>(MUL<X>(I.b_yh[h], *p2), MUL<X>(I.a_yh[h], pxy[lane]));
+                *p1 = v;
+                *p2 = w;
+                pyy[lane] = ADD<X>(DIVK<X>(pyy[lane], I.K_y[h]), v);
+                pxy[lane] = ADD<X>(DIVK<X>(pxy[lane], I.K_yh[h]), w);
+            }
+        }
+    }
+}
+
+// float2 store of a lane pair, or lane 0 alone for the last column of an odd nx
+__device__ __forceinline__ void st2(float *p, float2 v, bool two)
+{
+    if (two) *reinterpret_cast<float2 *>(p) = v;
+    else *p = v.x;
+}
+
+// Paired-column elastic stress update (k_update_s_el for two columns per thread).
+template <int R, bool X>
+__global__ void __launch_bounds__(128, 8) k_update_s_el2(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+{
+    const Inst &I = insts[blockIdx.y];
+    const int nt = *ntb + off - I.t0;   // the instance's own time step
+    if (nt < 1 || nt > I.nt) return;
+    const int b = blockIdx.x;
+    if (b >= I.tiles) return;
+    const int bxw = 2 * blockDim.x;
+    const int tx = b % I.tiles_x, tz = b / I.tiles_x;
+    const int i0 = tx * bxw + 2 * threadIdx.x + 1;
+    if (i0 > I.nx) return;
+    const int j0 = tz * I.zch + 1, j1 = min(j0 + I.zch - 1, I.ny);
+    const bool two = i0 + 1 <= I.nx;
+    const long long P = I.pitch;
+    float hc[R + 1];
+#pragma unroll
+    for (int m = 1; m <= R; m++) hc[m] = I.hc[m];
+    const float dhi = I.dhi_el;
+    for (int j = j0; j <= j1; j++) {
+        const long long o = (long long)j * P + i0;
+        {
+            constexpr int D = DN_PF_ROWS;
+            pf_l1(I.vx + o + (R + D) * P);
+            pf_l1(I.vy + o + (R - 1 + D) * P);
+            pf_l1(I.uipjp + o + D * P);
+            pf_l1(I.mu + o + D * P);
+            pf_l1(I.lam + o + D * P);
+            pf_l1(I.sxx + o + D * P);
+            pf_l1(I.syy + o + D * P);
+            pf_l1(I.sxy + o + D * P);
+        }
+        float2 vxx, vyx, vxy, vyy;
+        vderiv2<R, X>(I, hc, i0, j, o, P, dhi, vxx, vyx, vxy, vyy);
+        const float2 fipjp = ld2(I.uipjp + o), f = ld2(I.mu + o), g = ld2(I.lam + o);
+        const float2 s_xx = ldw2(I.sxx + o), s_yy = ldw2(I.syy + o), s_xy = ldw2(I.sxy + o);
+        const float2 div = ADD2<X>(vxx, vyy);
+        const float2 gdiv = MUL2<X>(g, div);
+        const float2 nsxy = ADD2<X>(s_xy, MUL2<X>(fipjp, ADD2<X>(vyx, vxy)));
+        float2 nsxx, nsyy;
+        {
+            const double f2x = 2.0 * (double)f.x, f2y = 2.0 * (double)f.y;
+            nsxx.x = F(DADD((double)s_xx.x, DADD((double)gdiv.x, DMUL(f2x, (double)vxx.x))));
+            nsxx.y = F(DADD((double)s_xx.y, DADD((double)gdiv.y, DMUL(f2y, (double)vxx.y))));
+            nsyy.x = F(DADD((double)s_yy.x, DADD((double)gdiv.x, DMUL(f2x, (double)vyy.x))));
+            nsyy.y = F(DADD((double)s_yy.y, DADD((double)gdiv.y, DMUL(f2y, (double)vyy.y))));
+        }
+        st2(I.sxy + o, nsxy, two);
+        st2(I.sxx + o, nsxx, two);
+        st2(I.syy + o, nsyy, two);
     }
 }
 

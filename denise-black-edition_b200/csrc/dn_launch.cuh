@@ -14,6 +14,7 @@ struct LaunchCfg {
     int R, L;
     bool exact;
     bool tma;   // stencil kernels fed by the bulk-copy row pipeline
+    bool pack;  // paired-column (FP32x2) stencil kernels, bx / 2 threads per tile
     bool any_surf, any_src_s, any_store, any_adj, any_rec;
 };
 

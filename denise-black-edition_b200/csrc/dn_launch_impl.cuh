@@ -12,6 +12,7 @@ void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int
 {
     MARK(0);
     if (c.tma) k_update_v_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QV>(slot_floats_v()), st>>>(d, ntb, off);
+    else if (c.pack) k_update_v2<R, X><<<c.tile_grid, c.bx / 2, 0, st>>>(d, ntb, off);
     else k_update_v<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
     MARK(1);
     k_inject_v<<<c.src_grid, 128, 0, st>>>(d, ntb, off);
@@ -20,6 +21,7 @@ void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int
     if (c.L == 0) {
         if (c.tma)
             k_update_s_el_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QS_EL>(slot_floats_s_el()), st>>>(d, ntb, off);
+        else if (c.pack) k_update_s_el2<R, X><<<c.tile_grid, c.bx / 2, 0, st>>>(d, ntb, off);
         else k_update_s_el<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
     } else if (c.tma) {
 #define DN_VI_TMA(LL)                                                                                          \
