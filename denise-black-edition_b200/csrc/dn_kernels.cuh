@@ -324,11 +324,11 @@ template <bool X> __device__ __forceinline__ float2 ADD2(float2 a, float2 b) { r
 // a - b as a + (-b): IEEE defines subtraction as addition of the negation (same bits, signed zeros included)
 template <bool X> __device__ __forceinline__ float2 SUB2(float2 a, float2 b) { return __fadd2_rn(a, neg2(b)); }
 __device__ __forceinline__ float2 ld2(const float *p) { return __ldg(reinterpret_cast<const float2 *>(p)); }
+__device__ __forceinline__ float2 ldw2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 __device__ __forceinline__ void pf_l1(const float *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 #ifndef DN_PF_ROWS
 #define DN_PF_ROWS 1
 #endif
-__device__ __forceinline__ float2 ldw2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 
 // division by DH of both lanes, as DIVH per lane
 template <bool X>
