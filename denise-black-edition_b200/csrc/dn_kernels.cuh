@@ -330,6 +330,13 @@ __device__ __forceinline__ void pf_l1(const float *p) { asm volatile("prefetch.g
 #define DN_PF_ROWS 1
 #endif
 
+// float2 store of a lane pair, or lane 0 alone for the last column of an odd nx
+__device__ __forceinline__ void st2(float *p, float2 v, bool two)
+{
+    if (two) *reinterpret_cast<float2 *>(p) = v;
+    else *p = v.x;
+}
+
 // division by DH of both lanes, as DIVH per lane
 template <bool X>
 __device__ __forceinline__ float2 DIVH2(float2 a, bool fd, float DH, float rdh)
@@ -795,12 +802,6 @@ __device__ __forceinline__ void vderiv2(const Inst &I, const float *hc, int i0, 
     }
 }
 
-// float2 store of a lane pair, or lane 0 alone for the last column of an odd nx
-__device__ __forceinline__ void st2(float *p, float2 v, bool two)
-{
-    if (two) *reinterpret_cast<float2 *>(p) = v;
-    else *p = v.x;
-}
 
 // Paired-column elastic stress update (k_update_s_el for two columns per thread).
 template <int R, bool X>
