@@ -389,6 +389,10 @@ __global__ void __launch_bounds__(128, 8) k_update_v2(const Inst *__restrict__ i
             pf_l1(I.rjp + o + D * P);
             pf_l1(I.vx + o + D * P);
             pf_l1(I.vy + o + D * P);
+            if (mode == 1) {   // the adjoint accumulates vxp1, vyp1 in place
+                pf_l1(I.vxp1 + o + D * P);
+                pf_l1(I.vyp1 + o + D * P);
+            }
         }
         // sxx x stencil of lane 0: columns i0-R+1 .. i0+R (A[k], k = 0..2R); pairs (A[k], A[k+1]);
         // column i0-R+1+k is odd when k - R is odd
@@ -1304,6 +1308,14 @@ static __global__ void k_snap_store(const Inst *__restrict__ insts, const int *_
     }
 }
 
+// resident CTAs of 256 threads asked of the correlation kernel: uncapped, its three
+// double divisions per cell take 98 registers and the kernel waits on its loads with
+// 20 warps per SM; at 40 registers (a 20-byte spill) the 4-shot 2000 x 600 FP16
+// adjoint runs in 82.9 instead of 107.8 ms (64 registers: 89.9 ms)
+#ifndef DN_CORR_MINB
+#define DN_CORR_MINB 6
+#endif
+
 __device__ __forceinline__ float snap_load(const Inst &I, long long slot, long long idx)
 {
     const long long tile_cells = (long long)blockDim.x * I.zch;
@@ -1318,7 +1330,7 @@ __device__ __forceinline__ float snap_load(const Inst &I, long long slot, long l
 // Adjoint cross-correlation, psv.c:313-387 (GRAD_FORM 1, INVMAT1 1), at the
 // adjoint steps whose mirrored forward step NT-nt+1 stored a snapshot.
 // ===========================================================================
-static __global__ void k_correlate(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+static __global__ void __launch_bounds__(256, DN_CORR_MINB) k_correlate(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
     const int nt = *ntb + off - I.t0;   // the instance's own time step
