@@ -68,6 +68,27 @@ def test_forward_bitexact(case):
         np.testing.assert_array_equal(s.field(fid), ref.field(fid), err_msg=name)
 
 
+# odd widths: the paired-column kernels own columns (i, i+1) with i odd, so the last
+# column of an odd NX is computed alone and column NX+1 (halo) must stay zero;
+# widths just above a tile (128 columns) leave most threads of the last tile idle
+ODD = [dict(L=0, fdorder=8, nx=63, ny=41), dict(L=0, fdorder=12, nx=131, ny=37, free_surf=0),
+       dict(L=3, fdorder=8, nx=129, ny=45), dict(L=0, fdorder=2, nx=33, ny=30, styp=2),
+       dict(L=2, fdorder=6, nx=65, ny=33, styp=3)]
+
+
+@pytest.mark.parametrize("case", ODD, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
+def test_forward_bitexact_odd_widths(case):
+    p, model, src, rec = small_case(**case)
+    ref = O.Restatement(p, model, src, rec, "f")
+    ref.forward(store=False)
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run([s], dn.MODE_FORWARD)
+    for comp in range(5):
+        np.testing.assert_array_equal(s.sections(comp), ref.sections(comp), err_msg=f"section {comp}")
+    for name, fid in (("vx", 0), ("vy", 1), ("sxx", 2), ("syy", 3), ("sxy", 4)):
+        np.testing.assert_array_equal(s.field(fid), ref.field(fid), err_msg=name)
+
+
 @pytest.mark.parametrize("case", [dict(L=0, fdorder=8), dict(L=3, fdorder=8), dict(L=0, fdorder=4, free_surf=0)],
                          ids=["elastic8", "visco8", "elastic4-nofs"])
 def test_plain_path_bitexact(case):
@@ -97,9 +118,9 @@ def _residuals(p, syn_vx, syn_vy):
     return out
 
 
-@pytest.mark.parametrize("L", [0, 3])
-def test_gradient_bitexact(L):
-    p, model, src, rec = small_case(L=L, store_snapshots=1)
+@pytest.mark.parametrize("L,nx", [(0, 64), (3, 64), (0, 63), (3, 129)])
+def test_gradient_bitexact(L, nx):
+    p, model, src, rec = small_case(L=L, store_snapshots=1, nx=nx)
     ref = O.Restatement(p, model, src, rec, "f")
     ref.forward(store=True)
     rvx, rvy = _residuals(p, ref.sections(0), ref.sections(1))
