@@ -145,10 +145,14 @@ class FWI:
     snapshots.  limits: (vp_lo, vp_hi, vs_lo, vs_hi, rho_lo, rho_hi).
     precond: a precond.PrecondConfig applied to every stacked gradient;
     shot_taper: (srtshape, srtradius, filtsize) of the per-shot circular taper;
-    time_filter: (order, fc, fc_start) band-limiting sources and data."""
+    time_filter: (order, fc, fc_start) band-limiting sources and data;
+    residual: calc_res options (Shot.residual_ex keywords) for gradient and
+    misfit; energy: (C_vp, C_vs, C_rho) of the EPRECOND 1/3 scaling (params.eprecond
+    set); inv_iter: (INV_VP_ITER, INV_VS_ITER, INV_RHO_ITER)."""
 
     def __init__(self, params, model, shots, obs, limits, device=0, nlbfgs=20, eps_scale=0.01, scalefac=2.0,
-                 stepmax=4, dist=None, precond=None, shot_taper=None, time_filter=None):
+                 stepmax=4, dist=None, precond=None, shot_taper=None, time_filter=None, residual=None, energy=None,
+                 inv_iter=(1, 1, 1)):
         self.p = params
         self.vp, self.vs, self.rho = [np.ascontiguousarray(a, np.float32) for a in model[:3]]
         if time_filter is not None:
@@ -161,6 +165,7 @@ class FWI:
                      for sh in shots]
             obs = [tuple(tdfilt(o, params.dt, order, fc, fc_start, device) for o in ob) for ob in obs]
         self.shots, self.obs, self.limits = shots, obs, limits
+        self.residual, self.energy, self.inv_iter = residual, energy, tuple(inv_iter)
         self.device, self.dist = device, dist
         self.eps_scale, self.scalefac, self.stepmax = eps_scale, scalefac, stepmax
         self.scale = np.array([self.vp.max(), self.vs.max(), self.rho.max()], np.float64)
@@ -185,7 +190,7 @@ class FWI:
 
         m = model or (self.vp, self.vs, self.rho)
         g_vp, g_vs, g_rho, L2 = sharded_gradient(self.p, m, self.shots, self.obs, self.dist, self.device,
-                                                 self.shot_taper)
+                                                 self.shot_taper, self.residual, self.energy)
         if self.precond is not None:
             from . import api as dn
 
@@ -204,8 +209,12 @@ class FWI:
         ss = [dn.Shot(m, *sh[:5]) for sh in self.shots]
         dn.run(ss, _lib.MODE_OBJECTIVE)
         L2 = 0.0
-        for s, (ovx, ovy) in zip(ss, self.obs):
-            L2 += s.residual(ovx, _lib.SEC_VX) + s.residual(ovy, _lib.SEC_VY)
+        for s, sh, (ovx, ovy) in zip(ss, self.shots, self.obs):
+            if self.residual is None:
+                L2 += s.residual(ovx, _lib.SEC_VX) + s.residual(ovy, _lib.SEC_VY)
+            else:
+                opts = dict({"src_x": float(sh[0][0]) * self.p.dh, "src_z": float(sh[1][0]) * self.p.dh}, **self.residual)
+                L2 += s.residual_ex(ovx, _lib.SEC_VX, **opts) + s.residual_ex(ovy, _lib.SEC_VY, **opts)
         for s in ss:
             s.close()
         m.close()
@@ -231,12 +240,13 @@ class FWI:
 
         def objective(eps):
             ntests[0] += 1
-            vp, vs, rho, _ = mat_update(self.vp, self.vs, self.rho, *d, eps, self.limits, it)
+            vp, vs, rho, _ = mat_update(self.vp, self.vs, self.rho, *d, eps, self.limits, it, self.inv_iter)
             return self.misfit((vp, vs, rho))
 
         eps, L2t, epst, found = step_length(objective, L2, self.eps_scale, self.scalefac, self.stepmax)
         if found:
-            self.vp, self.vs, self.rho, _ = mat_update(self.vp, self.vs, self.rho, *d, eps, self.limits, it)
+            self.vp, self.vs, self.rho, _ = mat_update(self.vp, self.vs, self.rho, *d, eps, self.limits, it,
+                                                       self.inv_iter)
         t3 = time.perf_counter()
         self.history.append({"iteration": it, "misfit": L2, "eps": eps, "L2t": L2t, "epst": epst, "found": found,
                              "gradient_s": t1 - t0, "lbfgs_s": t2 - t1, "step_search_s": t3 - t2,

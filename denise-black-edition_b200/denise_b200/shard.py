@@ -48,7 +48,8 @@ def allreduce_sum(arrays, dist=None, device=None):
     return out
 
 
-def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_taper=None):
+def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_taper=None, residual=None,
+                     energy=None):
     """FWI gradient of `shots` sharded over the ranks of `dist` (all ranks pass
     the same arguments).  Each rank runs its share as one batch on its GPU:
     forward with snapshots, device residuals against `obs`, adjoint, and stacks
@@ -56,7 +57,10 @@ def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_
     then summed over ranks.  Returns (g_vp, g_vs, g_rho, misfit), float64, on
     every rank.  shot_taper = (srtshape, srtradius, filtsize) applies the
     per-shot circular taper (taper_grad_shot.c) around each shot's first source
-    before stacking."""
+    before stacking; residual = the calc_res options of Shot.residual_ex (LNORM,
+    N_ORDER, OFFSET_MUTE, ...; None: the L2 residual); energy = (C_vp, C_vs,
+    C_rho) scales each shot's gradient by its energy weights (EPRECOND 1 or 3
+    in params)."""
     from . import api as dn
     from ._lib import MODE_ADJOINT, MODE_FORWARD, SEC_VX, SEC_VY
 
@@ -72,14 +76,20 @@ def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_
         ss = [dn.Shot(m, *shots[k][:5]) for k in mine]
         dn.run(ss, MODE_FORWARD)
         for s, k in zip(ss, mine):
-            misfit += s.residual(obs[k][0], SEC_VX) + s.residual(obs[k][1], SEC_VY)
+            if residual is None:
+                misfit += s.residual(obs[k][0], SEC_VX) + s.residual(obs[k][1], SEC_VY)
+            else:
+                src = {"src_x": float(shots[k][0][0]) * params.dh, "src_z": float(shots[k][1][0]) * params.dh}
+                opts = dict(src, **residual)
+                misfit += s.residual_ex(obs[k][0], SEC_VX, **opts) + s.residual_ex(obs[k][1], SEC_VY, **opts)
         dn.run(ss, MODE_ADJOINT)
         for s, k in zip(ss, mine):
-            if shot_taper is None:
+            if shot_taper is None and energy is None:
                 s.accumulate_gradient()
             else:
                 sx, sz = float(shots[k][0][0]) * params.dh, float(shots[k][1][0]) * params.dh
-                s.accumulate_gradient_ex(circular_taper=tuple(shot_taper) + (sx, sz))
+                s.accumulate_gradient_ex(energy=energy,
+                                         circular_taper=None if shot_taper is None else tuple(shot_taper) + (sx, sz))
         g = [x.astype(np.float64) for x in m.gradient()]
         for s in ss:
             s.close()

@@ -1,0 +1,153 @@
+"""Multi-stage FWI workflow: the stage loop of FWI_PSV.c:398-840 driven by a
+workflow file in the reference's format (read_par_inv.c).
+
+A workflow file holds one header line of 30 names and one line of 30 values
+per stage, read with fscanf, so line breaks inside a stage do not matter; the
+number of stages is the number of newlines minus one (FWI_PSV.c:157-163).
+Each stage configures the inversion: time-domain filter (TIME_FILT, ORDER,
+FC_START, FC_END), objective (LNORM, N_ORDER, OFFSET_MUTE, OFFSETC, TIMEWIN 5
+with GAMMA and TWLENGTH_MINUS), smoothing (SPATFILTER, WD_DAMP, WD_DAMP1),
+energy preconditioning (EPRECOND 1 or 3, with C_vp, C_vs, C_rho the averages
+of the starting model, FWI_PSV.c:538-580) and the iterations from which vp, vs
+and rho are inverted (INV_*_ITER), and it runs until the misfit of the last
+iteration differs from the one two iterations earlier by at most PRO
+(relative) after MIN_ITER iterations, or the step search fails, or ITERMAX
+iterations ran (FWI_PSV.c:784-830).  The L-BFGS history is cleared between
+stages.  Options the GPU path does not provide raise NotImplementedError:
+ROWI, INV_STF, NORMALIZE, ENV (LNORM 6), GAMMA_GRAV and TIMEWIN 1-4; Qs
+(INV_QS_ITER) is not inverted.
+"""
+import dataclasses
+
+import numpy as np
+
+STAGE_KEYS = ("PRO", "TIME_FILT", "FC_START", "FC_END", "ORDER", "TIMEWIN", "GAMMA", "TWLENGTH_MINUS",
+              "TWLENGTH_PLUS", "INV_VP_ITER", "INV_VS_ITER", "INV_RHO_ITER", "INV_QS_ITER", "SPATFILTER", "WD_DAMP",
+              "WD_DAMP1", "EPRECOND", "LNORM", "ROWI", "INV_STF", "OFFSETC_STF", "EPS_STF", "NORMALIZE",
+              "OFFSET_MUTE", "OFFSETC", "SCALERHO", "SCALEQS", "ENV", "GAMMA_GRAV", "N_ORDER")
+INT_KEYS = {"TIME_FILT", "ORDER", "TIMEWIN", "INV_VP_ITER", "INV_VS_ITER", "INV_RHO_ITER", "INV_QS_ITER",
+            "SPATFILTER", "EPRECOND", "LNORM", "ROWI", "INV_STF", "NORMALIZE", "OFFSET_MUTE", "ENV", "N_ORDER"}
+
+
+def _c_int(tok):
+    """fscanf %i: decimal, 0x hexadecimal or 0 octal, with an optional sign."""
+    t = tok.strip()
+    sign = -1 if t.startswith("-") else 1
+    t = t.lstrip("+-")
+    if t.lower().startswith("0x"):
+        return sign * int(t, 16)
+    if len(t) > 1 and t.startswith("0"):
+        return sign * int(t, 8)
+    return sign * int(t)
+
+
+def read_workflow(path):
+    """The stages of a workflow file as a list of dicts keyed by STAGE_KEYS.  As
+    read_par_inv's fscanf does, a stage whose values run out (more newlines than
+    stage lines, e.g. a stage broken over two lines) keeps the values of the stage
+    before it for the keys it could not read."""
+    text = open(path).read()
+    nstages = text.count("\n") - 1
+    tok = text.split()
+    n = len(STAGE_KEYS)
+    if nstages < 1 or len(tok) < 2 * n:
+        raise ValueError(f"{path}: {len(tok)} values, {nstages} stages of {n}")
+    stages, cur, pos = [], {key: 0 for key in STAGE_KEYS}, n
+    for _ in range(nstages):
+        cur = dict(cur)
+        for key in STAGE_KEYS:
+            if pos >= len(tok):
+                break
+            cur[key] = _c_int(tok[pos]) if key in INT_KEYS else float(tok[pos])
+            pos += 1
+        stages.append(cur)
+    return stages
+
+
+def model_averages(vp, vs, rho):
+    """C_vp, C_vs, C_rho of FWI_PSV.c:538-580: float sums in the reference's loop order
+    (x outer, depth inner = file order) divided by NX*NY."""
+    out = []
+    for a in (vp, vs, rho):
+        a = np.ascontiguousarray(a, np.float32)
+        total = np.cumsum(a.ravel(), dtype=np.float32)[-1]
+        out.append(float(np.float32(total / np.float32(a.size))))
+    return tuple(out)
+
+
+@dataclasses.dataclass
+class StageResult:
+    stage: int
+    iterations: int
+    misfits: list
+    reason: str
+
+
+def _check_supported(st, params):
+    for key in ("ROWI", "INV_STF", "NORMALIZE", "ENV"):
+        if st[key]:
+            raise NotImplementedError(f"{key} = {st[key]} is not provided by the GPU path")
+    if st["GAMMA_GRAV"]:
+        raise NotImplementedError("joint gravity inversion (GAMMA_GRAV) is not provided")
+    if st["TIMEWIN"] not in (0, 5):
+        raise NotImplementedError(f"TIMEWIN {st['TIMEWIN']} (picked-time windows) is not provided")
+    if st["LNORM"] == 6:
+        raise NotImplementedError("LNORM 6 (envelope misfit) needs a Hilbert transform")
+    if st["EPRECOND"] not in (0, 1, 3):
+        raise NotImplementedError(f"EPRECOND {st['EPRECOND']} is not provided")
+
+
+def stage_fwi(params, model, shots, obs, limits, st, averages, precond_base=None, shot_taper=None, device=0,
+              nlbfgs=20, eps_scale=0.01, scalefac=2.0, stepmax=4, dist=None):
+    """An fwi.FWI configured by one workflow stage."""
+    from . import fwi
+    from .precond import PrecondConfig
+
+    _check_supported(st, params)
+    p = params.replace(eprecond=st["EPRECOND"])
+    time_filter = None
+    if st["TIME_FILT"]:
+        time_filter = (st["ORDER"], st["FC_END"], st["FC_START"] if st["FC_START"] > 0 else 0.0)
+    residual = {"lnorm": st["LNORM"], "grad_form": p.grad_form, "n_order": st["N_ORDER"],
+                "offset_mute": st["OFFSET_MUTE"], "offsetc": st["OFFSETC"], "timewin": st["TIMEWIN"],
+                "gamma": st["GAMMA"], "twlength_minus": st["TWLENGTH_MINUS"]}
+    precond = None
+    if st["SPATFILTER"] or precond_base is not None:
+        base = precond_base if precond_base is not None else PrecondConfig()
+        precond = dataclasses.replace(base, spatfilter=st["SPATFILTER"], wd_damp=st["WD_DAMP"],
+                                      wd_damp1=st["WD_DAMP1"], fc_end=st["FC_END"],
+                                      c_vs=averages[1] if not base.c_vs else base.c_vs)
+    energy = averages if st["EPRECOND"] in (1, 3) else None
+    return fwi.FWI(p, model, shots, obs, limits, device=device, nlbfgs=nlbfgs, eps_scale=eps_scale,
+                   scalefac=scalefac, stepmax=stepmax, dist=dist, precond=precond, shot_taper=shot_taper,
+                   time_filter=time_filter, residual=residual, energy=energy,
+                   inv_iter=(st["INV_VP_ITER"], st["INV_VS_ITER"], st["INV_RHO_ITER"]))
+
+
+def run_workflow(params, model, shots, obs, limits, stages, itermax, min_iter=0, precond_base=None,
+                 shot_taper=None, device=0, dist=None, **fwi_kw):
+    """Runs the stages in order from the starting model; returns (vp, vs, rho, [StageResult])."""
+    vp, vs, rho = [np.ascontiguousarray(a, np.float32) for a in model[:3]]
+    averages = model_averages(vp, vs, rho)          # of the starting model (iter_true == 1)
+    results = []
+    for k, st in enumerate(stages, 1):
+        f = stage_fwi(params, (vp, vs, rho), shots, obs, limits, st, averages, precond_base, shot_taper, device,
+                      dist=dist, **fwi_kw)
+        misfits, reason, it = [], "ITERMAX", 0
+        try:
+            for it in range(1, itermax + 1):
+                misfits.append(f.iterate(it))
+                found = f.history[-1]["found"]
+                if it > min_iter and it >= 3 and abs(misfits[-3] - misfits[-1]) / misfits[-3] <= st["PRO"]:
+                    reason = "PRO"
+                    break
+                if not found:
+                    reason = "step search failed"
+                    break
+        finally:
+            f.lbfgs.close()
+            if f.precond is not None:
+                f.precond.close()
+        vp, vs, rho = f.vp, f.vs, f.rho
+        results.append(StageResult(k, it, misfits, reason))
+    return vp, vs, rho, results

@@ -744,3 +744,26 @@ int refh_apply_tdfilt(int ntr, int ns, float dt, int order, float fc2, float fc1
     free_matrix(s, 1, ntr, 1, ns);
     return 0;
 }
+
+/* read_par_inv (src/read_par_inv.c): stage nstage of a workflow file; out[30]
+ * = PRO, TIME_FILT, FC_START, FC_END, ORDER, TIMEWIN, GAMMA, TWLENGTH_MINUS,
+ * TWLENGTH_PLUS, INV_VP_ITER, INV_VS_ITER, INV_RHO_ITER, INV_QS_ITER,
+ * SPATFILTER, WD_DAMP, WD_DAMP1, EPRECOND, LNORM, ROWI, INV_STF, OFFSETC_STF,
+ * EPS_STF, NORMALIZE, OFFSET_MUTE, OFFSETC, SCALERHO, SCALEQS, ENV,
+ * GAMMA_GRAV, N_ORDER (as doubles). */
+extern int SPAT_FILT_SIZE, SPAT_FILT_1, SPAT_FILT_ITER, NORMALIZE, INV_QS_ITER, ENV, ORDER, ROWI;
+extern float PRO, EPS_STF, OFFSETC_STF, TWLENGTH_PLUS, SCALEQS, GAMMA_GRAV;
+int refh_read_par_inv(const char *path, int nstage, int stagemax, double *out)
+{
+    MYID = 1;   /* no banner */
+    FILE *fp = fopen(path, "r");
+    if (!fp) return -1;
+    read_par_inv(fp, nstage, stagemax);
+    const double v[30] = {PRO, TIME_FILT, FC_START, FC_END, ORDER, TIMEWIN, GAMMA, TWLENGTH_MINUS, TWLENGTH_PLUS,
+                          INV_VP_ITER, INV_VS_ITER, INV_RHO_ITER, INV_QS_ITER, SPATFILTER, WD_DAMP, WD_DAMP1,
+                          EPRECOND, LNORM, ROWI, INV_STF, OFFSETC_STF, EPS_STF, NORMALIZE, OFFSET_MUTE, OFFSETC,
+                          SCALERHO, SCALEQS, ENV, GAMMA_GRAV, N_ORDER};
+    for (int k = 0; k < 30; k++) out[k] = v[k];
+    MYID = 0;
+    return 0;
+}

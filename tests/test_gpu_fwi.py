@@ -149,3 +149,38 @@ def test_fwi_with_time_filter():
     L0 = f.iterate(1)
     assert np.isfinite(L0) and f.history[0]["found"]
     f.lbfgs.close()
+
+
+def test_workflow_two_stages(tmp_path):
+    """A two-stage workflow file: a 25 Hz low-pass L2 stage with smooth2, then a
+    full-band stage with the energy preconditioning and the global-correlation
+    misfit; each stage runs up to two iterations and lowers its misfit."""
+    import denise_b200 as dn
+    from denise_b200 import workflow
+
+    req = _request(0, "gradient", 90, 60, 500, 8, 0, 4, 11)
+    p = req.params
+    vp, vs, rho = req.model
+    vpt, vst, rhot = synth.add_ellipse(vp, vs, rho, p.dh, 3, v=3600.0)
+    m = dn.Model(p.replace(store_snapshots=0), vpt, vst, rhot)
+    ss = [dn.Shot(m, *sh[:5]) for sh in req.shots]
+    dn.run(ss)
+    obs = [(s.sections(dn.SEC_VX), s.sections(dn.SEC_VY)) for s in ss]
+    for s in ss:
+        s.close()
+    m.close()
+    start = tuple(synth.smoothed(a, 3.0) for a in (vp, vs, rho))
+    lim = (1000.0, 6000.0, 500.0, 3500.0, 1000.0, 3500.0)
+    wf = tmp_path / "workflow.inp"
+    wf.write_text(" ".join(workflow.STAGE_KEYS) + "\n"
+                  "0.001 1 0.0 25.0 4 0 0.0 0.0 0.0 1 1 1 0 2 1.0 1.0 0 2 0 0 0.0 0.0 0 0 0.0 1.0 1.0 0 0.0 0\n"
+                  "0.001 0 0.0 40.0 4 0 0.0 0.0 0.0 1 1 1 0 0 0.0 0.0 1 5 0 0 0.0 0.0 0 0 0.0 1.0 1.0 0 0.0 0\n")
+    stages = workflow.read_workflow(str(wf))
+    assert len(stages) == 2
+    vp1, vs1, rho1, res = workflow.run_workflow(p, start, req.shots, obs, lim, stages, itermax=2, nlbfgs=5)
+    assert [r.stage for r in res] == [1, 2]
+    for r in res:
+        assert r.iterations >= 1 and all(np.isfinite(r.misfits))
+        if len(r.misfits) == 2 and r.reason == "ITERMAX":
+            assert r.misfits[1] < r.misfits[0] or r.misfits[1] <= 0.0, r
+    assert not np.array_equal(vp1, start[0])
