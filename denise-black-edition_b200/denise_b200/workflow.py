@@ -15,7 +15,9 @@ iteration differs from the one two iterations earlier by at most PRO
 iterations ran (FWI_PSV.c:784-830).  The L-BFGS history is cleared between
 stages.  Options the GPU path does not provide raise NotImplementedError:
 ROWI, INV_STF, NORMALIZE, ENV (LNORM 6), GAMMA_GRAV and TIMEWIN 1-4; Qs
-(INV_QS_ITER) is not inverted.
+(INV_QS_ITER) is not inverted.  Each stage's model can be written as
+model_freq_out_PSV.c names it and the misfit log as FWI_PSV.c writes it, and
+a run can resume after the last stage whose model files exist.
 """
 import dataclasses
 
@@ -124,19 +126,57 @@ def stage_fwi(params, model, shots, obs, limits, st, averages, precond_base=None
                    inv_iter=(st["INV_VP_ITER"], st["INV_VS_ITER"], st["INV_RHO_ITER"]))
 
 
+def stage_files(prefix, stage):
+    """The model files model_freq_out_PSV.c writes at the end of a stage:
+    <INV_MODELFILE>_{vp,vs,rho}_stage_<n>.bin, x-major float32."""
+    return tuple(f"{prefix}_{name}_stage_{stage}.bin" for name in ("vp", "vs", "rho"))
+
+
+def _write_log(path, f, st, stage):
+    """The misfit log line of FWI_PSV.c (MISFIT_LOG_FILE): opteps, epst1[1..3], L2t[1..4], FC_START, FC, stage."""
+    h = f.history[-1]
+    eps = h["eps"] if h["found"] else 0.0
+    L2t = list(h["L2t"]) + [h["misfit"]]
+    epst = list(h["epst"])
+    with open(path, "a") as fp:
+        fp.write("%e \t %e \t %e \t %e \t %e \t %e \t %e \t %e \t %f \t %f \t %d \n"
+                 % (eps, epst[0], epst[1], epst[2], L2t[0], L2t[1], L2t[2], L2t[3], st["FC_START"], st["FC_END"],
+                    stage))
+
+
 def run_workflow(params, model, shots, obs, limits, stages, itermax, min_iter=0, precond_base=None,
-                 shot_taper=None, device=0, dist=None, **fwi_kw):
-    """Runs the stages in order from the starting model; returns (vp, vs, rho, [StageResult])."""
+                 shot_taper=None, device=0, dist=None, out_prefix=None, misfit_log=None, resume=False, **fwi_kw):
+    """Runs the stages in order from the starting model; returns (vp, vs, rho, [StageResult]).
+
+    out_prefix: write each stage's final model as stage_files(out_prefix, stage) (rank 0 of dist).
+    misfit_log: append one line per iteration in the reference's misfit-log format.
+    resume: start after the last stage whose three model files exist, from that model (the
+    reference's restart from its last written model)."""
     vp, vs, rho = [np.ascontiguousarray(a, np.float32) for a in model[:3]]
     averages = model_averages(vp, vs, rho)          # of the starting model (iter_true == 1)
-    results = []
-    for k, st in enumerate(stages, 1):
+    nx, ny = params.nx, params.ny
+    rank0 = dist is None or not dist.is_initialized() or dist.get_rank() == 0
+    results, first = [], 1
+    if resume and out_prefix is not None:
+        import os
+
+        for k in range(len(stages), 0, -1):
+            files = stage_files(out_prefix, k)
+            if all(os.path.exists(x) for x in files):
+                vp, vs, rho = [np.fromfile(x, np.float32, nx * ny).reshape(nx, ny) for x in files]
+                results = [StageResult(j, 0, [], "resumed") for j in range(1, k + 1)]
+                first = k + 1
+                break
+    for k in range(first, len(stages) + 1):
+        st = stages[k - 1]
         f = stage_fwi(params, (vp, vs, rho), shots, obs, limits, st, averages, precond_base, shot_taper, device,
                       dist=dist, **fwi_kw)
         misfits, reason, it = [], "ITERMAX", 0
         try:
             for it in range(1, itermax + 1):
                 misfits.append(f.iterate(it))
+                if misfit_log is not None and rank0:
+                    _write_log(misfit_log, f, st, k)
                 found = f.history[-1]["found"]
                 if it > min_iter and it >= 3 and abs(misfits[-3] - misfits[-1]) / misfits[-3] <= st["PRO"]:
                     reason = "PRO"
@@ -149,5 +189,8 @@ def run_workflow(params, model, shots, obs, limits, stages, itermax, min_iter=0,
             if f.precond is not None:
                 f.precond.close()
         vp, vs, rho = f.vp, f.vs, f.rho
+        if out_prefix is not None and rank0:
+            for a, x in zip((vp, vs, rho), stage_files(out_prefix, k)):
+                np.ascontiguousarray(a, np.float32).tofile(x)
         results.append(StageResult(k, it, misfits, reason))
     return vp, vs, rho, results

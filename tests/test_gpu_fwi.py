@@ -177,10 +177,24 @@ def test_workflow_two_stages(tmp_path):
                   "0.001 0 0.0 40.0 4 0 0.0 0.0 0.0 1 1 1 0 0 0.0 0.0 1 5 0 0 0.0 0.0 0 0 0.0 1.0 1.0 0 0.0 0\n")
     stages = workflow.read_workflow(str(wf))
     assert len(stages) == 2
-    vp1, vs1, rho1, res = workflow.run_workflow(p, start, req.shots, obs, lim, stages, itermax=2, nlbfgs=5)
+    prefix, log = str(tmp_path / "model"), str(tmp_path / "misfit.dat")
+    vp1, vs1, rho1, res = workflow.run_workflow(p, start, req.shots, obs, lim, stages, itermax=2, nlbfgs=5,
+                                                out_prefix=prefix, misfit_log=log)
     assert [r.stage for r in res] == [1, 2]
     for r in res:
         assert r.iterations >= 1 and all(np.isfinite(r.misfits))
         if len(r.misfits) == 2 and r.reason == "ITERMAX":
             assert r.misfits[1] < r.misfits[0] or r.misfits[1] <= 0.0, r
     assert not np.array_equal(vp1, start[0])
+    # model files per stage (x-major float32) and one log line per iteration with the stage number
+    stage2 = [np.fromfile(x, np.float32).reshape(p.nx, p.ny) for x in workflow.stage_files(prefix, 2)]
+    np.testing.assert_array_equal(stage2[0], vp1)
+    np.testing.assert_array_equal(stage2[2], rho1)
+    lines = open(log).read().splitlines()
+    assert len(lines) == sum(r.iterations for r in res)
+    assert [int(x.split()[-1]) for x in lines] == [r.stage for r in res for _ in range(r.iterations)]
+    # a second run resumes after stage 2 from its files: nothing left to do
+    vp2, vs2, rho2, res2 = workflow.run_workflow(p, start, req.shots, obs, lim, stages, itermax=2, nlbfgs=5,
+                                                 out_prefix=prefix, resume=True)
+    assert [r.reason for r in res2] == ["resumed", "resumed"]
+    np.testing.assert_array_equal(vp2, vp1)
