@@ -1163,6 +1163,7 @@ static int run_ckpt(dn_shot *s, int mode, double &ms_total, long long &nl)
 
 extern "C" int dn_run(dn_shot *const *shots, int n, int mode)
 {
+    DnRange range(mode == 0 ? "dn_run forward" : mode == 1 ? "dn_run adjoint" : "dn_run objective");
     if (shots && n > 0 && shots[0] && shots[0]->nseg > 0) {
         // checkpointed shots run one after the other
         double ms = 0.0;
@@ -1758,6 +1759,7 @@ __global__ void k_ass_grad(int nx, int ny, int pitch, const float *rho, const fl
 
 static int accumulate(dn_shot *s, const dn_accum_opts *o)
 {
+    DnRange range("gradient assembly");
     if (!s) return dn_fail(DN_EINVAL, "null shot");
     if (!s->correlated) return dn_fail(DN_ESTATE, "dn_shot_accumulate_gradient: no completed adjoint run");
     const bool precond = o && o->energy;
@@ -1996,6 +1998,7 @@ extern "C" int dn_residual_run_ex(const float *syn_tm, const float *obs, float *
 // becomes the shot's adjoint source of that component
 static int shot_source(dn_shot *s, int comp, const float *obs, double *l2, const dn_residual_opts *o)
 {
+    DnRange range("adjoint source");
     if (!s || !obs || !o) return dn_fail(DN_EINVAL, "dn_shot_residual: null argument");
     if (comp != DN_SEC_VX && comp != DN_SEC_VY && comp != DN_SEC_P)
         return dn_fail(DN_EINVAL, "dn_shot_residual: component must be vx, vy or p");

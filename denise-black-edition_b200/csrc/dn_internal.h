@@ -43,6 +43,18 @@ int dn_model_view_get(dn_model *m, dn_model_view *v);
     } while (0)
 #endif
 
+#ifdef __cplusplus
+#include <nvtx3/nvToolsExt.h>
+/* NVTX range for the duration of a scope (shows the library's phases in a
+ * timeline profiler; the header-only NVTX calls cost nothing without one). */
+struct DnRange {
+    explicit DnRange(const char *name) { nvtxRangePushA(name); }
+    ~DnRange() { nvtxRangePop(); }
+    DnRange(const DnRange &) = delete;
+    DnRange &operator=(const DnRange &) = delete;
+};
+#endif
+
 /* Grid padding of every device field: HX columns left/right, HZ rows above/below
  * the interior.  HZ >= FDORDER/2 covers the free-surface image rows and the
  * stencil reach; HX = 8 keeps column i = 1 16-byte aligned. */

@@ -488,6 +488,7 @@ static int apply_t(const dn_precond_plan *p, const dn_model_view &v)
 
 extern "C" int dn_precond_apply(const dn_precond_plan *p, dn_model *m)
 {
+    DnRange range("gradient conditioning");
     if (!p || !m) return dn_fail(DN_EINVAL, "dn_precond_apply: null argument");
     dn_model_view v;
     int st = dn_model_view_get(m, &v);
