@@ -330,6 +330,7 @@ __device__ __forceinline__ void pf_l1(const float *p) { asm volatile("prefetch.g
 #define DN_PF_ROWS 1
 #endif
 
+
 // float2 store of a lane pair, or lane 0 alone for the last column of an odd nx
 __device__ __forceinline__ void st2(float *p, float2 v, bool two)
 {
@@ -389,10 +390,6 @@ __global__ void __launch_bounds__(128, 8) k_update_v2(const Inst *__restrict__ i
             pf_l1(I.rjp + o + D * P);
             pf_l1(I.vx + o + D * P);
             pf_l1(I.vy + o + D * P);
-            if (mode == 1) {   // the adjoint accumulates vxp1, vyp1 in place
-                pf_l1(I.vxp1 + o + D * P);
-                pf_l1(I.vyp1 + o + D * P);
-            }
         }
         // sxx x stencil of lane 0: columns i0-R+1 .. i0+R (A[k], k = 0..2R); pairs (A[k], A[k+1]);
         // column i0-R+1+k is odd when k - R is odd
@@ -435,6 +432,7 @@ __global__ void __launch_bounds__(128, 8) k_update_v2(const Inst *__restrict__ i
             sxy_y = ADD2<X>(sxy_y, MUL2<X>(bc2(hc[m]), SUB2<X>(ld2(I.sxy + o + (m - 1) * P), ld2(I.sxy + o - m * P))));
             syy_y = ADD2<X>(syy_y, MUL2<X>(bc2(hc[m]), SUB2<X>(ld2(I.syy + o + m * P), ld2(I.syy + o - (m - 1) * P))));
         }
+
         if (xframe) {
             // per lane: left frame h = i, right frame h1 = i - nx + 2 fw (both when they overlap)
             float *sx = &sxx_x.x, *sy = &sxy_x.x;
