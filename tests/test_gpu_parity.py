@@ -290,3 +290,24 @@ def test_energy_preconditioned_gradient_matches_reference(ep):
             np.testing.assert_array_equal(a, b, err_msg=n)
         else:
             assert O.rel_l2(a, b) < 1e-6, (n, O.rel_l2(a, b))
+
+
+@pytest.mark.parametrize("kernels", ["one-column", "tma"])
+@pytest.mark.parametrize("case", [dict(L=0, fdorder=8, nx=63), dict(L=3, fdorder=8), dict(L=0, fdorder=12, free_surf=0)],
+                         ids=["elastic8-odd", "visco8", "elastic12-nofs"])
+def test_alternative_kernels_bitexact(monkeypatch, kernels, case):
+    """The kernels kept beside the default paired-column ones: the one-column
+    register-streaming kernels (DN_PACK=0) and the bulk-copy row pipeline
+    (DN_KERNEL=tma), both bit-identical to the reference."""
+    if kernels == "one-column":
+        monkeypatch.setenv("DN_PACK", "0")
+    else:
+        monkeypatch.setenv("DN_KERNEL", "tma")
+    p, model, src, rec = small_case(**case)
+    ref = O.Restatement(p, model, src, rec, "f")
+    ref.forward(store=False)
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run([s], dn.MODE_FORWARD)
+    for comp in range(2):
+        np.testing.assert_array_equal(s.sections(comp), ref.sections(comp), err_msg=f"section {comp}")
+    np.testing.assert_array_equal(s.field(2), ref.field(2))
