@@ -1,11 +1,15 @@
 // Device kernels of the P-SV propagator (sm_100a).
 //
 // Every kernel works on a batch of shot instances: blockIdx.y selects the
-// instance, blockIdx.x a tile of it.  A tile is blockDim.x columns wide and
-// `zch` rows tall; each thread owns one column and streams down the rows,
-// keeping the vertical stencil of the fields it differentiates in z in a
-// register window (one new load per row per field).  Horizontal neighbours
-// come from L1 (the warp reads 32 consecutive floats, shifted by m).
+// instance, blockIdx.x a tile of it.  A tile is `bx` columns wide and `zch`
+// rows tall.  In the one-column kernels each of bx threads owns one column and
+// streams down the rows, keeping the vertical stencil of the fields it
+// differentiates in z in a register window (one new load per row per field);
+// horizontal neighbours come from L1 (the warp reads 32 consecutive floats,
+// shifted by m).  The paired-column kernels (k_update_v2, k_update_s_el2, the
+// default for the velocity and elastic stress updates) give each of bx / 2
+// threads two adjacent columns computed with packed FP32x2 instructions, read
+// their z neighbours from L1 and prefetch the next row's first lines.
 //
 // Arithmetic: with EXACT = true every float operation is issued with an
 // explicit round-to-nearest intrinsic (__fmul_rn, __fadd_rn, ...), which the
