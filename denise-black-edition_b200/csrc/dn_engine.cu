@@ -134,6 +134,7 @@ struct dn_model {
     float *dsurf = nullptr;        // visco surface constants: 4 x nx
     float eta[DN_MAX_L], bip[DN_MAX_L], cip[DN_MAX_L], s_bjm[DN_MAX_L];
     void *dgrad = nullptr;         // stacked gradient: 3 x nx*ny (float or double), row-major [j][i]
+    double *drcp = nullptr;        // [ny][nx] {RN(1/muss^2), RN(1/(lamss+muss)^2)} for the correlation
     int grad64;
     int nshots = 0;
     float rdh = 0.0f;              // RN(1 / DH)
@@ -223,6 +224,7 @@ extern "C" int dn_model_footprint(const dn_params *p, size_t *bytes)
     int nf = p->L > 0 ? MF_COUNT : MF_CMUIPJP;
     size_t b = (size_t)nf * L.plane * 4 + 12 * 2 * (size_t)std::max(p->fw, 1) * 4 + 4 * (size_t)p->nx * 4;
     b += 3 * (size_t)p->nx * p->ny * (p->grad_accum == DN_ACC_F64 ? 8 : 4);
+    b += 16 * (size_t)p->nx * p->ny;   // correlation reciprocals
     if (bytes) *bytes = b;
     return DN_OK;
 }
@@ -321,6 +323,17 @@ extern "C" int dn_model_create(const dn_params *p, const float *vp, const float 
         gmuss[k] = muss;
         glamss[k] = (float)((double)(r * pi * pi) - 2.0 * (double)muss);
     }
+    // the correlation's reciprocals, row-major [j][i]: RN(1/muss^2) is psv.c's own 1.0/(muss*muss)
+    // and both serve the kernel's exact quotients; cells with muss <= 0 take no mu term
+    std::vector<double> rcp(2 * n, 0.0);
+    for (size_t k = 0; k < n; k++) {
+        const float muss = gmuss[k];
+        if (!(muss > 0.0f)) continue;
+        const float mm = muss * muss, lm = glamss[k] + muss, ll = lm * lm;
+        const size_t i = k / p->ny, j = k % p->ny, w = j * p->nx + i;
+        rcp[2 * w] = 1.0 / (double)mm;
+        rcp[2 * w + 1] = 1.0 / (double)ll;
+    }
     file_to_padded(L, rip.data(), host, MF_RIP * L.plane);
     file_to_padded(L, rjp.data(), host, MF_RJP * L.plane);
     file_to_padded(L, uipjp.data(), host, MF_UIPJP * L.plane);
@@ -410,7 +423,7 @@ extern "C" int dn_model_create(const dn_params *p, const float *vp, const float 
     }
     size_t gbytes = 3 * n * (m->grad64 ? 8 : 4);
     if (cudaMalloc(&m->dmat, host.size() * 4) != cudaSuccess || cudaMalloc(&m->dpml, pml.size() * 4) != cudaSuccess ||
-        cudaMalloc(&m->dgrad, gbytes) != cudaSuccess ||
+        cudaMalloc(&m->dgrad, gbytes) != cudaSuccess || cudaMalloc(&m->drcp, rcp.size() * 8) != cudaSuccess ||
         (!surf.empty() && cudaMalloc(&m->dsurf, surf.size() * 4) != cudaSuccess)) {
         cudaGetLastError();
         dn_model_destroy(m);
@@ -419,6 +432,7 @@ extern "C" int dn_model_create(const dn_params *p, const float *vp, const float 
     if (cudaMemcpy(m->dmat, host.data(), host.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(m->dpml, pml.data(), pml.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(m->dgrad, 0, gbytes) != cudaSuccess ||
+        cudaMemcpy(m->drcp, rcp.data(), rcp.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
         (!surf.empty() && cudaMemcpy(m->dsurf, surf.data(), surf.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)) {
         dn_model_destroy(m);
         return dn_fail(DN_EDEVICE, "dn_model_create: upload failed");
@@ -444,6 +458,7 @@ extern "C" int dn_model_destroy(dn_model *m)
     cudaFree(m->dpml);
     cudaFree(m->dsurf);
     cudaFree(m->dgrad);
+    cudaFree(m->drcp);
     delete m;
     return DN_OK;
 }
@@ -816,6 +831,7 @@ static Inst make_inst(const dn_shot *s, int mode)
     I.vs = m->field(MF_VS);
     I.gmuss = m->field(MF_GMUSS);
     I.glamss = m->field(MF_GLAMSS);
+    I.grcp = (const double2 *)m->drcp;
     if (p.L > 0) {
         I.c_muipjp = m->field(MF_CMUIPJP);
         I.c_tausipjp = m->field(MF_CTAUSIPJP);

@@ -53,6 +53,7 @@ struct Inst {
     const float *rho, *vp, *vs;                       // raw model (gradient terms)
     const float *c_muipjp, *c_tausipjp, *c_mu, *c_taus, *c_pi, *c_taup;   // visco
     const float *gmuss, *glamss;                      // muss, lamss of psv.c:333-334
+    const double2 *grcp;                              // [ny][nx] {RN(1/muss^2), RN(1/(lamss+muss)^2)}
     float eta[DN_MAX_L], bip[DN_MAX_L], cip[DN_MAX_L];
     // visco free-surface constants per column i (index i-1)
     const float *s_mu, *s_pi, *s_taus, *s_taup;
@@ -1310,29 +1311,137 @@ static __global__ void k_snap_store(const Inst *__restrict__ insts, const int *_
     }
 }
 
-// resident CTAs of 256 threads asked of the correlation kernel: uncapped, its three
-// double divisions per cell take 98 registers and the kernel waits on its loads with
-// 20 warps per SM; at 40 registers (a 20-byte spill) the 4-shot 2000 x 600 FP16
-// adjoint runs in 82.9 instead of 107.8 ms (64 registers: 89.9 ms)
+// resident CTAs of 256 threads asked of the correlation kernel (40 registers at 6)
 #ifndef DN_CORR_MINB
 #define DN_CORR_MINB 6
 #endif
 
-__device__ __forceinline__ float snap_load(const Inst &I, long long slot, long long idx)
+// ---------------------------------------------------------------------------
+// a / b from y = RN(1/b) without the general division routine.  q0 = RN(a y)
+// is within 1.5 ulp of a / b; one correction q1 = RN(q0 + RN(a - b q0) y)
+// leaves a relative error of about 2^-104 before its rounding, so q1 is within
+// one ulp, and then by Markstein's theorem (P. W. Markstein, IBM J. Res.
+// Develop. 34(1), 1990) the remainder r1 = a - b q1 is exact in an fma and
+// RN(q1 + r1 y) is the correctly rounded quotient.  This holds while every
+// intermediate stays in the normal range of double, which is the case for
+// operands converted from float: |a| and |b| lie in [2^-151, 2^128], the
+// quotient in [2^-279, 2^279] and the remainders are multiples of 2^-480.  A
+// zero dividend, b = 0 (y = inf) and b = inf (y = 0) and non-finite
+// dividends make the corrections NaN or lose the sign of zero; there q0 is
+// the IEEE quotient (a * inf or a * 0 with the sign of a), so it is returned.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double ddiv_rcp(double a, double b, double y)
 {
-    const long long tile_cells = (long long)blockDim.x * I.zch;
-    const long long e = slot * tile_cells + idx;
-    if (I.snap_prec == DN_SNAP_F32) return ((const float *)I.snap)[e];
-    const float s = I.snap_scale[slot];
-    if (I.snap_prec == DN_SNAP_F16) return __half2float(((const __half *)I.snap)[e]) * s;
-    return __bfloat162float(((const __nv_bfloat16 *)I.snap)[e]) * s;
+    const double q0 = __dmul_rn(a, y);
+    const double q1 = __fma_rn(__fma_rn(-b, q0, a), y, q0);
+    const double q2 = __fma_rn(__fma_rn(-b, q1, a), y, q1);
+    return (isfinite(q2) && a != 0.0) ? q2 : q0;
+}
+
+// the snapshot value at element e of a tile slot with scale s
+template <int PREC> __device__ __forceinline__ float snap_at(const void *base, long long e, float s);
+template <> __device__ __forceinline__ float snap_at<DN_SNAP_F32>(const void *base, long long e, float)
+{
+    return ((const float *)base)[e];
+}
+template <> __device__ __forceinline__ float snap_at<DN_SNAP_F16>(const void *base, long long e, float s)
+{
+    return __half2float(((const __half *)base)[e]) * s;
+}
+template <> __device__ __forceinline__ float snap_at<DN_SNAP_BF16>(const void *base, long long e, float s)
+{
+    return __bfloat162float(((const __nv_bfloat16 *)base)[e]) * s;
 }
 
 // ===========================================================================
 // Adjoint cross-correlation, psv.c:313-387 (GRAD_FORM 1, INVMAT1 1), at the
-// adjoint steps whose mirrored forward step NT-nt+1 stored a snapshot.
+// adjoint steps whose mirrored forward step NT-nt+1 stored a snapshot.  The
+// mu term's three double divisions take their reciprocals from the model's
+// grcp table, {RN(1/muss^2), RN(1/(lamss+muss)^2)} per cell: psv.c's first
+// term multiplies by 1/muss^2 itself and the other two quotients come out of
+// ddiv_rcp, so every term is bit-identical to the divisions it replaces.
 // ===========================================================================
-static __global__ void __launch_bounds__(256, DN_CORR_MINB) k_correlate(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+// accumulator update in the accumulator's precision: float sums as psv.c's
+// float grad arrays, double sums for DN_ACC_F64
+__device__ __forceinline__ float acc_add(float w, float t) { return __fadd_rn(w, t); }
+__device__ __forceinline__ double acc_add(double w, float t) { return DADD(w, (double)t); }
+__device__ __forceinline__ float acc_add_mu(float w, double t) { return F(DADD((double)w, t)); }
+__device__ __forceinline__ double acc_add_mu(double w, double t) { return DADD(w, t); }
+
+// One tile column of the correlation.  Each row first loads everything it
+// reads, the three accumulators included, and only then stores: the stores
+// may alias the loads as far as the compiler knows, so loads placed after a
+// store would wait for it and serialise three memory round trips per row.
+template <int PREC, typename A>
+__device__ __forceinline__ void correlate_tile(const Inst &I, int k, int b, int i, int j0, int nrow)
+{
+    const long long P = I.pitch;
+    const long long T = I.tiles;
+    const long long tc = (long long)blockDim.x * I.zch;   // cells per tile slot
+    const long long s0 = (long long)k * 5 * T + b;        // slot of the first of the five fields
+    const size_t esz = PREC == DN_SNAP_F32 ? 4 : 2;
+    const char *sp = (const char *)I.snap + (s0 * tc + threadIdx.x) * esz;
+    const long long sstep = T * tc * esz;                 // bytes from one field's slot to the next
+    float sc[5];
+#pragma unroll
+    for (int f = 0; f < 5; f++) sc[f] = PREC == DN_SNAP_F32 ? 1.0f : I.snap_scale[s0 + f * T];
+    const long long o0 = (long long)j0 * P + i;
+    const long long w0 = (long long)(j0 - 1) * I.nx + (i - 1);
+    A *wc = (A *)I.wc + w0, *wcu = (A *)I.wcu + w0, *wcr = (A *)I.wcrho + w0;
+    const bool wr = I.eprecond == 1;
+#pragma unroll 1
+    for (int r = 0; r < nrow; r++) {
+        const long long o = o0 + r * P, w = r * (long long)I.nx;
+        const char *se = sp + (long long)r * blockDim.x * esz;
+        const float frx = snap_at<PREC>(se, 0, sc[0]);
+        const float fry = snap_at<PREC>(se + sstep, 0, sc[1]);
+        const float fx = snap_at<PREC>(se + 2 * sstep, 0, sc[2]);
+        const float fy = snap_at<PREC>(se + 3 * sstep, 0, sc[3]);
+        const float fu = snap_at<PREC>(se + 4 * sstep, 0, sc[4]);
+        const float vxp1 = I.vxp1[o], vyp1 = I.vyp1[o];
+        const float sxx = I.sxx[o], syy = I.syy[o], sxy = I.sxy[o];
+        const float muss = I.gmuss[o], lamss = I.glamss[o];
+        const double2 y = I.grcp[w0 + w];
+        const A ar = wcr[w], al = wc[w], au = wcu[w];
+        float vx = 0.0f, vy = 0.0f, wrv = 0.0f;
+        if (wr) {
+            vx = I.vx[o];
+            vy = I.vy[o];
+            wrv = I.Wr[w0 + w];
+        }
+        const float trho = __fadd_rn(__fmul_rn(vxp1, frx), __fmul_rn(vyp1, fry));
+        const float tlam = __fmul_rn(__fadd_rn(fx, fy), __fadd_rn(sxx, syy));
+        const bool mpos = muss > 0.0f;
+        double tmu = 0.0;
+        if (mpos) {
+            const double mm = (double)__fmul_rn(muss, muss);
+            const float lm = __fadd_rn(lamss, muss);
+            const double t1 = DMUL(y.x, (double)__fmul_rn(fu, sxy));
+            const double t2 = ddiv_rcp(DMUL(0.25, (double)tlam), (double)__fmul_rn(lm, lm), y.y);
+            const double t3 = ddiv_rcp(DMUL(0.25, (double)__fmul_rn(__fsub_rn(fx, fy), __fsub_rn(sxx, syy))), mm, y.x);
+            tmu = DADD(DADD(t1, t2), t3);
+        }
+        wcr[w] = acc_add(ar, trho);
+        wc[w] = acc_add(al, tlam);
+        if (mpos) wcu[w] = acc_add_mu(au, tmu);
+        if (wr) I.Wr[w0 + w] = __fadd_rn(wrv, __fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)));
+    }
+}
+
+template <int PREC>
+__device__ __forceinline__ void correlate_prec(const Inst &I, int k, int b, int i, int j0, int nrow)
+{
+    if (I.acc64)
+        correlate_tile<PREC, double>(I, k, b, i, j0, nrow);
+    else
+        correlate_tile<PREC, float>(I, k, b, i, j0, nrow);
+}
+
+// insts is not __restrict__ here: with it the compiler keeps a dozen instance
+// pointers live across the row loop and spills at 40 registers; without it they
+// are re-read from the (L1-resident) descriptor, which measured ~1 ms faster on the
+// 4-shot 2000 x 600 FP16 adjoint
+static __global__ void __launch_bounds__(256, DN_CORR_MINB) k_correlate(const Inst *insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
     const int nt = *ntb + off - I.t0;   // the instance's own time step
@@ -1348,47 +1457,12 @@ static __global__ void __launch_bounds__(256, DN_CORR_MINB) k_correlate(const In
     if (i > I.nx) return;
     const int j0 = tz * I.zch + 1;
     const int nrow = min(I.zch, I.ny - j0 + 1);
-    const long long P = I.pitch;
-    for (int r = 0; r < nrow; r++) {
-        const int j = j0 + r;
-        const long long o = (long long)j * P + i;
-        const long long idx = (long long)r * blockDim.x + threadIdx.x;
-        const long long s0 = ((long long)k * 5) * I.tiles + b;
-        const float frx = snap_load(I, s0 + 0 * (long long)I.tiles, idx);
-        const float fry = snap_load(I, s0 + 1 * (long long)I.tiles, idx);
-        const float fx = snap_load(I, s0 + 2 * (long long)I.tiles, idx);
-        const float fy = snap_load(I, s0 + 3 * (long long)I.tiles, idx);
-        const float fu = snap_load(I, s0 + 4 * (long long)I.tiles, idx);
-        const float vxp1 = I.vxp1[o], vyp1 = I.vyp1[o];
-        const float sxx = I.sxx[o], syy = I.syy[o], sxy = I.sxy[o];
-        const float trho = __fadd_rn(__fmul_rn(vxp1, frx), __fmul_rn(vyp1, fry));
-        const float tlam = __fmul_rn(__fadd_rn(fx, fy), __fadd_rn(sxx, syy));
-        const float muss = I.gmuss[o], lamss = I.glamss[o];
-        double tmu = 0.0;
-        const bool mpos = muss > 0.0f;
-        if (mpos) {
-            const double mm = (double)__fmul_rn(muss, muss);
-            const float lm = __fadd_rn(lamss, muss);
-            const double t1 = DMUL(DDIV(1.0, mm), (double)__fmul_rn(fu, sxy));
-            const double t2 = DDIV(DMUL(0.25, (double)tlam), (double)__fmul_rn(lm, lm));
-            const double t3 = DDIV(DMUL(0.25, (double)__fmul_rn(__fsub_rn(fx, fy), __fsub_rn(sxx, syy))), mm);
-            tmu = DADD(DADD(t1, t2), t3);
-        }
-        const long long w = (long long)(j - 1) * I.nx + (i - 1);
-        if (I.acc64) {
-            double *wc = (double *)I.wc, *wcu = (double *)I.wcu, *wcr = (double *)I.wcrho;
-            wcr[w] = DADD(wcr[w], (double)trho);
-            wc[w] = DADD(wc[w], (double)tlam);
-            if (mpos) wcu[w] = DADD(wcu[w], tmu);
-        } else {
-            float *wc = (float *)I.wc, *wcu = (float *)I.wcu, *wcr = (float *)I.wcrho;
-            wcr[w] = __fadd_rn(wcr[w], trho);
-            wc[w] = __fadd_rn(wc[w], tlam);
-            if (mpos) wcu[w] = F(DADD((double)wcu[w], tmu));
-        }
-        if (I.eprecond == 1)
-            I.Wr[w] = __fadd_rn(I.Wr[w], __fadd_rn(__fmul_rn(I.vx[o], I.vx[o]), __fmul_rn(I.vy[o], I.vy[o])));
-    }
+    if (I.snap_prec == DN_SNAP_F16)
+        correlate_prec<DN_SNAP_F16>(I, k, b, i, j0, nrow);
+    else if (I.snap_prec == DN_SNAP_BF16)
+        correlate_prec<DN_SNAP_BF16>(I, k, b, i, j0, nrow);
+    else
+        correlate_prec<DN_SNAP_F32>(I, k, b, i, j0, nrow);
 }
 
 }   // namespace dn
