@@ -1259,6 +1259,60 @@ __device__ __forceinline__ float pow2_scale(float amax)
     return ldexpf(1.0f, max(e - 15, -126));
 }
 
+// the scaled store of one field's tile column, values already in hand
+template <int PREC>
+__device__ __forceinline__ void snap_put(const Inst &I, long long base, int r, float x, float inv)
+{
+    const long long e = base + (long long)r * blockDim.x + threadIdx.x;
+    if (PREC == DN_SNAP_F16)
+        ((__half *)I.snap)[e] = __float2half_rn(x * inv);
+    else
+        ((__nv_bfloat16 *)I.snap)[e] = __float2bfloat16_rn(x * inv);
+}
+
+// Tiles of at most ZR rows (the default 8): each thread loads its column of all
+// five fields once, the five block maxima share one reduction, and the scaled
+// values are stored from registers.  Same maxima (fmaxf ignores NaN in any
+// order) and the same conversions as the two-pass loop below.
+template <int PREC, int ZR>
+__device__ __forceinline__ void snap_store_regs(const Inst &I, int k, int b, int i, int j0, int nrow, bool in, float *red)
+{
+    const long long P = I.pitch;
+    const long long tile_cells = (long long)blockDim.x * I.zch;
+    const float *src[5] = {I.vxp1, I.vyp1, I.sxx, I.syy, I.sxy};
+    float v[5][ZR], am[5];
+#pragma unroll
+    for (int f = 0; f < 5; f++) {
+        am[f] = 0.0f;
+#pragma unroll
+        for (int r = 0; r < ZR; r++) {
+            v[f][r] = (in && r < nrow) ? src[f][(long long)(j0 + r) * P + i] : 0.0f;
+            am[f] = fmaxf(am[f], fabsf(v[f][r]));
+        }
+    }
+    const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int f = 0; f < 5; f++) {
+        const float m = warp_max(am[f]);
+        if ((threadIdx.x & 31) == 0) red[f * 8 + w] = m;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int f = 0; f < 5; f++) {
+        float m = 0.0f;
+        for (int q = 0; q < nw; q++) m = fmaxf(m, red[f * 8 + q]);
+        const long long slot = ((long long)k * 5 + f) * I.tiles + b;
+        const float sc = pow2_scale(m);
+        const float inv = 1.0f / sc;   // exact: power of two
+        if (threadIdx.x == 0) I.snap_scale[slot] = sc;
+        if (in) {
+#pragma unroll
+            for (int r = 0; r < ZR; r++)
+                if (r < nrow) snap_put<PREC>(I, slot * tile_cells, r, v[f][r], inv);
+        }
+    }
+}
+
 static __global__ void k_snap_store(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
@@ -1268,7 +1322,7 @@ static __global__ void k_snap_store(const Inst *__restrict__ insts, const int *_
     if (k < 0 || k >= I.nsnap) return;
     const int b = blockIdx.x;
     if (b >= I.tiles) return;
-    __shared__ float red[32];
+    __shared__ float red[5 * 8];   // five maxima of up to 8 warps
     const int tx = b % I.tiles_x, tz = b / I.tiles_x;
     const int i = tx * blockDim.x + threadIdx.x + 1;
     const int j0 = tz * I.zch + 1;
@@ -1284,6 +1338,13 @@ static __global__ void k_snap_store(const Inst *__restrict__ insts, const int *_
             I.Ws[w] = __fadd_rn(I.Ws[w], __fadd_rn(__fmul_rn(I.vx[o], I.vx[o]), __fmul_rn(I.vy[o], I.vy[o])));
         }
     }
+    if (I.snap_prec != DN_SNAP_F32 && I.zch <= 8) {
+        if (I.snap_prec == DN_SNAP_F16)
+            snap_store_regs<DN_SNAP_F16, 8>(I, k, b, i, j0, nrow, in, red);
+        else
+            snap_store_regs<DN_SNAP_BF16, 8>(I, k, b, i, j0, nrow, in, red);
+        return;
+    }
     for (int f = 0; f < 5; f++) {
         const long long slot = ((long long)k * 5 + f) * I.tiles + b;
         const long long base = slot * tile_cells;
@@ -1296,17 +1357,15 @@ static __global__ void k_snap_store(const Inst *__restrict__ insts, const int *_
         float amax = 0.0f;
         for (int r = 0; r < nrow && in; r++) amax = fmaxf(amax, fabsf(src[f][(long long)(j0 + r) * P + i]));
         amax = block_max(amax, red);
-        const float s = pow2_scale(amax);
-        const float inv = 1.0f / s;   // exact: power of two
-        if (threadIdx.x == 0) I.snap_scale[slot] = s;
-        if (I.snap_prec == DN_SNAP_F16) {
-            __half *dst = (__half *)I.snap + base;
-            for (int r = 0; r < nrow; r++)
-                if (in) dst[(long long)r * blockDim.x + threadIdx.x] = __float2half_rn(src[f][(long long)(j0 + r) * P + i] * inv);
-        } else {
-            __nv_bfloat16 *dst = (__nv_bfloat16 *)I.snap + base;
-            for (int r = 0; r < nrow; r++)
-                if (in) dst[(long long)r * blockDim.x + threadIdx.x] = __float2bfloat16_rn(src[f][(long long)(j0 + r) * P + i] * inv);
+        const float sc = pow2_scale(amax);
+        const float inv = 1.0f / sc;   // exact: power of two
+        if (threadIdx.x == 0) I.snap_scale[slot] = sc;
+        for (int r = 0; r < nrow && in; r++) {
+            const float x = src[f][(long long)(j0 + r) * P + i];
+            if (I.snap_prec == DN_SNAP_F16)
+                snap_put<DN_SNAP_F16>(I, base, r, x, inv);
+            else
+                snap_put<DN_SNAP_BF16>(I, base, r, x, inv);
         }
     }
 }

@@ -237,6 +237,58 @@ def test_half_snapshots_of_tiny_wavefields_stay_finite(prec):
         assert np.all(np.isfinite(g))
 
 
+def _encode_tiles(x, bx, zch, prec):
+    """The half-precision snapshot rule on a [nx][ny] field: tiles of bx columns
+    x zch rows, per tile s = 2^max(e - 15, -126) with max|x| = f 2^e, f in
+    [0.5, 1) (s = 1 for an all-zero tile), stored as RN(x / s) in FP16 or BF16
+    and decoded as float(h) * s."""
+    out = np.empty_like(x)
+    for i0 in range(0, x.shape[0], bx):
+        for j0 in range(0, x.shape[1], zch):
+            t = x[i0:i0 + bx, j0:j0 + zch]
+            am = np.float32(np.max(np.abs(t)))
+            sc = np.float32(1.0)
+            if am > 0 and np.isfinite(am):
+                e = int(np.frexp(am)[1])
+                sc = np.ldexp(np.float32(1.0), max(e - 15, -126)).astype(np.float32)
+            y = (t * (np.float32(1.0) / sc)).astype(np.float32)
+            if prec == dn.SNAP_F16:
+                h = y.astype(np.float16).astype(np.float32)
+            else:   # bfloat16: round to nearest even on the upper 16 bits
+                u = y.view(np.uint32).astype(np.uint64)
+                h = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32).view(np.float32)
+            out[i0:i0 + bx, j0:j0 + zch] = h * sc
+    return out
+
+
+@pytest.mark.parametrize("prec", [dn.SNAP_F16, dn.SNAP_BF16], ids=["fp16", "bf16"])
+@pytest.mark.parametrize("zch", [8, 16, 5], ids=["rows8", "rows16", "rows5"])
+def test_half_snapshot_encoding(prec, zch):
+    """Decoded FP16/BF16 snapshots equal the per-tile power-of-two encoding of
+    the FP32 snapshots bit for bit, on a grid with partial tiles in x and z and
+    for tile heights served by the single-pass store (up to 8 rows) and by the
+    general one."""
+    from denise_b200 import tune
+
+    kw = dict(nx=150, ny=45, nt=120, store_snapshots=1)
+    p32, model, src, rec = small_case(**kw, snap_precision=dn.SNAP_F32)
+    ph, _, _, _ = small_case(**kw, snap_precision=prec)
+    tune.set_rule(ph.fdorder, ph.L, 0, 1 << 40, 128, zch)
+    try:
+        bx, z = tune.tile_for(ph)
+        assert (bx, z) == (128, zch)
+        m32, s32 = gpu_shot(p32, model, src, rec)
+        mh, sh = gpu_shot(ph, model, src, rec)
+        dn.run([s32, sh], dn.MODE_FORWARD)
+    finally:
+        tune.clear_rules()
+    nsnap = -(-p32.nt // p32.dtinv)
+    for k in (0, nsnap // 2, nsnap - 1):
+        for f in range(5):
+            ref = _encode_tiles(s32.snapshot(k, f), bx, zch, prec)
+            np.testing.assert_array_equal(sh.snapshot(k, f), ref, err_msg=f"snapshot {k} field {f}")
+
+
 @pytest.mark.parametrize("L,prec,ckpt", [(0, dn.SNAP_F32, 39), (2, dn.SNAP_F32, 27), (0, dn.SNAP_F16, 63)],
                          ids=["elastic-fp32", "visco-fp32-odd-segments", "elastic-fp16"])
 def test_checkpointed_adjoint_equals_stored_snapshots(L, prec, ckpt):
