@@ -409,7 +409,7 @@ def run_gradient(a, device):
     fp = ctypes.c_size_t()
     pc = p.to_c()
     dn._lib.check(dn._lib.lib.dn_shot_footprint(ctypes.byref(pc), len(ri), 1, ctypes.byref(fp)))
-    free, total = torch.cuda.mem_get_info(device)
+    free, total = dn.device_memory(device)
     batch = max(1, min(n, int(0.8 * free / fp.value) - 1))
 
     def grad(params, idx):

@@ -24,7 +24,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_CFLAGS = ["-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-Wno-unused-function"]
 
-CU_SOURCES = ["dn_engine.cu", "dn_residual.cu", "dn_fwi.cu", "dn_precond.cu", "dn_tdfilt.cu"] + [f"dn_launch_r{r}.cu" for r in range(1, 7)]
+CU_SOURCES = ["dn_engine.cu", "dn_alloc.cu", "dn_residual.cu", "dn_fwi.cu", "dn_precond.cu", "dn_tdfilt.cu"] + [f"dn_launch_r{r}.cu" for r in range(1, 7)]
 C_SOURCES = ["dn_setup.c", "dn_opt.c", "dn_precond_host.c"]
 HOST_SOURCES = ["dn_io.c", "dn_driver.c"]
 CLI_SOURCES = ["denise_b200_main.c"]

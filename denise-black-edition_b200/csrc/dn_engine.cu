@@ -61,6 +61,7 @@ extern "C" int dn_device_memory(int device, size_t *free_bytes, size_t *total_by
     size_t f = 0, t = 0;
     e = cudaMemGetInfo(&f, &t);
     if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "cudaMemGetInfo: %s", cudaGetErrorString(e));
+    f += dn_pool_idle_bytes(device);   // cached by the library, free for its next allocation
     if (free_bytes) *free_bytes = f;
     if (total_bytes) *total_bytes = t;
     return DN_OK;
@@ -88,7 +89,7 @@ static int dev_state(int device, DevState **out)
         DevState st;
         CU(cudaSetDevice(device));
         CU(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
-        CU(cudaMalloc(&st.d_zero, 2 * sizeof(int)));
+        CU(dn_malloc(&st.d_zero, 2 * sizeof(int)));
         CU(cudaMemset(st.d_zero, 0, 2 * sizeof(int)));
         st.d_step = st.d_zero + 1;
         CU(cudaEventCreate(&st.ev0));
@@ -134,7 +135,6 @@ struct dn_model {
     float *dsurf = nullptr;        // visco surface constants: 4 x nx
     float eta[DN_MAX_L], bip[DN_MAX_L], cip[DN_MAX_L], s_bjm[DN_MAX_L];
     void *dgrad = nullptr;         // stacked gradient: 3 x nx*ny (float or double), row-major [j][i]
-    double *drcp = nullptr;        // [ny][nx] {RN(1/muss^2), RN(1/(lamss+muss)^2)} for the correlation
     int grad64;
     int nshots = 0;
     float rdh = 0.0f;              // RN(1 / DH)
@@ -224,7 +224,6 @@ extern "C" int dn_model_footprint(const dn_params *p, size_t *bytes)
     int nf = p->L > 0 ? MF_COUNT : MF_CMUIPJP;
     size_t b = (size_t)nf * L.plane * 4 + 12 * 2 * (size_t)std::max(p->fw, 1) * 4 + 4 * (size_t)p->nx * 4;
     b += 3 * (size_t)p->nx * p->ny * (p->grad_accum == DN_ACC_F64 ? 8 : 4);
-    b += 16 * (size_t)p->nx * p->ny;   // correlation reciprocals
     if (bytes) *bytes = b;
     return DN_OK;
 }
@@ -265,7 +264,7 @@ static int fastdiv_setup(int device, float dh, int *ok, float *y)
     const char *ev = getenv("DN_FASTDIV");
     const bool enabled = !(ev && ev[0] == '0');
     char *buf = nullptr;
-    if (cudaMalloc(&buf, 16) != cudaSuccess) return dn_fail(DN_ENOMEM, "fast division check: allocation failed");
+    if (dn_malloc(&buf, 16) != cudaSuccess) return dn_fail(DN_ENOMEM, "fast division check: allocation failed");
     unsigned long long hbad = 0;
     float hy = 0.0f;
     cudaError_t e = cudaMemset(buf, 0, 16);
@@ -277,7 +276,7 @@ static int fastdiv_setup(int device, float dh, int *ok, float *y)
     }
     if (e == cudaSuccess) e = cudaMemcpy(&hbad, buf, 8, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(&hy, buf + 8, 4, cudaMemcpyDeviceToHost);
-    cudaFree(buf);
+    dn_free(buf);
     if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "fast division check: %s", cudaGetErrorString(e));
     *ok = enabled && hbad == 0;
     *y = hy;
@@ -322,17 +321,6 @@ extern "C" int dn_model_create(const dn_params *p, const float *vp, const float 
         float muss = r * u * u;
         gmuss[k] = muss;
         glamss[k] = (float)((double)(r * pi * pi) - 2.0 * (double)muss);
-    }
-    // the correlation's reciprocals, row-major [j][i]: RN(1/muss^2) is psv.c's own 1.0/(muss*muss)
-    // and both serve the kernel's exact quotients; cells with muss <= 0 take no mu term
-    std::vector<double> rcp(2 * n, 0.0);
-    for (size_t k = 0; k < n; k++) {
-        const float muss = gmuss[k];
-        if (!(muss > 0.0f)) continue;
-        const float mm = muss * muss, lm = glamss[k] + muss, ll = lm * lm;
-        const size_t i = k / p->ny, j = k % p->ny, w = j * p->nx + i;
-        rcp[2 * w] = 1.0 / (double)mm;
-        rcp[2 * w + 1] = 1.0 / (double)ll;
     }
     file_to_padded(L, rip.data(), host, MF_RIP * L.plane);
     file_to_padded(L, rjp.data(), host, MF_RJP * L.plane);
@@ -422,9 +410,9 @@ extern "C" int dn_model_create(const dn_params *p, const float *vp, const float 
         return dn_fail(DN_EDEVICE, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
     }
     size_t gbytes = 3 * n * (m->grad64 ? 8 : 4);
-    if (cudaMalloc(&m->dmat, host.size() * 4) != cudaSuccess || cudaMalloc(&m->dpml, pml.size() * 4) != cudaSuccess ||
-        cudaMalloc(&m->dgrad, gbytes) != cudaSuccess || cudaMalloc(&m->drcp, rcp.size() * 8) != cudaSuccess ||
-        (!surf.empty() && cudaMalloc(&m->dsurf, surf.size() * 4) != cudaSuccess)) {
+    if (dn_malloc(&m->dmat, host.size() * 4) != cudaSuccess || dn_malloc(&m->dpml, pml.size() * 4) != cudaSuccess ||
+        dn_malloc(&m->dgrad, gbytes) != cudaSuccess ||
+        (!surf.empty() && dn_malloc(&m->dsurf, surf.size() * 4) != cudaSuccess)) {
         cudaGetLastError();
         dn_model_destroy(m);
         return dn_fail(DN_ENOMEM, "dn_model_create: device allocation failed");
@@ -432,7 +420,6 @@ extern "C" int dn_model_create(const dn_params *p, const float *vp, const float 
     if (cudaMemcpy(m->dmat, host.data(), host.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(m->dpml, pml.data(), pml.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(m->dgrad, 0, gbytes) != cudaSuccess ||
-        cudaMemcpy(m->drcp, rcp.data(), rcp.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
         (!surf.empty() && cudaMemcpy(m->dsurf, surf.data(), surf.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)) {
         dn_model_destroy(m);
         return dn_fail(DN_EDEVICE, "dn_model_create: upload failed");
@@ -454,11 +441,10 @@ extern "C" int dn_model_destroy(dn_model *m)
 {
     if (!m) return DN_OK;
     cudaSetDevice(m->device);
-    cudaFree(m->dmat);
-    cudaFree(m->dpml);
-    cudaFree(m->dsurf);
-    cudaFree(m->dgrad);
-    cudaFree(m->drcp);
+    dn_free(m->dmat);
+    dn_free(m->dpml);
+    dn_free(m->dsurf);
+    dn_free(m->dgrad);
     delete m;
     return DN_OK;
 }
@@ -673,17 +659,17 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
         delete s;
         return dn_fail(DN_EDEVICE, "cudaSetDevice: %s", cudaGetErrorString(e));
     }
-    bool ok = cudaMalloc(&s->dstate, s->state_bytes) == cudaSuccess && cudaMalloc(&s->dacq, acq_bytes) == cudaSuccess &&
-              cudaMalloc(&s->d_sec, sec_n * 4) == cudaSuccess && cudaMalloc(&s->d_res, res_n * 4) == cudaSuccess &&
-              cudaMalloc(&s->d_acc, acc_bytes) == cudaSuccess;
+    bool ok = dn_malloc(&s->dstate, s->state_bytes) == cudaSuccess && dn_malloc(&s->dacq, acq_bytes) == cudaSuccess &&
+              dn_malloc(&s->d_sec, sec_n * 4) == cudaSuccess && dn_malloc(&s->d_res, res_n * 4) == cudaSuccess &&
+              dn_malloc(&s->d_acc, acc_bytes) == cudaSuccess;
     if (ok && s->nsnap > 0) {
-        ok = cudaMalloc(&s->d_snap, std::max(snap_n, (size_t)1) * snap_elem_bytes(p->snap_precision)) == cudaSuccess &&
-             cudaMalloc(&s->d_snap_scale, std::max((size_t)s->nsnap * 5 * s->tiles, (size_t)1) * 4) == cudaSuccess;
+        ok = dn_malloc(&s->d_snap, std::max(snap_n, (size_t)1) * snap_elem_bytes(p->snap_precision)) == cudaSuccess &&
+             dn_malloc(&s->d_snap_scale, std::max((size_t)s->nsnap * 5 * s->tiles, (size_t)1) * 4) == cudaSuccess;
     }
     if (ok && p->store_snapshots && p->ckpt_steps > 0) {
         s->nseg = (p->nt + p->ckpt_steps - 1) / p->ckpt_steps;
-        ok = cudaMalloc(&s->dckpt, s->state_bytes * s->nseg) == cudaSuccess &&
-             cudaMalloc(&s->dstate2, s->state_bytes) == cudaSuccess;
+        ok = dn_malloc(&s->dckpt, s->state_bytes * s->nseg) == cudaSuccess &&
+             dn_malloc(&s->dstate2, s->state_bytes) == cudaSuccess;
     }
     if (!ok) {
         cudaGetLastError();
@@ -752,15 +738,15 @@ extern "C" int dn_shot_destroy(dn_shot *s)
     if (!s) return DN_OK;
     forget_shot(s);
     cudaSetDevice(s->m->device);
-    cudaFree(s->dstate);
-    cudaFree(s->dacq);
-    cudaFree(s->d_sec);
-    cudaFree(s->d_res);
-    cudaFree(s->d_snap);
-    cudaFree(s->d_snap_scale);
-    cudaFree(s->d_acc);
-    cudaFree(s->dckpt);
-    cudaFree(s->dstate2);
+    dn_free(s->dstate);
+    dn_free(s->dacq);
+    dn_free(s->d_sec);
+    dn_free(s->d_res);
+    dn_free(s->d_snap);
+    dn_free(s->d_snap_scale);
+    dn_free(s->d_acc);
+    dn_free(s->dckpt);
+    dn_free(s->dstate2);
     s->m->nshots--;
     delete s;
     return DN_OK;
@@ -831,7 +817,6 @@ static Inst make_inst(const dn_shot *s, int mode)
     I.vs = m->field(MF_VS);
     I.gmuss = m->field(MF_GMUSS);
     I.glamss = m->field(MF_GLAMSS);
-    I.grcp = (const double2 *)m->drcp;
     if (p.L > 0) {
         I.c_muipjp = m->field(MF_CMUIPJP);
         I.c_tausipjp = m->field(MF_CTAUSIPJP);
@@ -973,7 +958,7 @@ static void batch_free(Batch *b)
 {
     cudaSetDevice(b->device);
     if (b->exec) cudaGraphExecDestroy(b->exec);
-    cudaFree(b->d_insts);
+    dn_free(b->d_insts);
     delete b;
 }
 
@@ -1135,11 +1120,11 @@ static int run_ckpt(dn_shot *s, int mode, double &ms_total, long long &nl)
         }
     }
     Inst *d = nullptr;
-    CU(cudaMalloc(&d, sizeof(Inst) * h.size()));
+    CU(dn_malloc(&d, sizeof(Inst) * h.size()));
     cudaError_t e = cudaMemcpyAsync(d, h.data(), sizeof(Inst) * h.size(), cudaMemcpyHostToDevice, sm);
     if (e == cudaSuccess) e = cudaStreamSynchronize(sm);
     if (e != cudaSuccess) {
-        cudaFree(d);
+        dn_free(d);
         return dn_fail(DN_EDEVICE, "checkpointed run: %s", cudaGetErrorString(e));
     }
     if (mode != 1) {
@@ -1149,7 +1134,7 @@ static int run_ckpt(dn_shot *s, int mode, double &ms_total, long long &nl)
         st = dn_fail(DN_EDEVICE, "checkpointed adjoint: state reset failed");
     }
     if (st) {
-        cudaFree(d);
+        dn_free(d);
         return st;
     }
     cudaEventRecord(ds->ev0, sm);
@@ -1172,7 +1157,7 @@ static int run_ckpt(dn_shot *s, int mode, double &ms_total, long long &nl)
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, ds->ev0, ds->ev1);
     ms_total += ms;
-    cudaFree(d);
+    dn_free(d);
     if (le != cudaSuccess) return dn_fail(DN_EDEVICE, "kernel launch failed: %s", cudaGetErrorString(le));
     return st;
 }
@@ -1227,7 +1212,7 @@ extern "C" int dn_run(dn_shot *const *shots, int n, int mode)
         b->mode = mode;
         b->shots.assign(shots, shots + n);
         for (int k = 0; k < n; k++) b->h_insts.push_back(make_inst(shots[k], mode));
-        if (cudaMalloc(&b->d_insts, sizeof(Inst) * n) != cudaSuccess) {
+        if (dn_malloc(&b->d_insts, sizeof(Inst) * n) != cudaSuccess) {
             delete b;
             return dn_fail(DN_ENOMEM, "dn_run: descriptor allocation failed");
         }
@@ -1291,13 +1276,13 @@ static int run_direct(dn_shot *s, int mode, int nt0, int nt1, bool zero)
     if (st) return st;
     Inst h = make_inst(s, mode);
     Inst *d = nullptr;
-    CU(cudaMalloc(&d, sizeof(Inst)));
+    CU(dn_malloc(&d, sizeof(Inst)));
     CU(cudaMemcpyAsync(d, &h, sizeof(Inst), cudaMemcpyHostToDevice, ds->stream));
     CU(cudaStreamSynchronize(ds->stream));
     if (zero) {
         st = zero_for_run(s, mode, ds->stream);
         if (st) {
-            cudaFree(d);
+            dn_free(d);
             return st;
         }
     }
@@ -1315,7 +1300,7 @@ static int run_direct(dn_shot *s, int mode, int nt0, int nt1, bool zero)
     cudaEventElapsedTime(&ms, ds->ev0, ds->ev1);
     g_last_ms = ms;
     g_last_launches = nl;
-    cudaFree(d);
+    dn_free(d);
     if (le != cudaSuccess) return dn_fail(DN_EDEVICE, "kernel launch failed: %s", cudaGetErrorString(le));
     return st;
 }
@@ -1384,7 +1369,7 @@ extern "C" int dn_queue_create(int device, int chunk, dn_queue **out)
     q->device = device;
     q->chunk = chunk;
     if (cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&q->d_step, sizeof(int)) != cudaSuccess ||
+        dn_malloc(&q->d_step, sizeof(int)) != cudaSuccess ||
         cudaEventCreateWithFlags(&q->ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaMemset(q->d_step, 0, sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
@@ -1401,8 +1386,8 @@ extern "C" int dn_queue_destroy(dn_queue *q)
     cudaSetDevice(q->device);
     if (q->stream) cudaStreamSynchronize(q->stream);
     if (q->exec) cudaGraphExecDestroy(q->exec);
-    cudaFree(q->d_insts);
-    cudaFree(q->d_step);
+    dn_free(q->d_insts);
+    dn_free(q->d_step);
     if (q->ev) cudaEventDestroy(q->ev);
     if (q->stream) cudaStreamDestroy(q->stream);
     delete q;
@@ -1456,10 +1441,10 @@ static int queue_capture(dn_queue *q)
     st = prepare_launch(c);
     if (st) return st;
     if (n > q->cap_insts) {
-        cudaFree(q->d_insts);
+        dn_free(q->d_insts);
         q->d_insts = nullptr;
         q->cap_insts = 0;
-        if (cudaMalloc(&q->d_insts, sizeof(Inst) * n) != cudaSuccess)
+        if (dn_malloc(&q->d_insts, sizeof(Inst) * n) != cudaSuccess)
             return dn_fail(DN_ENOMEM, "dn_queue_step: descriptor allocation failed");
         q->cap_insts = n;
     }
@@ -1833,7 +1818,7 @@ static int accumulate(dn_shot *s, const dn_accum_opts *o)
         free(cells);
     }
     const size_t total = tap_off + hbuf.size();
-    if (total) CU(cudaMalloc(&buf, total));
+    if (total) CU(dn_malloc(&buf, total));
     if (precond) {
         We = (float *)buf;
         maxbits = (unsigned *)(buf + carve_size(n, 4));
@@ -1853,7 +1838,7 @@ static int accumulate(dn_shot *s, const dn_accum_opts *o)
                                                We, maxbits, cvp, cvs, crho, tp);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(ds->stream);
-    cudaFree(buf);
+    dn_free(buf);
     if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "gradient assembly: %s", cudaGetErrorString(e));
     return DN_OK;
 }
@@ -1967,12 +1952,12 @@ extern "C" int dn_profile_steps(dn_shot *const *shots, int n, int mode, int nste
     }
     nsteps = std::min(nsteps, maxnt);
     Inst *d = nullptr;
-    CU(cudaMalloc(&d, sizeof(Inst) * n));
+    CU(dn_malloc(&d, sizeof(Inst) * n));
     CU(cudaMemcpyAsync(d, h.data(), sizeof(Inst) * n, cudaMemcpyHostToDevice, ds->stream));
     for (int k = 0; k < n; k++) {
         st = zero_for_run(shots[k], mode, ds->stream);
         if (st) {
-            cudaFree(d);
+            dn_free(d);
             return st;
         }
     }
@@ -1993,7 +1978,7 @@ extern "C" int dn_profile_steps(dn_shot *const *shots, int n, int mode, int nste
     for (int k = 0; k < 9; k++) cudaEventDestroy(ev[k]);
     cudaError_t e = cudaGetLastError();
     cudaStreamSynchronize(ds->stream);
-    cudaFree(d);
+    dn_free(d);
     for (int k = 0; k < n; k++) {
         if (mode == 0) shots[k]->stored = 0;
         if (mode == 1) shots[k]->correlated = 0;
@@ -2026,7 +2011,7 @@ static int shot_source(dn_shot *s, int comp, const float *obs, double *l2, const
     const int nt = s->p.nt, ntr = s->ntr;
     const size_t n = (size_t)ntr * nt;
     float *dobs = nullptr;
-    if (cudaMalloc(&dobs, n * 4) != cudaSuccess) {
+    if (dn_malloc(&dobs, n * 4) != cudaSuccess) {
         cudaGetLastError();
         return dn_fail(DN_ENOMEM, "dn_shot_residual: device allocation failed");
     }
@@ -2039,7 +2024,7 @@ static int shot_source(dn_shot *s, int comp, const float *obs, double *l2, const
                                 s->rec_i.data(), s->rec_j.data(), o, &h, ds->stream);
     else
         st = dn_fail(DN_EDEVICE, "dn_shot_residual: %s", cudaGetErrorString(e));
-    cudaFree(dobs);
+    dn_free(dobs);
     if (st) return st;
     s->has_res[k] = 1;
     if (l2) *l2 = h;

@@ -91,10 +91,10 @@ extern "C" int dn_dot(const double *a, const double *b, long long n, double *out
 {
     if (!a || !b || !out || n < 0) return dn_fail(DN_EINVAL, "dn_dot: bad arguments");
     double *scratch = nullptr;
-    if (cudaMalloc(&scratch, sizeof(double) * (DOT_BLOCKS + 1)) != cudaSuccess)
+    if (dn_malloc(&scratch, sizeof(double) * (DOT_BLOCKS + 1)) != cudaSuccess)
         return dn_fail(DN_ENOMEM, "dn_dot: scratch allocation failed");
     int st = dot_on(a, b, n, scratch, 0, out);
-    cudaFree(scratch);
+    dn_free(scratch);
     return st;
 }
 
@@ -109,9 +109,9 @@ extern "C" int dn_lbfgs_create(long long n, int m, int device, dn_lbfgs **out)
     L->n = n;
     L->m = m;
     L->rho.assign(m, 0.0);
-    if (cudaMalloc(&L->S, sizeof(double) * n * m) != cudaSuccess ||
-        cudaMalloc(&L->Y, sizeof(double) * n * m) != cudaSuccess ||
-        cudaMalloc(&L->scratch, sizeof(double) * (DOT_BLOCKS + 1)) != cudaSuccess ||
+    if (dn_malloc(&L->S, sizeof(double) * n * m) != cudaSuccess ||
+        dn_malloc(&L->Y, sizeof(double) * n * m) != cudaSuccess ||
+        dn_malloc(&L->scratch, sizeof(double) * (DOT_BLOCKS + 1)) != cudaSuccess ||
         cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
         dn_lbfgs_destroy(L);
@@ -126,9 +126,9 @@ extern "C" int dn_lbfgs_destroy(dn_lbfgs *L)
     if (!L) return DN_OK;
     cudaSetDevice(L->device);
     if (L->stream) cudaStreamSynchronize(L->stream);
-    cudaFree(L->S);
-    cudaFree(L->Y);
-    cudaFree(L->scratch);
+    dn_free(L->S);
+    dn_free(L->Y);
+    dn_free(L->scratch);
     if (L->stream) cudaStreamDestroy(L->stream);
     delete L;
     return DN_OK;

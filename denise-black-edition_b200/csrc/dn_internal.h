@@ -43,6 +43,19 @@ int dn_model_view_get(dn_model *m, dn_model_view *v);
     } while (0)
 #endif
 
+#ifdef __CUDACC__
+/* Device memory through the library's block cache (dn_alloc.cu): drop-in
+ * replacements of cudaMalloc / cudaFree on the current device. */
+cudaError_t dn_malloc_bytes(void **p, size_t bytes);
+template <typename T>
+inline cudaError_t dn_malloc(T **p, size_t bytes)
+{
+    return dn_malloc_bytes(reinterpret_cast<void **>(p), bytes);
+}
+void dn_free(void *p);
+size_t dn_pool_idle_bytes(int device);
+#endif
+
 #ifdef __cplusplus
 #include <nvtx3/nvToolsExt.h>
 /* NVTX range for the duration of a scope (shows the library's phases in a

@@ -53,7 +53,6 @@ struct Inst {
     const float *rho, *vp, *vs;                       // raw model (gradient terms)
     const float *c_muipjp, *c_tausipjp, *c_mu, *c_taus, *c_pi, *c_taup;   // visco
     const float *gmuss, *glamss;                      // muss, lamss of psv.c:333-334
-    const double2 *grcp;                              // [ny][nx] {RN(1/muss^2), RN(1/(lamss+muss)^2)}
     float eta[DN_MAX_L], bip[DN_MAX_L], cip[DN_MAX_L];
     // visco free-surface constants per column i (index i-1)
     const float *s_mu, *s_pi, *s_taus, *s_taup;
@@ -1414,11 +1413,11 @@ template <> __device__ __forceinline__ float snap_at<DN_SNAP_BF16>(const void *b
 
 // ===========================================================================
 // Adjoint cross-correlation, psv.c:313-387 (GRAD_FORM 1, INVMAT1 1), at the
-// adjoint steps whose mirrored forward step NT-nt+1 stored a snapshot.  The
-// mu term's three double divisions take their reciprocals from the model's
-// grcp table, {RN(1/muss^2), RN(1/(lamss+muss)^2)} per cell: psv.c's first
-// term multiplies by 1/muss^2 itself and the other two quotients come out of
-// ddiv_rcp, so every term is bit-identical to the divisions it replaces.
+// adjoint steps whose mirrored forward step NT-nt+1 stored a snapshot.  Of the
+// mu term's three double divisions, the two by muss^2 share one reciprocal:
+// psv.c's first term multiplies by 1.0/(muss*muss) itself and the third
+// quotient comes out of ddiv_rcp from the same reciprocal, bit-identical to
+// the division it replaces.
 // ===========================================================================
 // accumulator update in the accumulator's precision: float sums as psv.c's
 // float grad arrays, double sums for DN_ACC_F64
@@ -1460,7 +1459,6 @@ __device__ __forceinline__ void correlate_tile(const Inst &I, int k, int b, int 
         const float vxp1 = I.vxp1[o], vyp1 = I.vyp1[o];
         const float sxx = I.sxx[o], syy = I.syy[o], sxy = I.sxy[o];
         const float muss = I.gmuss[o], lamss = I.glamss[o];
-        const double2 y = I.grcp[w0 + w];
         const A ar = wcr[w], al = wc[w], au = wcu[w];
         float vx = 0.0f, vy = 0.0f, wrv = 0.0f;
         if (wr) {
@@ -1475,9 +1473,10 @@ __device__ __forceinline__ void correlate_tile(const Inst &I, int k, int b, int 
         if (mpos) {
             const double mm = (double)__fmul_rn(muss, muss);
             const float lm = __fadd_rn(lamss, muss);
-            const double t1 = DMUL(y.x, (double)__fmul_rn(fu, sxy));
-            const double t2 = ddiv_rcp(DMUL(0.25, (double)tlam), (double)__fmul_rn(lm, lm), y.y);
-            const double t3 = ddiv_rcp(DMUL(0.25, (double)__fmul_rn(__fsub_rn(fx, fy), __fsub_rn(sxx, syy))), mm, y.x);
+            const double y = DDIV(1.0, mm);
+            const double t1 = DMUL(y, (double)__fmul_rn(fu, sxy));
+            const double t2 = DDIV(DMUL(0.25, (double)tlam), (double)__fmul_rn(lm, lm));
+            const double t3 = ddiv_rcp(DMUL(0.25, (double)__fmul_rn(__fsub_rn(fx, fy), __fsub_rn(sxx, syy))), mm, y);
             tmu = DADD(DADD(t1, t2), t3);
         }
         wcr[w] = acc_add(ar, trho);

@@ -224,7 +224,7 @@ struct dn_precond_plan {
 
 static int upload(void **dst, const void *src, size_t bytes)
 {
-    if (cudaMalloc(dst, bytes) != cudaSuccess) return dn_fail(DN_ENOMEM, "gradient conditioning: %zu bytes", bytes);
+    if (dn_malloc(dst, bytes) != cudaSuccess) return dn_fail(DN_ENOMEM, "gradient conditioning: %zu bytes", bytes);
     if (cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
         return dn_fail(DN_EDEVICE, "gradient conditioning: copy to the device failed");
     return DN_OK;
@@ -286,7 +286,7 @@ extern "C" int dn_precond_destroy(dn_precond_plan *p)
     if (p->stream) cudaStreamSynchronize(p->stream);
     void *bufs[] = {p->vrow, p->hcol, p->src, p->file[0], p->file[1], p->file[2], p->mask, p->dx, p->ex, p->dz,
                     p->ez, p->gk, p->tab, p->sums, p->off, p->flag, p->maxbits, p->scratch};
-    for (void *b : bufs) cudaFree(b);
+    for (void *b : bufs) dn_free(b);
     if (p->stream) cudaStreamDestroy(p->stream);
     delete p;
     return DN_OK;
@@ -386,10 +386,10 @@ extern "C" int dn_precond_create(int nx, int ny, float dh, const dn_precond *c, 
             if ((st = upload((void **)&p->gk, k.data(), sizeof(float) * k.size()))) return fail(st);
         }
     }
-    if (c->spatfilter >= 2 && cudaMalloc(&p->scratch, n * sizeof(double)) != cudaSuccess)
+    if (c->spatfilter >= 2 && dn_malloc(&p->scratch, n * sizeof(double)) != cudaSuccess)
         return fail(dn_fail(DN_ENOMEM, "dn_precond_create: scratch"));
-    if (c->spatfilter == 4 && (cudaMalloc(&p->flag, sizeof(int)) != cudaSuccess ||
-                               cudaMalloc(&p->maxbits, sizeof(unsigned)) != cudaSuccess))
+    if (c->spatfilter == 4 && (dn_malloc(&p->flag, sizeof(int)) != cudaSuccess ||
+                               dn_malloc(&p->maxbits, sizeof(unsigned)) != cudaSuccess))
         return fail(dn_fail(DN_ENOMEM, "dn_precond_create"));
     *out = p;
     return DN_OK;
@@ -426,9 +426,9 @@ static int gauss_var_table(const dn_precond_plan *p, const dn_model_view &v, cud
     size_t q = 0;
     for (int hx = 3; hx <= HX; hx++)
         for (int hz = 3; hz <= HZ; hz++, q++) sums[q] = dnp_gauss_kernel(hx, hz, tab.data() + off[q]);
-    cudaFree(p->tab);
-    cudaFree(p->sums);
-    cudaFree(p->off);
+    dn_free(p->tab);
+    dn_free(p->sums);
+    dn_free(p->off);
     p->tab = p->sums = nullptr;
     p->off = nullptr;
     int s = upload((void **)&p->tab, tab.data(), sizeof(float) * tab.size());

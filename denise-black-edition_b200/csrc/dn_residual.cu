@@ -301,7 +301,7 @@ static int residual_bufs(ResBufs &b, int ntr, int nt, const dn_residual_opts *o,
     size_t off_s2 = off_s1 + up(4 * n7), off_k = off_s2 + up(4 * n7);
     size_t off_i = off_k + (o->kill ? up(4 * (size_t)ntr) : 0), off_j = off_i + (pos ? up(4 * (size_t)ntr) : 0);
     size_t total = off_j + (pos ? up(4 * (size_t)ntr) : 0);
-    if (cudaMalloc(&b.buf, total) != cudaSuccess) {
+    if (dn_malloc(&b.buf, total) != cudaSuccess) {
         cudaGetLastError();
         return dn_fail(DN_ENOMEM, "residual: %zu bytes of device scratch", total);
     }
@@ -343,7 +343,7 @@ extern "C" int dn_residual_run_ex(const float *syn_tm, const float *obs, float *
     } else {
         cudaStreamSynchronize(st);
     }
-    cudaFree(b.buf);
+    dn_free(b.buf);
     if (!rc && misfit) *misfit = h;
     return rc;
 }
@@ -362,7 +362,7 @@ extern "C" int dn_residual_l2(const float *syn_tm, const float *obs, float *res,
         return dn_fail(DN_EINVAL, "dn_residual_l2: bad arguments");
     if (grad_form != 1 && grad_form != 2) return dn_fail(DN_EINVAL, "dn_residual_l2: GRAD_FORM must be 1 or 2");
     double *scratch = nullptr;
-    cudaError_t e = cudaMalloc(&scratch, sizeof(double) * ((size_t)ntr + 1));
+    cudaError_t e = dn_malloc(&scratch, sizeof(double) * ((size_t)ntr + 1));
     if (e != cudaSuccess) return dn_fail(DN_ENOMEM, "dn_residual_l2: scratch allocation failed");
     int st = dn_residual_l2_launch(syn_tm, obs, res, ntr, nt, dt, grad_form, scratch, 0);
     double h = 0.0;
@@ -370,7 +370,7 @@ extern "C" int dn_residual_l2(const float *syn_tm, const float *obs, float *res,
         e = cudaMemcpy(&h, scratch + ntr, sizeof(double), cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) st = dn_fail(DN_EDEVICE, "dn_residual_l2: %s", cudaGetErrorString(e));
     }
-    cudaFree(scratch);
+    dn_free(scratch);
     if (!st && l2) *l2 = h;
     return st;
 }

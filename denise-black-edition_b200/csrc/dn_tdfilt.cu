@@ -130,7 +130,7 @@ extern "C" int dn_tdfilt_host(float *traces, int ntr, int ns, float dt, int orde
     CU(cudaSetDevice(device));
     const size_t bytes = sizeof(float) * (size_t)ntr * ns;
     float *d = nullptr;
-    if (cudaMalloc(&d, bytes) != cudaSuccess) {
+    if (dn_malloc(&d, bytes) != cudaSuccess) {
         cudaGetLastError();
         return dn_fail(DN_ENOMEM, "dn_tdfilt_host: %zu bytes", bytes);
     }
@@ -139,7 +139,7 @@ extern "C" int dn_tdfilt_host(float *traces, int ntr, int ns, float dt, int orde
         st = launch(d, ntr, ns, dt, order, fc_low, fc_high, 0);
         if (!st) e = cudaMemcpy(traces, d, bytes, cudaMemcpyDeviceToHost);
     }
-    cudaFree(d);
+    dn_free(d);
     if (!st && e != cudaSuccess) st = dn_fail(DN_EDEVICE, "dn_tdfilt_host: %s", cudaGetErrorString(e));
     return st;
 }

@@ -198,6 +198,7 @@ SIGNATURES = {
     "dn_mat_update": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [_c_float_p] * 6 + [ctypes.c_float, _c_float_p,
                                      ctypes.c_int, _c_int_p, ctypes.c_float] + [_c_float_p] * 4),
     "dn_device_memory": (ctypes.c_int, [ctypes.c_int, _P(ctypes.c_size_t), _P(ctypes.c_size_t)]),
+    "dn_device_trim": (ctypes.c_int, [ctypes.c_int]),
     "dn_inp_read": (ctypes.c_int, [ctypes.c_char_p, _vp]),
     "dn_inp_nt": (ctypes.c_int, [_vp]),
     "dn_inp_params": (ctypes.c_int, [_vp, ctypes.c_float, _P(Params)]),

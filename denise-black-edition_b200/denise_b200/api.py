@@ -142,6 +142,18 @@ def model_footprint(params: PsvParams):
     return b.value
 
 
+def device_memory(device=0):
+    """(free, total) bytes of a device; free counts the blocks the library keeps cached."""
+    free, total = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    check(lib.dn_device_memory(int(device), ctypes.byref(free), ctypes.byref(total)))
+    return free.value, total.value
+
+
+def device_trim(device=0):
+    """Frees the device blocks the library keeps cached for reuse."""
+    check(lib.dn_device_trim(int(device)))
+
+
 def shot_footprint(params: PsvParams, ntr, store):
     b = ctypes.c_size_t(0)
     p = params.to_c()

@@ -152,8 +152,14 @@ typedef struct dn_shot dn_shot;     /* device-resident wavefield state of one sh
 const char *dn_last_error(void);      /* thread-local text of the last failure */
 int dn_version(int *major, int *minor);
 int dn_device_count(int *count);
-/* Free and total memory of a device (cudaMemGetInfo with that device current). */
+/* Free and total memory of a device (cudaMemGetInfo with that device current);
+ * free includes the blocks the library keeps cached for reuse. */
 int dn_device_memory(int device, size_t *free_bytes, size_t *total_bytes);
+/* Device memory of models and shots is cached per device when freed and
+ * handed to the next request of nearly the same size (DN_POOL=0: plain
+ * cudaMalloc / cudaFree).  Frees the cached blocks, e.g. before another
+ * allocator needs the memory. */
+int dn_device_trim(int device);
 
 /* ---- host set-up numerics (bit-identical to the reference) ----------------- */
 /* holbergcoeff(): src/holbergcoeff.c:19-90; hc[0..6] */
