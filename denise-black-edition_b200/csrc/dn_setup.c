@@ -13,6 +13,7 @@
 #include "denise_b200.h"
 #include "dn_internal.h"
 
+#include <complex.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -449,17 +450,29 @@ int dn_visc_cell_factors(const dn_params *p, const float *vp, const float *vs, c
 }
 
 /* ------------------------------------------------------------------------
- * Source wavelets, src/wavelet.c:39-94 (QUELLART 1, 2, 4, 5, 6) and the
- * N_ORDER integration of :97-106.
+ * Source wavelets, src/wavelet.c:33-106: QUELLART 1 Ricker, 2 fuchs-mueller,
+ * 3 samples from a file, 4 sin^3, 5 first derivative of a Gaussian, 6 spike
+ * (band-limited afterwards by the caller, FD_PSV.c:324-331), 7 Klauder
+ * (chirp from FC_SPIKE_1 to FC_SPIKE_2 over TS), then the N_ORDER
+ * integration of :97-106.  Float and double operations in the order and
+ * precision of the reference's expressions.
  * ------------------------------------------------------------------------ */
-int dn_wavelet(int quellart, int nt, float DT, float tshift, float fc, float a, int n_order, float *out)
+int dn_wavelet_ex(int quellart, int nt, float DT, float tshift, float fc, float a, int n_order, float fc_spike_1,
+                  float fc_spike_2, float ts_chirp, const float *file_signal, int file_ns, float *out)
 {
     if (!out || nt < 1) return dn_fail(DN_EINVAL, "dn_wavelet: bad arguments");
+    if (quellart == 3 && (!file_signal || file_ns < nt))
+        return dn_fail(DN_EINVAL, "QUELLART 3: the wavelet file holds %d samples, NT = %d", file_signal ? file_ns : 0, nt);
+    float k1 = 0.0f, f0 = 0.0f;
+    if (quellart == 7) {
+        k1 = (fc_spike_2 - fc_spike_1) / ts_chirp;   /* rate of change of the frequency */
+        f0 = (fc_spike_2 + fc_spike_1) / 2.0;        /* mid frequency */
+    }
     for (int k = 1; k <= nt; k++) {
         float t = (float)k * DT;
         float ts = 1.0 / fc;
         float ag = DN_PI * DN_PI * fc * fc;
-        float amp = 0.0, tau;
+        float amp = 0.0, tau, t1;
         switch (quellart) {
         case 1:
             tau = DN_PI * (t - 1.5 * ts - tshift) / (1.5 * ts);
@@ -468,6 +481,9 @@ int dn_wavelet(int quellart, int nt, float DT, float tshift, float fc, float a, 
         case 2:
             if ((t < tshift) || (t > (tshift + ts))) amp = 0.0;
             else amp = ((sin(2.0 * DN_PI * (t - tshift) * fc) - 0.5 * sin(4.0 * DN_PI * (t - tshift) * fc)));
+            break;
+        case 3:
+            amp = file_signal[k - 1];
             break;
         case 4:
             if ((t < tshift) || (t > (tshift + ts))) amp = 0.0;
@@ -482,8 +498,14 @@ int dn_wavelet(int quellart, int nt, float DT, float tshift, float fc, float a, 
             amp = 0.0;
             if (k == 1 + (int)floor(tshift / DT + 0.5)) amp = 1.0;
             break;
+        case 7:
+            ts = 1.5 / fc_spike_1;
+            t1 = t - ts - tshift;
+            amp = creal(cexp(0.0 + 2.0 * DN_PI * f0 * t1 * I) * sin(DN_PI * k1 * t1 * (ts_chirp - t1)) /
+                        (DN_PI * k1 * t1));
+            break;
         default:
-            return dn_fail(DN_ENOTSUP, "Which source-wavelet ? (QUELLART=%d is not built)", quellart);
+            return dn_fail(DN_ENOTSUP, "Which source-wavelet ? (QUELLART=%d)", quellart);
         }
         out[k - 1] = amp * a;
     }
@@ -492,4 +514,11 @@ int dn_wavelet(int quellart, int nt, float DT, float tshift, float fc, float a, 
         for (int k = 2; k <= nt; k++) out[k - 1] = out[k - 2] + out[k - 1] * DT;
     }
     return DN_OK;
+}
+
+int dn_wavelet(int quellart, int nt, float DT, float tshift, float fc, float a, int n_order, float *out)
+{
+    if (quellart == 3 || quellart == 7)
+        return dn_fail(DN_EINVAL, "dn_wavelet: QUELLART %d needs dn_wavelet_ex (file samples / chirp band)", quellart);
+    return dn_wavelet_ex(quellart, nt, DT, tshift, fc, a, n_order, 0.0f, 0.0f, 0.0f, NULL, 0, out);
 }

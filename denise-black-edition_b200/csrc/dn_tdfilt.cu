@@ -94,7 +94,9 @@ int check_args(int ntr, int ns, float dt, int order, float fc_low, float fc_high
     if (ntr < 1 || ns < 1 || !(dt > 0.0f)) return dn_fail(DN_EINVAL, "dn_tdfilt: %d traces of %d samples, DT %g", ntr, ns, dt);
     if (order < 1 || order > 16) return dn_fail(DN_EINVAL, "dn_tdfilt: filter order %d (1..16)", order);
     if (!(fc_low > 0.0f)) return dn_fail(DN_EINVAL, "dn_tdfilt: low-pass corner %g must be positive", fc_low);
-    if (fc_high < 0.0f || fc_high != fc_high) return dn_fail(DN_EINVAL, "dn_tdfilt: high-pass corner %g", fc_high);
+    // apply_tdfilt.c high-passes only for fc1 > 0: zero or negative corners (the
+    // FC_SPIKE_1 = -5 of the reference's example files) mean no high-pass
+    if (fc_high != fc_high) return dn_fail(DN_EINVAL, "dn_tdfilt: high-pass corner %g", fc_high);
     return DN_OK;
 }
 

@@ -139,6 +139,9 @@ SIGNATURES = {
     "dn_prepare_visc": (ctypes.c_int, [_P(Params)] + [_c_float_p] * 16),
     "dn_wavelet": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                   ctypes.c_float, ctypes.c_float, ctypes.c_int, _c_float_p]),
+    "dn_wavelet_ex": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                     ctypes.c_float, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                     _c_float_p, ctypes.c_int, _c_float_p]),
     "dn_model_create": (ctypes.c_int, [_P(Params), _c_float_p, _c_float_p, _c_float_p,
                                        _c_float_p, _c_float_p, ctypes.c_int, _P(_vp)]),
     "dn_model_destroy": (ctypes.c_int, [_vp]),
@@ -204,6 +207,7 @@ SIGNATURES = {
     "dn_inp_params": (ctypes.c_int, [_vp, ctypes.c_float, _P(Params)]),
     "dn_read_model_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _c_float_p]),
     "dn_read_sources": (ctypes.c_int, [ctypes.c_char_p, _P(ctypes.c_int), _P(_c_float_p), _P(ctypes.c_float)]),
+    "dn_read_signal_file": (ctypes.c_int, [ctypes.c_char_p, _P(ctypes.c_int), _P(_c_float_p)]),
     "dn_source_cell": (ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.c_float, _P(ctypes.c_int),
                                       _P(ctypes.c_int)]),
     "dn_read_receivers": (ctypes.c_int, [ctypes.c_char_p, _c_float_p, ctypes.c_float, _P(ctypes.c_int),

@@ -122,9 +122,16 @@ def prepare_visc(params: PsvParams, vp, vs, rho, qp=None, qs=None):
     return out
 
 
-def wavelet(quellart, nt, dt, tshift, fc, amp, n_order=0):
+def wavelet(quellart, nt, dt, tshift, fc, amp, n_order=0, fc_spike_1=0.0, fc_spike_2=0.0, ts=0.0, signal=None):
+    """wavelet.c for one source.  QUELLART 3 takes `signal` (the samples of the
+    wavelet file, at least nt), 7 the chirp band FC_SPIKE_1..FC_SPIKE_2 over TS;
+    the spike of 6 comes unfiltered (band-limit it with tdfilt)."""
     out = np.zeros(nt, np.float32)
-    check(lib.dn_wavelet(quellart, nt, dt, tshift, fc, amp, n_order, fptr(out)))
+    sig = None if signal is None else np.ascontiguousarray(signal, np.float32)
+    check(lib.dn_wavelet_ex(int(quellart), int(nt), ctypes.c_float(dt), ctypes.c_float(tshift), ctypes.c_float(fc),
+                            ctypes.c_float(amp), int(n_order), ctypes.c_float(fc_spike_1), ctypes.c_float(fc_spike_2),
+                            ctypes.c_float(ts), None if sig is None else fptr(sig), 0 if sig is None else sig.size,
+                            fptr(out)))
     return out
 
 

@@ -83,6 +83,16 @@ def read_sources(path):
     return out, ts.value
 
 
+def read_signal_file(path):
+    """rd_sour: the samples of a QUELLART 3 wavelet file (one per line)."""
+    n = ctypes.c_int()
+    sp = _lib._c_float_p()
+    check(lib.dn_read_signal_file(str(path).encode(), ctypes.byref(n), ctypes.byref(sp)))
+    out = np.ctypeslib.as_array(sp, shape=(max(n.value, 1),)).copy()[:n.value]
+    _libc_free(sp)
+    return out
+
+
 def source_cell(x, y, dh):
     i, j = ctypes.c_int(), ctypes.c_int()
     check(lib.dn_source_cell(ctypes.c_float(x), ctypes.c_float(y), ctypes.c_float(dh), ctypes.byref(i),

@@ -35,9 +35,11 @@ static void free_src(shot_src *s)
     memset(s, 0, sizeof(*s));
 }
 
-/* sources of shot `k` (0-based) in grid indices, with their wavelets */
+/* sources of shot `k` (0-based) in grid indices, with their wavelets (wavelet.c;
+ * QUELLART 3 reads "<SIGNAL_FILE>_shot_<k+1>.dat", 7 chirps over ts = TS, and
+ * the spike of QUELLART 6 is band-limited as FD_PSV.c:324-331 does) */
 static int build_sources(const dn_inp *in, const dn_params *p, const float *srcpos, int nsrc, int k, int all,
-                         shot_src *out)
+                         float ts, int device, shot_src *out)
 {
     memset(out, 0, sizeof(*out));
     const int first = all ? 0 : k, count = all ? nsrc : 1;
@@ -53,12 +55,24 @@ static int build_sources(const dn_inp *in, const dn_params *p, const float *srcp
     const float *s0 = srcpos + (size_t)k * 8;
     out->xs = s0[0];
     out->ys = s0[1];
+    float *file_sig = NULL;
+    int file_ns = 0;
+    if (in->quellart == 3) {
+        char path[2 * DN_STR];
+        snprintf(path, sizeof(path), "%s_shot_%i.dat", in->signal_file, k + 1);
+        int st = dn_read_signal_file(path, &file_ns, &file_sig);
+        if (st) {
+            free_src(out);
+            return st;
+        }
+    }
     int n = 0;
     for (int l = first; l < first + count; l++) {
         const float *s = srcpos + (size_t)l * 8;
         int i, j;
         int st = dn_source_cell(s[0], s[1], p->dh, &i, &j);
         if (st) {
+            free(file_sig);
             free_src(out);
             return st;
         }
@@ -71,14 +85,24 @@ static int build_sources(const dn_inp *in, const dn_params *p, const float *srcp
         out->sj[n] = j;
         out->type[n] = (int)s[7];
         out->azi[n] = s[6];
-        st = dn_wavelet(in->quellart, p->nt, p->dt, s[3], s[4], s[5], 0, out->sig + (size_t)n * p->nt);
+        st = dn_wavelet_ex(in->quellart, p->nt, p->dt, s[3], s[4], s[5], 0, in->fc_spike_1, in->fc_spike_2, ts,
+                           file_sig, file_ns, out->sig + (size_t)n * p->nt);
         if (st) {
+            free(file_sig);
             free_src(out);
             return st;
         }
         n++;
     }
+    free(file_sig);
     out->nsrc = n;
+    if (in->quellart == 6 && n > 0) {
+        const int st = dn_tdfilt_host(out->sig, n, p->nt, p->dt, in->order_spike, in->fc_spike_2, in->fc_spike_1, device);
+        if (st) {
+            free_src(out);
+            return st;
+        }
+    }
     return DN_OK;
 }
 
@@ -117,8 +141,6 @@ int dn_forward_inp(const char *inp_path, int device)
     if (in.srcrec != 1) return dn_fail(DN_ENOTSUP, "SRCREC=%d: sources are read from SOURCE_FILE (SRCREC=1)", in.srcrec);
     if (in.readrec != 1) return dn_fail(DN_ENOTSUP, "READREC=%d: receivers are read from one REC_FILE (READREC=1)", in.readrec);
     if (in.seis_format != 1) return dn_fail(DN_ENOTSUP, "SEIS_FORMAT=%d: SU output (1) is built", in.seis_format);
-    if (in.quellart == 3 || in.quellart == 6 || in.quellart == 7)
-        return dn_fail(DN_ENOTSUP, "QUELLART=%d (file, filtered spike, Klauder) is not built", in.quellart);
     if (in.seismo < 1 || in.seismo > 4) return dn_fail(DN_EINVAL, "SEISMO=%d: nothing to record", in.seismo);
 
     int nsrc = 0, ntr = 0, *ri = NULL, *rj = NULL;
@@ -173,7 +195,7 @@ int dn_forward_inp(const char *inp_path, int device)
     for (int b0 = 0; !st && b0 < nshots; b0 += per_batch) {
         const int b1 = b0 + per_batch < nshots ? b0 + per_batch : nshots;
         for (int k = b0; k < b1 && !st; k++) {
-            st = build_sources(&in, &p, srcpos, nsrc, k, !in.run_multiple_shots, &srcs[k]);
+            st = build_sources(&in, &p, srcpos, nsrc, k, !in.run_multiple_shots, ts, device, &srcs[k]);
             if (st) break;
             dn_acq a = {srcs[k].nsrc, srcs[k].si, srcs[k].sj, srcs[k].type, srcs[k].azi, srcs[k].sig, ntr, ri, rj};
             st = dn_shot_create(model, &a, &shots[k]);

@@ -190,6 +190,30 @@ int dn_read_model_file(const char *path, int nx, int ny, float *out)
     return DN_OK;
 }
 
+int dn_read_signal_file(const char *path, int *ns, float **samples)
+{
+    if (!path || !ns || !samples) return dn_fail(DN_EINVAL, "dn_read_signal_file: null argument");
+    *samples = NULL;
+    *ns = 0;
+    FILE *f = fopen(path, "r");
+    if (!f) return dn_fail(DN_EIO, " Source file %s could no be opened !", path);
+    int n = 0, c;
+    while ((c = fgetc(f)) != EOF)   /* rd_sour.c:18-20: one sample per newline */
+        if (c == '\n') n++;
+    rewind(f);
+    float *v = (float *)calloc((size_t)(n > 0 ? n : 1), sizeof(float));
+    if (!v) {
+        fclose(f);
+        return dn_fail(DN_ENOMEM, "dn_read_signal_file: out of memory");
+    }
+    for (int k = 0; k < n; k++)
+        if (fscanf(f, "%e\n", &v[k]) != 1) break;   /* unread samples stay 0, as vector() left them */
+    fclose(f);
+    *ns = n;
+    *samples = v;
+    return DN_OK;
+}
+
 int dn_read_sources(const char *path, int *nsrc, float **srcpos, float *ts)
 {
     if (!path || !nsrc || !srcpos) return dn_fail(DN_EINVAL, "dn_read_sources: null argument");

@@ -184,6 +184,14 @@ int dn_prepare_visc(const dn_params *p, const float *vp, const float *vs, const 
 /* Ricker / fumue / sin^3 / Gaussian-derivative / spike wavelets of wavelet.c:12-120
  * (QUELLART 1,2,4,5,6) for one source, with N_ORDER time integrations.  out[nt]. */
 int dn_wavelet(int quellart, int nt, float dt, float tshift, float fc, float amp, int n_order, float *out);
+/* wavelet(): src/wavelet.c:33-106 for one source, every QUELLART: 3 takes its
+ * samples from `file_signal` (file_ns >= nt values, as dn_read_signal_file
+ * reads "<SIGNAL_FILE>_shot_<n>.dat"), 6 is the unfiltered spike (the callers
+ * of wavelet() band-limit it with apply_tdfilt(ORDER_SPIKE, FC_SPIKE_2,
+ * FC_SPIKE_1): dn_tdfilt), 7 the Klauder chirp from FC_SPIKE_1 to FC_SPIKE_2
+ * over TS (ts_chirp).  dn_wavelet covers QUELLART 1, 2, 4, 5 and 6. */
+int dn_wavelet_ex(int quellart, int nt, float dt, float tshift, float fc, float amp, int n_order, float fc_spike_1,
+                  float fc_spike_2, float ts_chirp, const float *file_signal, int file_ns, float *out);
 
 /* ---- models and shots (device) -------------------------------------------- */
 /* Builds every derived coefficient on the host (the functions above) and uploads

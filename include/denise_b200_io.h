@@ -9,6 +9,7 @@
  *   readmod_elastic_PSV src/PSV/readmod_elastic_PSV.c:72-85, readmod_visc_PSV (model files)
  *   sources             src/sources.c:11       (SOURCE_FILE table)
  *   receiver            src/receiver.c:11      (REC_FILE table, READREC = 1)
+ *   rd_sour             src/rd_sour.c:9        (QUELLART 3 wavelet file)
  *   splitsrc            src/splitsrc.c         (source grid indices, one rank)
  *   outseis_glob        src/outseis_glob.c:12  (SU output, SEIS_FORMAT = 1)
  *   saveseis_glob       src/saveseis_glob.c    (file names per SEISMO)
@@ -94,6 +95,11 @@ int dn_read_model_file(const char *path, int nx, int ny, float *out);
  * type.  *ts = 1 / max fc.  The caller frees *srcpos with free(). */
 int dn_read_sources(const char *path, int *nsrc, float **srcpos, float *ts);
 
+/* rd_sour (src/rd_sour.c): the wavelet file of QUELLART 3,
+ * "<SIGNAL_FILE>_shot_<n>.dat", one sample per line; *ns = the number of
+ * newlines.  The caller frees *samples with free(). */
+int dn_read_signal_file(const char *path, int *ns, float **samples);
+
 /* Source grid indices of one rank (splitsrc.c): iround(x / DH), iround(y / DH). */
 int dn_source_cell(float x, float y, float dh, int *i, int *j);
 
@@ -114,7 +120,8 @@ int dn_write_su(const char *path, const float *section, int ntr, int nt, int ndt
 int dn_read_su(const char *path, int ntr, int ns, float *section);
 
 /* MODE 0 of FD_PSV for a parameter file: models, sources, receivers, wavelets
- * (QUELLART 1, 2, 4, 5); one shot per line of the source table, firing that
+ * (QUELLART 1-7; 3 from "<SIGNAL_FILE>_shot_<n>.dat", the spike of 6
+ * band-limited by ORDER_SPIKE, FC_SPIKE_2, FC_SPIKE_1); one shot per line of the source table, firing that
  * source (RUN_MULTIPLE_SHOTS = 1) or all sources (0), as count_src.c and
  * FD_PSV.c:252-300 do; the shots run as batches on `device` and the
  * seismograms are written as saveseis_glob names them (SEIS_FILE_*.shot<n>).

@@ -767,3 +767,33 @@ int refh_read_par_inv(const char *path, int nstage, int stagemax, double *out)
     MYID = 0;
     return 0;
 }
+
+/* wavelet() of the reference for one source with every global it reads set here:
+ * NT, DT, QUELLART, N_ORDER, FC_SPIKE_1, FC_SPIKE_2, TS and SIGNAL_FILE (QUELLART 3
+ * reads "<signal_file>_shot_<ishot>.dat"); for QUELLART 6 the caller's
+ * apply_tdfilt with ORDER_SPIKE, FC_SPIKE_2, FC_SPIKE_1 follows when filt > 0. */
+extern float FC_SPIKE_1, FC_SPIKE_2;
+int refh_wavelet_ex(int quellart, int n_order, int nt, float dt, float tshift, float fc, float amp, float fc_spike_1,
+                    float fc_spike_2, float ts, const char *signal_file, int ishot, int filt_order, float *out)
+{
+    if (!FP) FP = null_log();   /* wavelet() logs to FP */
+    float **sp = matrix(1, 8, 1, 1);
+    sp[4][1] = tshift;
+    sp[5][1] = fc;
+    sp[6][1] = amp;
+    NT = nt;
+    DT = dt;
+    QUELLART = quellart;
+    N_ORDER = n_order;
+    FC_SPIKE_1 = fc_spike_1;
+    FC_SPIKE_2 = fc_spike_2;
+    TS = ts;
+    if (signal_file) snprintf(SIGNAL_FILE, STRING_SIZE, "%s", signal_file);
+    float **sig = wavelet(sp, 1, ishot);
+    if (quellart == 6 && filt_order > 0) apply_tdfilt(sig, 1, nt, filt_order, fc_spike_2, fc_spike_1);
+    for (int t = 1; t <= nt; t++) out[t - 1] = sig[1][t];
+    N_ORDER = 0;
+    free_matrix(sig, 1, 1, 1, nt);
+    free_matrix(sp, 1, 8, 1, 1);
+    return 0;
+}

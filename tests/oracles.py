@@ -312,6 +312,24 @@ def ref_calc_res_ex(workdir, data, syn, dt, dh, iopt, fopt, rec_i, rec_j, src, k
     return out, l2
 
 
+def ref_wavelet_ex(workdir, quellart, n_order, nt, dt, tshift, fc, amp, fc_spike_1=0.0, fc_spike_2=0.0, ts=0.0,
+                   signal=None, ishot=1, filt_order=0):
+    """The reference's wavelet() (and, for QUELLART 6 with filt_order > 0, the
+    apply_tdfilt of FD_PSV.c:324-331) for one source; QUELLART 3 reads
+    `signal` from "sig_shot_<ishot>.dat" in workdir.  Run it in run_isolated()."""
+    os.chdir(workdir)
+    lib = _ref_lib()
+    if signal is not None:
+        with open(f"sig_shot_{ishot}.dat", "w") as f:
+            f.write("".join(f"{float(v):.9e}\n" for v in np.asarray(signal, np.float32)))
+    out = np.zeros(nt, np.float32)
+    lib.refh_wavelet_ex(ctypes.c_int(quellart), ctypes.c_int(n_order), ctypes.c_int(nt), ctypes.c_float(dt),
+                        ctypes.c_float(tshift), ctypes.c_float(fc), ctypes.c_float(amp), ctypes.c_float(fc_spike_1),
+                        ctypes.c_float(fc_spike_2), ctypes.c_float(ts), b"sig", ctypes.c_int(ishot),
+                        ctypes.c_int(filt_order), out.ctypes.data_as(_f))
+    return out
+
+
 def ref_apply_tdfilt(data, dt, order, fc2, fc1):
     """The reference's apply_tdfilt on [ntr][ns] float32 traces; run it in run_isolated()."""
     lib = _ref_lib()

@@ -25,6 +25,10 @@ CASES = {
     "elastic-all-components-ndt2": dict(SEISMO=4, NDT=2, FREE_SURF=0, FDORDER=6),
     "one-shot-all-sources": dict(RUN_MULTIPLE_SHOTS=0, nshots=2),
     "rotated-force-sources": dict(src_type=4),
+    "spike-band-pass-quellart6": dict(QUELLART=6, FC_SPIKE_1=5.0, FC_SPIKE_2=40.0, ORDER_SPIKE=4),
+    "spike-low-pass-quellart6": dict(QUELLART=6, FC_SPIKE_1=-5.0, FC_SPIKE_2=30.0, ORDER_SPIKE=5),
+    "wavelet-file-quellart3": dict(QUELLART=3, SIGNAL_FILE="wavelet/sig", wavelet_files=True),
+    "klauder-quellart7": dict(QUELLART=7, FC_SPIKE_1=7.0, FC_SPIKE_2=45.0),
 }
 
 
@@ -43,7 +47,16 @@ def _make(root, kw):
     kw = dict(kw)
     nshots = kw.pop("nshots", 3)
     styp = kw.pop("src_type", 1)
+    wavelet_files = kw.pop("wavelet_files", False)
     inp = inp_case.write_case(root, nshots=nshots, **kw)
+    if wavelet_files:   # QUELLART 3: "<SIGNAL_FILE>_shot_<n>.dat", one sample per line
+        os.makedirs(os.path.join(root, "wavelet"), exist_ok=True)
+        nt = io.inp_nt(io.read_inp(inp))
+        for k in range(1, nshots + 1):
+            rng = np.random.default_rng(100 + k)
+            w = 1e3 * np.cumsum(rng.standard_normal(nt + 3)).astype(np.float32) / np.sqrt(nt)
+            with open(os.path.join(root, "wavelet", f"sig_shot_{k}.dat"), "w") as f:
+                f.write("".join(f"{v:.7e}\n" for v in w))
     if styp != 1:
         path = os.path.join(root, "source", "sources.dat")
         lines = open(path).read().splitlines()

@@ -91,3 +91,48 @@ def test_setup_matches_live_reference(kw):
     pv = dn.prepare_visc(p, vp, vs, rho, qp, qs)
     np.testing.assert_array_equal(pv["fipjp"], R["fipjp"])
     np.testing.assert_array_equal(pv["d"][0], R["d1"])
+
+
+# (QUELLART, n_order, tshift, fc, amp, fc_spike_1, fc_spike_2, ts)
+WAVELETS = [(1, 0, 0.01, 12.0, 2.5, 0, 0, 0), (1, 2, 0.0, 30.0, 1.0, 0, 0, 0), (2, 0, 0.004, 40.0, 1.0, 0, 0, 0),
+            (4, 1, 0.002, 25.0, 3.0, 0, 0, 0), (5, 0, 0.0, 18.0, 1.0, 0, 0, 0), (6, 0, 0.0135, 10.0, 7.0, 0, 0, 0),
+            (6, 1, 0.0, 10.0, 1.0, 0, 0, 0), (7, 0, 0.003, 10.0, 2.0, 7.0, 45.0, 0.04),
+            (7, 1, 0.0, 10.0, 1.0, 12.0, 60.0, 0.03), (3, 0, 0.0, 10.0, 1.5, 0, 0, 0), (3, 2, 0.0, 10.0, 1.0, 0, 0, 0)]
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="reference build not present")
+@pytest.mark.parametrize("w", WAVELETS, ids=lambda w: f"q{w[0]}-n{w[1]}-t{w[2]}")
+def test_wavelets_match_live_reference(tmp_path, w):
+    """dn_wavelet_ex against the reference's wavelet() with every global it reads
+    set: all seven QUELLART, time shifts on and off the sample grid, N_ORDER
+    integrations, the Klauder chirp band and the wavelet file of QUELLART 3."""
+    qa, n_order, tshift, fc, amp, f1, f2, ts = w
+    nt, dt = 700, 2.5e-4
+    signal = None
+    if qa == 3:
+        rng = np.random.default_rng(7)
+        signal = np.cumsum(rng.standard_normal(nt + 5)).astype(np.float32)
+    want = O.run_isolated(O.ref_wavelet_ex, str(tmp_path), qa, n_order, nt, dt, tshift, fc, amp, f1, f2, ts, signal)
+    if qa == 3:   # what the reference read back from the text file
+        from denise_b200 import io
+
+        signal = io.read_signal_file(str(tmp_path / "sig_shot_1.dat"))
+        assert signal.size == nt + 5
+    got = dn.wavelet(qa, nt, dt, tshift, fc, amp, n_order, fc_spike_1=f1, fc_spike_2=f2, ts=ts, signal=signal)
+    np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_wavelet_file_shorter_than_nt_is_rejected():
+    """A wavelet file with fewer samples than NT is an error (the reference would
+    read past its buffer); dn_wavelet asks for dn_wavelet_ex for QUELLART 3 and 7."""
+    import ctypes
+
+    from denise_b200 import _lib
+
+    with pytest.raises(dn.DeniseError, match="DN_EINVAL"):
+        dn.wavelet(3, 100, 1e-3, 0.0, 10.0, 1.0, signal=np.zeros(99, np.float32))
+    out = np.zeros(100, np.float32)
+    for qa in (3, 7):
+        with pytest.raises(dn.DeniseError, match="DN_EINVAL"):
+            _lib.check(_lib.lib.dn_wavelet(qa, 100, ctypes.c_float(1e-3), ctypes.c_float(0.0), ctypes.c_float(10.0),
+                                           ctypes.c_float(1.0), 0, out.ctypes.data_as(_lib._c_float_p)))

@@ -14,8 +14,11 @@ import tdfilt_oracle as tf  # noqa: E402
 
 needs_ref = pytest.mark.skipif(not O.reference_available(), reason="reference build not present")
 
-# (order, fc_low, fc_high): odd and even orders, low-pass only and band-pass
-CASES = [(4, 20.0, 0.0), (5, 30.0, 3.0), (2, 12.5, 1.0), (1, 40.0, 5.0), (6, 8.0, 2.0), (3, 45.0, 0.0)]
+# (order, fc_low, fc_high): odd and even orders, low-pass only and band-pass; a
+# negative high-pass corner (FC_SPIKE_1 = -5 in the reference's example files)
+# means no high-pass, as apply_tdfilt only high-passes for fc1 > 0
+CASES = [(4, 20.0, 0.0), (5, 30.0, 3.0), (2, 12.5, 1.0), (1, 40.0, 5.0), (6, 8.0, 2.0), (3, 45.0, 0.0),
+         (5, 15.0, -5.0)]
 
 
 def traces(seed=0, ntr=6, ns=500):
@@ -58,6 +61,6 @@ def test_device_filter_on_device_buffer_and_errors():
     _lib.check(_lib.lib.dn_tdfilt(t.data_ptr(), 8, 1000, ctypes.c_float(1e-3), 4, ctypes.c_float(25.0),
                                   ctypes.c_float(2.0)))
     np.testing.assert_array_equal(t.cpu().numpy(), tf.apply_tdfilt(d, 1e-3, 4, 25.0, 2.0))
-    for bad in ((0, 25.0, 0.0), (17, 25.0, 0.0), (4, 0.0, 0.0), (4, 25.0, -1.0)):
+    for bad in ((0, 25.0, 0.0), (17, 25.0, 0.0), (4, 0.0, 0.0), (4, 25.0, float("nan"))):
         with pytest.raises(dn.DeniseError, match="DN_EINVAL"):
             dn.tdfilt(d, 1e-3, *bad)
