@@ -39,6 +39,21 @@ class Inp(ctypes.Structure):
            ("gradt", ctypes.c_int * 5), ("invmat1", ctypes.c_int), ("grad_form", ctypes.c_int),
            ("quelltypb", ctypes.c_int), ("testshot", ctypes.c_int * 4), ("dtinv", ctypes.c_int),
            ("lnorm", ctypes.c_int), ("lines", ctypes.c_int)]
+        + [(n, ctypes.c_int) for n in ("sws_taper_grad_vert", "sws_taper_grad_hor")]
+        + [("exp_taper_grad_hor", ctypes.c_float)]
+        + [(n, ctypes.c_int) for n in ("sws_taper_grad_sources", "sws_taper_circular_per_shot", "srtshape")]
+        + [("srtradius", ctypes.c_float), ("filtsize", ctypes.c_int), ("sws_taper_file", ctypes.c_int),
+           ("tfile", ctypes.c_char * DN_STR), ("inv_mod_out", ctypes.c_int), ("inv_modelfile", ctypes.c_char * DN_STR)]
+        + [(n, ctypes.c_float) for n in ("vpupperlim", "vplowerlim", "vsupperlim", "vslowerlim", "rhoupperlim",
+                                         "rholowerlim", "qsupperlim", "qslowerlim")]
+        + [(n, ctypes.c_int) for n in ("grad_method", "pcg_beta", "nlbfgs", "model_filter", "filt_size")]
+        + [("eps_scale", ctypes.c_float), ("stepmax", ctypes.c_int), ("scalefac", ctypes.c_float),
+           ("trkill", ctypes.c_int)]
+        + [(n, ctypes.c_char * DN_STR) for n in ("trkill_file", "picks_file", "misfit_log_file")]
+        + [(n, ctypes.c_int) for n in ("min_iter", "grad_filter", "filt_size_grad", "timelapse")]
+        + [("data_dir_t0", ctypes.c_char * DN_STR)]
+        + [(n, ctypes.c_int) for n in ("rtmod", "gravity", "ngravb", "nzgrav", "grav_type", "back_density")]
+        + [("dfile", ctypes.c_char * DN_STR), ("rtm_shot", ctypes.c_int)]
     )
 
     def get(self, name):

@@ -29,8 +29,8 @@ typedef struct {
 } line_spec;
 
 #define OFF(f) offsetof(dn_inp, f)
-/* parameter lines the path uses, stored; every other line up to 115 is scanned
- * with its own format and discarded, so the stream advances identically */
+/* the parameter lines of read_par.c (cases 1-115), each scanned with its own
+ * format; lines past 115 are counted but not scanned, as in the reference */
 static const line_spec SPEC[] = {
     {1, K_INT, OFF(mode)}, {2, K_INT, OFF(physics)}, {3, K_INT, OFF(nprocx)}, {4, K_INT, OFF(nprocy)},
     {5, K_INT, OFF(fdorder)}, {6, K_INT, OFF(maxrelerror)}, {7, K_INT, OFF(nx)}, {8, K_INT, OFF(ny)},
@@ -50,41 +50,34 @@ static const line_spec SPEC[] = {
     {58, K_STR, OFF(log_file)}, {59, K_INT, OFF(log)}, {60, K_INT, OFF(itermax)}, {61, K_STR, OFF(jacobian)},
     {62, K_STR, OFF(data_dir)}, {63, K_INT, OFF(taper)}, {64, K_INT, OFF(taperlength)}, {65, K_INT4, OFF(gradt)},
     {66, K_INT, OFF(invmat1)}, {67, K_INT, OFF(grad_form)}, {68, K_INT, OFF(quelltypb)}, {69, K_INT3, OFF(testshot)},
-    {95, K_INT, OFF(dtinv)},
+    {70, K_INT, OFF(sws_taper_grad_vert)}, {71, K_INT, OFF(sws_taper_grad_hor)}, {72, K_FLT, OFF(exp_taper_grad_hor)},
+    {73, K_INT, OFF(sws_taper_grad_sources)}, {74, K_INT, OFF(sws_taper_circular_per_shot)},
+    {75, K_INT, OFF(srtshape)}, {76, K_FLT, OFF(srtradius)}, {77, K_INT, OFF(filtsize)},
+    {78, K_INT, OFF(sws_taper_file)}, {79, K_STR, OFF(tfile)}, {80, K_INT, OFF(inv_mod_out)},
+    {81, K_STR, OFF(inv_modelfile)}, {82, K_FLT, OFF(vpupperlim)}, {83, K_FLT, OFF(vplowerlim)},
+    {84, K_FLT, OFF(vsupperlim)}, {85, K_FLT, OFF(vslowerlim)}, {86, K_FLT, OFF(rhoupperlim)},
+    {87, K_FLT, OFF(rholowerlim)}, {88, K_FLT, OFF(qsupperlim)}, {89, K_FLT, OFF(qslowerlim)},
+    {90, K_INT, OFF(grad_method)}, {91, K_INT, OFF(pcg_beta)}, {92, K_INT, OFF(nlbfgs)},
+    {93, K_INT, OFF(model_filter)}, {94, K_INT, OFF(filt_size)}, {95, K_INT, OFF(dtinv)},
+    {96, K_FLT, OFF(eps_scale)}, {97, K_INT, OFF(stepmax)}, {98, K_FLT, OFF(scalefac)}, {99, K_INT, OFF(trkill)},
+    {100, K_STR, OFF(trkill_file)}, {101, K_STR, OFF(picks_file)}, {102, K_STR, OFF(misfit_log_file)},
+    {103, K_INT, OFF(min_iter)}, {104, K_INT, OFF(grad_filter)}, {105, K_INT, OFF(filt_size_grad)},
+    {106, K_INT, OFF(timelapse)}, {107, K_STR, OFF(data_dir_t0)}, {108, K_INT, OFF(rtmod)},
+    {109, K_INT, OFF(gravity)}, {110, K_INT, OFF(ngravb)}, {111, K_INT, OFF(nzgrav)}, {112, K_INT, OFF(grav_type)},
+    {113, K_INT, OFF(back_density)}, {114, K_STR, OFF(dfile)}, {115, K_INT, OFF(rtm_shot)},
 };
-#define LAST_PARAM_LINE 115
-
-/* format kind of a line that is not stored (read_par.c cases 70-115) */
-static int unstored_kind(int line)
-{
-    switch (line) {
-    case 72: case 76: case 82: case 83: case 84: case 85: case 86: case 87: case 88: case 89: case 96: case 98:
-        return K_FLT;
-    case 79: case 81: case 100: case 101: case 102: case 107: case 114:
-        return K_STR;
-    default:
-        return K_INT;
-    }
-}
 
 static void scan_line(FILE *fp, int line, dn_inp *in)
 {
     static char key[4096];
     int kind = -1;
     void *dst = NULL;
-    int ti[4];
-    float tf[2];
-    char ts[DN_STR];
     for (size_t k = 0; k < sizeof(SPEC) / sizeof(SPEC[0]); k++)
         if (SPEC[k].line == line) {
             kind = SPEC[k].kind;
             dst = (char *)in + SPEC[k].off;
         }
-    if (kind < 0) {
-        if (line > LAST_PARAM_LINE) return;   /* the reference's default: no scan */
-        kind = unstored_kind(line);
-        dst = kind == K_STR ? (void *)ts : kind == K_FLT ? (void *)tf : (void *)ti;
-    }
+    if (kind < 0) return;   /* past line 115: the reference's default, no scan */
     switch (kind) {
     case K_INT: (void)!fscanf(fp, "%4095s =%i", key, (int *)dst); break;
     case K_INT_NL: (void)!fscanf(fp, "\n%4095s =%i", key, (int *)dst); break;

@@ -66,6 +66,27 @@ typedef struct dn_inp {
     int taper, taperlength, gradt[5], invmat1, grad_form, quelltypb, testshot[4];
     int dtinv, lnorm;
     int lines;                 /* parameter lines counted (the reference's lineno) */
+    /* lines 70-115 (inversion; read_par.c cases 70-115) */
+    int sws_taper_grad_vert, sws_taper_grad_hor;
+    float exp_taper_grad_hor;
+    int sws_taper_grad_sources, sws_taper_circular_per_shot, srtshape;
+    float srtradius;
+    int filtsize, sws_taper_file;
+    char tfile[DN_STR];
+    int inv_mod_out;
+    char inv_modelfile[DN_STR];
+    float vpupperlim, vplowerlim, vsupperlim, vslowerlim, rhoupperlim, rholowerlim, qsupperlim, qslowerlim;
+    int grad_method, pcg_beta, nlbfgs, model_filter, filt_size;
+    float eps_scale;
+    int stepmax;
+    float scalefac;
+    int trkill;
+    char trkill_file[DN_STR], picks_file[DN_STR], misfit_log_file[DN_STR];
+    int min_iter, grad_filter, filt_size_grad, timelapse;
+    char data_dir_t0[DN_STR];
+    int rtmod, gravity, ngravb, nzgrav, grav_type, back_density;
+    char dfile[DN_STR];
+    int rtm_shot;
 } dn_inp;
 
 /* read_par: the reference's positional reader.  After a newline, the next

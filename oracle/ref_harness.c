@@ -797,3 +797,35 @@ int refh_wavelet_ex(int quellart, int n_order, int nt, float dt, float tshift, f
     free_matrix(sp, 1, 8, 1, 1);
     return 0;
 }
+
+/* read_par() lines 60-115 (inversion): iv[36] ints, fv[12] floats, strs 8 x 74 chars
+ * (TFILE, INV_MODELFILE, TRKILL_FILE, PICKS_FILE, MISFIT_LOG_FILE, DATA_DIR_T0, DFILE, DATA_DIR) */
+extern int ITERMAX, TAPER, TAPERLENGTH, TESTSHOT_START, TESTSHOT_END, TESTSHOT_INCR;
+extern int SWS_TAPER_CIRCULAR_PER_SHOT, INV_MOD_OUT, GRAD_METHOD, NLBFGS, PCG_BETA, MODEL_FILTER, FILT_SIZE;
+extern int STEPMAX, TRKILL, MIN_ITER, GRAD_FILTER, FILT_SIZE_GRAD, TIMELAPSE, RTMOD;
+extern int GRAVITY, NZGRAV, NGRAVB, GRAV_TYPE, BACK_DENSITY, RTM_SHOT;
+extern float EPS_SCALE, SCALEFAC, QSUPPERLIM, QSLOWERLIM;
+extern char INV_MODELFILE[STRING_SIZE], PICKS_FILE[STRING_SIZE], MISFIT_LOG_FILE[STRING_SIZE];
+extern char DATA_DIR_T0[STRING_SIZE], DFILE[STRING_SIZE], DATA_DIR[STRING_SIZE];
+int refh_read_par_fwi(const char *path, int *iv, float *fv, char *strs)
+{
+    FILE *f = fopen(path, "r");
+    if (!f) return -1;
+    if (!FL) FL = vector(1, 8);
+    read_par(f);   /* closes f */
+    const int I[36] = {ITERMAX, TAPER, TAPERLENGTH, GRADT1, GRADT2, GRADT3, GRADT4, TESTSHOT_START, TESTSHOT_END,
+                       TESTSHOT_INCR, SWS_TAPER_GRAD_VERT, SWS_TAPER_GRAD_HOR, SWS_TAPER_GRAD_SOURCES,
+                       SWS_TAPER_CIRCULAR_PER_SHOT, SRTSHAPE, FILTSIZE, SWS_TAPER_FILE, INV_MOD_OUT, GRAD_METHOD,
+                       PCG_BETA, NLBFGS, MODEL_FILTER, FILT_SIZE, STEPMAX, TRKILL, MIN_ITER, GRAD_FILTER,
+                       FILT_SIZE_GRAD, TIMELAPSE, RTMOD, GRAVITY, NGRAVB, NZGRAV, GRAV_TYPE, BACK_DENSITY, RTM_SHOT};
+    for (int k = 0; k < 36; k++) iv[k] = I[k];
+    const float F[12] = {EXP_TAPER_GRAD_HOR, SRTRADIUS, VPUPPERLIM, VPLOWERLIM, VSUPPERLIM, VSLOWERLIM,
+                         RHOUPPERLIM, RHOLOWERLIM, QSUPPERLIM, QSLOWERLIM, EPS_SCALE, SCALEFAC};
+    for (int k = 0; k < 12; k++) fv[k] = F[k];
+    const char *S[8] = {TFILE, INV_MODELFILE, TRKILL_FILE, PICKS_FILE, MISFIT_LOG_FILE, DATA_DIR_T0, DFILE, DATA_DIR};
+    for (int k = 0; k < 8; k++) {
+        strncpy(strs + 74 * k, S[k], 73);
+        strs[74 * k + 73] = 0;
+    }
+    return 0;
+}

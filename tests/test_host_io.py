@@ -97,6 +97,52 @@ def test_inp_reader_matches_read_par(tmp_path, name):
         assert ours.get(f) == strs[k], f
 
 
+def _ref_read_par_fwi(path):
+    lib = ctypes.CDLL(O.REF_SO)
+    iv = np.zeros(36, np.int32)
+    fv = np.zeros(12, np.float32)
+    strs = ctypes.create_string_buffer(74 * 8)
+    assert lib.refh_read_par_fwi(path.encode(), O._ip(iv), O._fp(fv), strs) == 0
+    names = [strs.raw[74 * k:74 * (k + 1)].split(b"\0")[0].decode() for k in range(8)]
+    return iv, fv, names
+
+
+FWI_INT = ["itermax", "taper", "taperlength", ("gradt", 1), ("gradt", 2), ("gradt", 3), ("gradt", 4),
+           ("testshot", 1), ("testshot", 2), ("testshot", 3), "sws_taper_grad_vert", "sws_taper_grad_hor",
+           "sws_taper_grad_sources", "sws_taper_circular_per_shot", "srtshape", "filtsize", "sws_taper_file",
+           "inv_mod_out", "grad_method", "pcg_beta", "nlbfgs", "model_filter", "filt_size", "stepmax", "trkill",
+           "min_iter", "grad_filter", "filt_size_grad", "timelapse", "rtmod", "gravity", "ngravb", "nzgrav",
+           "grav_type", "back_density", "rtm_shot"]
+FWI_FLT = ["exp_taper_grad_hor", "srtradius", "vpupperlim", "vplowerlim", "vsupperlim", "vslowerlim", "rhoupperlim",
+           "rholowerlim", "qsupperlim", "qslowerlim", "eps_scale", "scalefac"]
+FWI_STR = ["tfile", "inv_modelfile", "trkill_file", "picks_file", "misfit_log_file", "data_dir_t0", "dfile",
+           "data_dir"]
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["plain", "stray-line-shifts"])
+def test_inp_reader_inversion_lines_match_read_par(tmp_path, name):
+    """Lines 60-115 (iterations, tapers, limits, L-BFGS, step search, logs) as read_par reads them."""
+    path = str(tmp_path / "p.inp")
+    kw = dict(INP_VARIANTS[name], MODE=1, ITERMAX=7, GRADT=[3, 9, 110, 140], TESTSHOT=[2, 5, 3], SWS_TAPER_GRAD_VERT=1,
+              SWS_TAPER_GRAD_HOR=1, EXP_TAPER_GRAD_HOR=2.5, SWS_TAPER_GRAD_SOURCES=1, SWS_TAPER_CIRCULAR_PER_SHOT=1,
+              SRTSHAPE=2, SRTRADIUS=12.5, FILTSIZE=3, INV_MODELFILE="model/inv", VPUPPERLIM=5500.0, VPLOWERLIM=1400.0,
+              VSUPPERLIM=3300.0, VSLOWERLIM=0.0, RHOUPPERLIM=2800.0, RHOLOWERLIM=1000.0, NLBFGS=12, EPS_SCALE=0.02,
+              STEPMAX=6, SCALEFAC=3.0, MISFIT_LOG_FILE="L2_LOG.dat", MIN_ITER=2, DATA_DIR="su/obs")
+    inp_case.write_inp(path, **kw)
+    ours = io.read_inp(path)
+    iv, fv, strs = O.run_isolated(_ref_read_par_fwi, path)
+    for k, f in enumerate(FWI_INT):
+        got = getattr(ours, f[0])[f[1]] if isinstance(f, tuple) else ours.get(f)
+        assert got == int(iv[k]), f
+    for k, f in enumerate(FWI_FLT):
+        assert np.float32(ours.get(f)) == fv[k], f
+    for k, f in enumerate(FWI_STR):
+        assert ours.get(f) == strs[k], f
+    if name == "plain":
+        assert ours.itermax == 7 and ours.nlbfgs == 12 and ours.get("misfit_log_file") == "L2_LOG.dat"
+
+
 def test_inp_reader_known_values(tmp_path):
     """Without the reference: the positional semantics on a file this test writes."""
     path = str(tmp_path / "p.inp")
