@@ -148,11 +148,15 @@ class FWI:
     time_filter: (order, fc, fc_start) band-limiting sources and data;
     residual: calc_res options (Shot.residual_ex keywords) for gradient and
     misfit; energy: (C_vp, C_vs, C_rho) of the EPRECOND 1/3 scaling (params.eprecond
-    set); inv_iter: (INV_VP_ITER, INV_VS_ITER, INV_RHO_ITER)."""
+    set); inv_iter: (INV_VP_ITER, INV_VS_ITER, INV_RHO_ITER); test_shots: indices of
+    the shots whose misfit is the objective and whose forward runs test the step
+    lengths (TESTSHOT_START..END by INCR, grad_obj_psv.c and step_length_est_psv.c;
+    None: all shots).  Shot tuples are (src_i, src_j, signals, rec_i, rec_j) with
+    optional src_type, src_azi and the (x, z) source position in metres."""
 
     def __init__(self, params, model, shots, obs, limits, device=0, nlbfgs=20, eps_scale=0.01, scalefac=2.0,
                  stepmax=4, dist=None, precond=None, shot_taper=None, time_filter=None, residual=None, energy=None,
-                 inv_iter=(1, 1, 1)):
+                 inv_iter=(1, 1, 1), test_shots=None):
         self.p = params
         self.vp, self.vs, self.rho = [np.ascontiguousarray(a, np.float32) for a in model[:3]]
         if time_filter is not None:
@@ -166,6 +170,7 @@ class FWI:
             obs = [tuple(tdfilt(o, params.dt, order, fc, fc_start, device) for o in ob) for ob in obs]
         self.shots, self.obs, self.limits = shots, obs, limits
         self.residual, self.energy, self.inv_iter = residual, energy, tuple(inv_iter)
+        self.test_shots = None if test_shots is None else sorted(set(int(k) for k in test_shots))
         self.device, self.dist = device, dist
         self.eps_scale, self.scalefac, self.stepmax = eps_scale, scalefac, stepmax
         self.scale = np.array([self.vp.max(), self.vs.max(), self.rho.max()], np.float64)
@@ -190,7 +195,7 @@ class FWI:
 
         m = model or (self.vp, self.vs, self.rho)
         g_vp, g_vs, g_rho, L2 = sharded_gradient(self.p, m, self.shots, self.obs, self.dist, self.device,
-                                                 self.shot_taper, self.residual, self.energy)
+                                                 self.shot_taper, self.residual, self.energy, self.test_shots)
         if self.precond is not None:
             from . import api as dn
 
@@ -205,15 +210,20 @@ class FWI:
         """mode-2 forward runs of all shots on a test model; sum of the vx and vy misfits."""
         from . import api as dn
 
+        from .shard import make_shot, source_position
+
         m = dn.Model(self.p.replace(store_snapshots=0, ckpt_steps=0), *model, device=self.device)
-        ss = [dn.Shot(m, *sh[:5]) for sh in self.shots]
+        idx = range(len(self.shots)) if self.test_shots is None else self.test_shots
+        ss = [make_shot(m, self.shots[k]) for k in idx]
         dn.run(ss, _lib.MODE_OBJECTIVE)
         L2 = 0.0
-        for s, sh, (ovx, ovy) in zip(ss, self.shots, self.obs):
+        for s, k in zip(ss, idx):
+            sh, (ovx, ovy) = self.shots[k], self.obs[k]
             if self.residual is None:
                 L2 += s.residual(ovx, _lib.SEC_VX) + s.residual(ovy, _lib.SEC_VY)
             else:
-                opts = dict({"src_x": float(sh[0][0]) * self.p.dh, "src_z": float(sh[1][0]) * self.p.dh}, **self.residual)
+                sx, sz = source_position(sh, self.p.dh)
+                opts = dict({"src_x": sx, "src_z": sz}, **self.residual)
                 L2 += s.residual_ex(ovx, _lib.SEC_VX, **opts) + s.residual_ex(ovy, _lib.SEC_VY, **opts)
         for s in ss:
             s.close()
@@ -261,12 +271,13 @@ def rtm_image(params, model, shots, obs, device=0, batch=None):
     images RTM_PSV_out.c writes).  `params` must store snapshots.  Returns
     (P image, S image) in file order."""
     from . import api as dn
+    from .shard import make_shot
 
     m = dn.Model(params, *model[:3], model[3] if params.L else None, model[4] if params.L else None,
                  device=device)
     batch = batch or len(shots)
     for b0 in range(0, len(shots), batch):
-        ss = [dn.Shot(m, *sh[:5]) for sh in shots[b0:b0 + batch]]
+        ss = [make_shot(m, sh) for sh in shots[b0:b0 + batch]]
         dn.run(ss, _lib.MODE_FORWARD)
         for s, (ovx, ovy) in zip(ss, obs[b0:b0 + batch]):
             s.rtm_source(ovx, _lib.SEC_VX)

@@ -48,8 +48,23 @@ def allreduce_sum(arrays, dist=None, device=None):
     return out
 
 
+def make_shot(model, sh):
+    """A Shot from a shot tuple (src_i, src_j, signals, rec_i, rec_j[, src_type[, src_azi[, (x, z)]]])."""
+    from . import api as dn
+
+    return dn.Shot(model, *sh[:5], src_type=sh[5] if len(sh) > 5 else None, src_azi=sh[6] if len(sh) > 6 else None)
+
+
+def source_position(sh, dh):
+    """The shot's first source in metres: the table's (x, z) when the tuple carries
+    it (as the reference's srcpos), else its grid cell times DH."""
+    if len(sh) > 7 and sh[7] is not None:
+        return float(sh[7][0]), float(sh[7][1])
+    return float(sh[0][0]) * dh, float(sh[1][0]) * dh
+
+
 def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_taper=None, residual=None,
-                     energy=None):
+                     energy=None, misfit_shots=None):
     """FWI gradient of `shots` sharded over the ranks of `dist` (all ranks pass
     the same arguments).  Each rank runs its share as one batch on its GPU:
     forward with snapshots, device residuals against `obs`, adjoint, and stacks
@@ -60,7 +75,8 @@ def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_
     before stacking; residual = the calc_res options of Shot.residual_ex (LNORM,
     N_ORDER, OFFSET_MUTE, ...; None: the L2 residual); energy = (C_vp, C_vs,
     C_rho) scales each shot's gradient by its energy weights (EPRECOND 1 or 3
-    in params)."""
+    in params); misfit_shots: the indices whose misfit is summed (the reference's
+    test shots, TESTSHOT_START..END by INCR; None: all)."""
     from . import api as dn
     from ._lib import MODE_ADJOINT, MODE_FORWARD, SEC_VX, SEC_VY
 
@@ -73,21 +89,23 @@ def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_
     if mine:
         m = dn.Model(params, *model[:3], model[3] if params.L else None, model[4] if params.L else None,
                      device=device_index)
-        ss = [dn.Shot(m, *shots[k][:5]) for k in mine]
+        ss = [make_shot(m, shots[k]) for k in mine]
         dn.run(ss, MODE_FORWARD)
         for s, k in zip(ss, mine):
             if residual is None:
-                misfit += s.residual(obs[k][0], SEC_VX) + s.residual(obs[k][1], SEC_VY)
+                mk = s.residual(obs[k][0], SEC_VX) + s.residual(obs[k][1], SEC_VY)
             else:
-                src = {"src_x": float(shots[k][0][0]) * params.dh, "src_z": float(shots[k][1][0]) * params.dh}
-                opts = dict(src, **residual)
-                misfit += s.residual_ex(obs[k][0], SEC_VX, **opts) + s.residual_ex(obs[k][1], SEC_VY, **opts)
+                sx, sz = source_position(shots[k], params.dh)
+                opts = dict({"src_x": sx, "src_z": sz}, **residual)
+                mk = s.residual_ex(obs[k][0], SEC_VX, **opts) + s.residual_ex(obs[k][1], SEC_VY, **opts)
+            if misfit_shots is None or k in misfit_shots:
+                misfit += mk
         dn.run(ss, MODE_ADJOINT)
         for s, k in zip(ss, mine):
             if shot_taper is None and energy is None:
                 s.accumulate_gradient()
             else:
-                sx, sz = float(shots[k][0][0]) * params.dh, float(shots[k][1][0]) * params.dh
+                sx, sz = source_position(shots[k], params.dh)
                 s.accumulate_gradient_ex(energy=energy,
                                          circular_taper=None if shot_taper is None else tuple(shot_taper) + (sx, sz))
         g = [x.astype(np.float64) for x in m.gradient()]

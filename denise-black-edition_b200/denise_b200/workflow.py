@@ -100,7 +100,7 @@ def _check_supported(st, params):
 
 
 def stage_fwi(params, model, shots, obs, limits, st, averages, precond_base=None, shot_taper=None, device=0,
-              nlbfgs=20, eps_scale=0.01, scalefac=2.0, stepmax=4, dist=None):
+              nlbfgs=20, eps_scale=0.01, scalefac=2.0, stepmax=4, dist=None, test_shots=None):
     """An fwi.FWI configured by one workflow stage."""
     from . import fwi
     from .precond import PrecondConfig
@@ -123,7 +123,7 @@ def stage_fwi(params, model, shots, obs, limits, st, averages, precond_base=None
     return fwi.FWI(p, model, shots, obs, limits, device=device, nlbfgs=nlbfgs, eps_scale=eps_scale,
                    scalefac=scalefac, stepmax=stepmax, dist=dist, precond=precond, shot_taper=shot_taper,
                    time_filter=time_filter, residual=residual, energy=energy,
-                   inv_iter=(st["INV_VP_ITER"], st["INV_VS_ITER"], st["INV_RHO_ITER"]))
+                   inv_iter=(st["INV_VP_ITER"], st["INV_VS_ITER"], st["INV_RHO_ITER"]), test_shots=test_shots)
 
 
 def stage_files(prefix, stage):
@@ -133,22 +133,46 @@ def stage_files(prefix, stage):
 
 
 def _write_log(path, f, st, stage):
-    """The misfit log line of FWI_PSV.c (MISFIT_LOG_FILE): opteps, epst1[1..3], L2t[1..4], FC_START, FC, stage."""
+    """The misfit log line of FWI_PSV.c:734-743 (MISFIT_LOG_FILE): opteps, epst1[1..3],
+    L2t[1..4] and the stage, with FC_START and FC before the stage when TIME_FILT is set."""
     h = f.history[-1]
     eps = h["eps"] if h["found"] else 0.0
     L2t = list(h["L2t"]) + [h["misfit"]]
     epst = list(h["epst"])
+    v = (eps, epst[0], epst[1], epst[2], L2t[0], L2t[1], L2t[2], L2t[3])
     with open(path, "a") as fp:
-        fp.write("%e \t %e \t %e \t %e \t %e \t %e \t %e \t %e \t %f \t %f \t %d \n"
-                 % (eps, epst[0], epst[1], epst[2], L2t[0], L2t[1], L2t[2], L2t[3], st["FC_START"], st["FC_END"],
-                    stage))
+        if st["TIME_FILT"] == 0:
+            fp.write("%e \t %e \t %e \t %e \t %e \t %e \t %e \t %e \t %d \n" % (v + (stage,)))
+        else:
+            fp.write("%e \t %e \t %e \t %e \t %e \t %e \t %e \t %e \t %f \t %f \t %d \n"
+                     % (v + (st["FC_START"], st["FC_END"], stage)))
+
+
+def iteration_files(prefix, stage, it):
+    """The model files model_it_out_PSV.c writes after every iteration (INV_MOD_OUT 1):
+    <INV_MODELFILE>_{vp,vs,rho}_stage_<n>_it_<iter>.bin."""
+    return tuple(f"{prefix}_{name}_stage_{stage}_it_{it}.bin" for name in ("vp", "vs", "rho"))
+
+
+def _write_model(files, model):
+    for a, x in zip(model, files):
+        np.ascontiguousarray(a, np.float32).tofile(x)
 
 
 def run_workflow(params, model, shots, obs, limits, stages, itermax, min_iter=0, precond_base=None,
-                 shot_taper=None, device=0, dist=None, out_prefix=None, misfit_log=None, resume=False, **fwi_kw):
+                 shot_taper=None, device=0, dist=None, out_prefix=None, misfit_log=None, resume=False,
+                 shots_for_stage=None, inv_mod_out=None, **fwi_kw):
     """Runs the stages in order from the starting model; returns (vp, vs, rho, [StageResult]).
 
+    shots_for_stage: a function of the stage's dict returning its shots, for
+    wavelets that depend on the stage (wavelet.c integrates N_ORDER times);
+    otherwise every stage uses `shots`.
+
     out_prefix: write each stage's final model as stage_files(out_prefix, stage) (rank 0 of dist).
+    inv_mod_out: None writes every stage's final model; 0 or 1 follow FWI_PSV.c: 0 writes
+    a stage's model only when the stage ends by the abort criterion or a failed step
+    search (model_freq_out_PSV), 1 writes the model after every iteration
+    (iteration_files, model_it_out_PSV) and no stage files.
     misfit_log: append one line per iteration in the reference's misfit-log format.
     resume: start after the last stage whose three model files exist, from that model (the
     reference's restart from its last written model)."""
@@ -157,6 +181,8 @@ def run_workflow(params, model, shots, obs, limits, stages, itermax, min_iter=0,
     nx, ny = params.nx, params.ny
     rank0 = dist is None or not dist.is_initialized() or dist.get_rank() == 0
     results, first = [], 1
+    if misfit_log is not None and rank0 and not resume:
+        open(misfit_log, "w").close()   # FWI_PSV.c:586-589: opened with "w" at the first iteration
     if resume and out_prefix is not None:
         import os
 
@@ -169,7 +195,8 @@ def run_workflow(params, model, shots, obs, limits, stages, itermax, min_iter=0,
                 break
     for k in range(first, len(stages) + 1):
         st = stages[k - 1]
-        f = stage_fwi(params, (vp, vs, rho), shots, obs, limits, st, averages, precond_base, shot_taper, device,
+        sh = shots_for_stage(st) if shots_for_stage is not None else shots
+        f = stage_fwi(params, (vp, vs, rho), sh, obs, limits, st, averages, precond_base, shot_taper, device,
                       dist=dist, **fwi_kw)
         misfits, reason, it = [], "ITERMAX", 0
         try:
@@ -178,19 +205,24 @@ def run_workflow(params, model, shots, obs, limits, stages, itermax, min_iter=0,
                 if misfit_log is not None and rank0:
                     _write_log(misfit_log, f, st, k)
                 found = f.history[-1]["found"]
+                stop = None
                 if it > min_iter and it >= 3 and abs(misfits[-3] - misfits[-1]) / misfits[-3] <= st["PRO"]:
-                    reason = "PRO"
+                    stop = "PRO"
+                elif not found:
+                    stop = "step search failed"
+                if stop is not None:
+                    reason = stop
+                    if out_prefix is not None and rank0 and inv_mod_out == 0:
+                        _write_model(stage_files(out_prefix, k), (f.vp, f.vs, f.rho))
                     break
-                if not found:
-                    reason = "step search failed"
-                    break
+                if out_prefix is not None and rank0 and inv_mod_out == 1:
+                    _write_model(iteration_files(out_prefix, k, it), (f.vp, f.vs, f.rho))
         finally:
             f.lbfgs.close()
             if f.precond is not None:
                 f.precond.close()
         vp, vs, rho = f.vp, f.vs, f.rho
-        if out_prefix is not None and rank0:
-            for a, x in zip((vp, vs, rho), stage_files(out_prefix, k)):
-                np.ascontiguousarray(a, np.float32).tofile(x)
+        if out_prefix is not None and rank0 and inv_mod_out is None:
+            _write_model(stage_files(out_prefix, k), (vp, vs, rho))
         results.append(StageResult(k, it, misfits, reason))
     return vp, vs, rho, results

@@ -23,8 +23,8 @@ int main(int argc, char **argv)
     dn_inp in;
     int st = dn_inp_read(argv[1], &in);
     if (st == DN_OK && in.mode != 0) {
-        fprintf(stderr, "denise_b200: MODE=%d: the command line runs forward modelling (MODE=0); "
-                        "FWI gradients are driven through the library API\n", in.mode);
+        fprintf(stderr, "denise_b200: MODE=%d: this command runs forward modelling (MODE=0); "
+                        "FWI (MODE=1) runs as: python -m denise_b200 <par.inp> <workflow.inp>\n", in.mode);
         return 1;
     }
     if (st == DN_OK) st = dn_forward_inp(argv[1], device);
