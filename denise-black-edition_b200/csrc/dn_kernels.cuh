@@ -1337,6 +1337,13 @@ static __global__ void k_snap_store(const Inst *__restrict__ insts, const int *_
             I.Ws[w] = __fadd_rn(I.Ws[w], __fadd_rn(__fmul_rn(I.vx[o], I.vx[o]), __fmul_rn(I.vy[o], I.vy[o])));
         }
     }
+    if (I.snap_prec != DN_SNAP_F32 && I.zch <= 4) {   // the default tile height: 20 values in registers
+        if (I.snap_prec == DN_SNAP_F16)
+            snap_store_regs<DN_SNAP_F16, 4>(I, k, b, i, j0, nrow, in, red);
+        else
+            snap_store_regs<DN_SNAP_BF16, 4>(I, k, b, i, j0, nrow, in, red);
+        return;
+    }
     if (I.snap_prec != DN_SNAP_F32 && I.zch <= 8) {
         if (I.snap_prec == DN_SNAP_F16)
             snap_store_regs<DN_SNAP_F16, 8>(I, k, b, i, j0, nrow, in, red);

@@ -262,7 +262,7 @@ def _encode_tiles(x, bx, zch, prec):
 
 
 @pytest.mark.parametrize("prec", [dn.SNAP_F16, dn.SNAP_BF16], ids=["fp16", "bf16"])
-@pytest.mark.parametrize("zch", [8, 16, 5], ids=["rows8", "rows16", "rows5"])
+@pytest.mark.parametrize("zch", [4, 8, 16, 5], ids=["rows4", "rows8", "rows16", "rows5"])
 def test_half_snapshot_encoding(prec, zch):
     """Decoded FP16/BF16 snapshots equal the per-tile power-of-two encoding of
     the FP32 snapshots bit for bit, on a grid with partial tiles in x and z and
