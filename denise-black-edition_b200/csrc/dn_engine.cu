@@ -211,9 +211,14 @@ static int validate_params(const dn_params *p)
 
 static void file_to_padded(const Layout &L, const float *file, std::vector<float> &pad, long long plane_off)
 {
-    for (int i = 1; i <= L.nx; i++)
-        for (int j = 1; j <= L.ny; j++)
-            pad[plane_off + L.origin + (long long)j * L.pitch + i] = file[(size_t)(i - 1) * L.ny + (j - 1)];
+    // x-major file order to the padded [z][x] plane, in 32 x 32 blocks so that
+    // both sides of the transposition stay in cache
+    float *dst = pad.data() + plane_off + L.origin;
+    for (int i0 = 1; i0 <= L.nx; i0 += 32)
+        for (int j0 = 1; j0 <= L.ny; j0 += 32)
+            for (int i = i0; i < i0 + 32 && i <= L.nx; i++)
+                for (int j = j0; j < j0 + 32 && j <= L.ny; j++)
+                    dst[(long long)j * L.pitch + i] = file[(size_t)(i - 1) * L.ny + (j - 1)];
 }
 
 extern "C" int dn_model_footprint(const dn_params *p, size_t *bytes)

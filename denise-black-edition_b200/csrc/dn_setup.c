@@ -429,8 +429,8 @@ int dn_visc_cell_factors(const dn_params *p, const float *vp, const float *vs, c
     }
     float ws = 2.0 * DN_PI * p->fl[0];
     float sumu = dn_visc_sum(p, ws);
-    for (int j = 1; j <= ny; j++) {
-        for (int i = 1; i <= nx; i++) {
+    for (int i = 1; i <= nx; i++) {       /* cells are independent: file order, contiguous in o */
+        for (int j = 1; j <= ny; j++) {
             size_t o = (size_t)(i - 1) * ny + (j - 1);
             float tsij = 0.25 * (*hg_at(&T, j, i) + *hg_at(&T, j, i + 1) + *hg_at(&T, j + 1, i) + *hg_at(&T, j + 1, i + 1));
             float tp = dn_visc_tau_from_q(p->honor_q ? qp[o] : 30.0f);
