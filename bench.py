@@ -410,7 +410,11 @@ def run_gradient(a, device):
     pc = p.to_c()
     dn._lib.check(dn._lib.lib.dn_shot_footprint(ctypes.byref(pc), len(ri), 1, ctypes.byref(fp)))
     free, total = dn.device_memory(device)
-    batch = max(1, min(n, int(0.8 * free / fp.value) - 1))
+    # as many shots per batch as 90 % of the free HBM holds, spread evenly over the
+    # batches (32 shots: 4 x 8 rather than 4 x 7 + 4; larger batches run faster per shot)
+    most = max(1, min(n, int(0.9 * free / fp.value)))
+    nbatch = -(-n // most)
+    batch = -(-n // nbatch)
 
     def grad(params, idx):
         m = dn.Model(params, *start, device=device)
