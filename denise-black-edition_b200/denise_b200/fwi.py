@@ -212,21 +212,25 @@ class FWI:
 
         from .shard import make_shot, source_position
 
-        m = dn.Model(self.p.replace(store_snapshots=0, ckpt_steps=0), *model, device=self.device)
+        from .shard import memory_batches
+
+        p = self.p.replace(store_snapshots=0, ckpt_steps=0)
+        m = dn.Model(p, *model, device=self.device)
         idx = range(len(self.shots)) if self.test_shots is None else self.test_shots
-        ss = [make_shot(m, self.shots[k]) for k in idx]
-        dn.run(ss, _lib.MODE_OBJECTIVE)
         L2 = 0.0
-        for s, k in zip(ss, idx):
-            sh, (ovx, ovy) = self.shots[k], self.obs[k]
-            if self.residual is None:
-                L2 += s.residual(ovx, _lib.SEC_VX) + s.residual(ovy, _lib.SEC_VY)
-            else:
-                sx, sz = source_position(sh, self.p.dh)
-                opts = dict({"src_x": sx, "src_z": sz}, **self.residual)
-                L2 += s.residual_ex(ovx, _lib.SEC_VX, **opts) + s.residual_ex(ovy, _lib.SEC_VY, **opts)
-        for s in ss:
-            s.close()
+        for part in memory_batches(p, self.shots, idx, 0, self.device):
+            ss = [make_shot(m, self.shots[k]) for k in part]
+            dn.run(ss, _lib.MODE_OBJECTIVE)
+            for s, k in zip(ss, part):
+                sh, (ovx, ovy) = self.shots[k], self.obs[k]
+                if self.residual is None:
+                    L2 += s.residual(ovx, _lib.SEC_VX) + s.residual(ovy, _lib.SEC_VY)
+                else:
+                    sx, sz = source_position(sh, self.p.dh)
+                    opts = dict({"src_x": sx, "src_z": sz}, **self.residual)
+                    L2 += s.residual_ex(ovx, _lib.SEC_VX, **opts) + s.residual_ex(ovy, _lib.SEC_VY, **opts)
+            for s in ss:
+                s.close()
         m.close()
         return L2
 

@@ -63,10 +63,28 @@ def source_position(sh, dh):
     return float(sh[0][0]) * dh, float(sh[1][0]) * dh
 
 
+def memory_batches(params, shots, idx, store, device=0, share=0.9):
+    """idx split into batches that fit `share` of the device's free memory (the
+    library's cached blocks counted as free), spread evenly: 32 shots that fit
+    9 at a time run as 4 x 8."""
+    from . import api as dn
+
+    idx = list(idx)
+    if not idx:
+        return []
+    ntr = max(len(shots[k][3]) for k in idx)
+    fp = dn.shot_footprint(params, ntr, store)
+    free, _ = dn.device_memory(device)
+    most = max(1, int(share * free / max(fp, 1)))
+    nb = -(-len(idx) // most)
+    size = -(-len(idx) // nb)
+    return [idx[k:k + size] for k in range(0, len(idx), size)]
+
+
 def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_taper=None, residual=None,
                      energy=None, misfit_shots=None):
     """FWI gradient of `shots` sharded over the ranks of `dist` (all ranks pass
-    the same arguments).  Each rank runs its share as one batch on its GPU:
+    the same arguments).  Each rank runs its share in batches that fit its GPU's memory:
     forward with snapshots, device residuals against `obs`, adjoint, and stacks
     its shots' gradients in shot order; the partial gradients and misfits are
     then summed over ranks.  Returns (g_vp, g_vs, g_rho, misfit), float64, on
@@ -89,28 +107,29 @@ def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_
     if mine:
         m = dn.Model(params, *model[:3], model[3] if params.L else None, model[4] if params.L else None,
                      device=device_index)
-        ss = [make_shot(m, shots[k]) for k in mine]
-        dn.run(ss, MODE_FORWARD)
-        for s, k in zip(ss, mine):
-            if residual is None:
-                mk = s.residual(obs[k][0], SEC_VX) + s.residual(obs[k][1], SEC_VY)
-            else:
-                sx, sz = source_position(shots[k], params.dh)
-                opts = dict({"src_x": sx, "src_z": sz}, **residual)
-                mk = s.residual_ex(obs[k][0], SEC_VX, **opts) + s.residual_ex(obs[k][1], SEC_VY, **opts)
-            if misfit_shots is None or k in misfit_shots:
-                misfit += mk
-        dn.run(ss, MODE_ADJOINT)
-        for s, k in zip(ss, mine):
-            if shot_taper is None and energy is None:
-                s.accumulate_gradient()
-            else:
-                sx, sz = source_position(shots[k], params.dh)
-                s.accumulate_gradient_ex(energy=energy,
-                                         circular_taper=None if shot_taper is None else tuple(shot_taper) + (sx, sz))
+        for part in memory_batches(params, shots, mine, 1, device_index):
+            ss = [make_shot(m, shots[k]) for k in part]
+            dn.run(ss, MODE_FORWARD)
+            for s, k in zip(ss, part):
+                if residual is None:
+                    mk = s.residual(obs[k][0], SEC_VX) + s.residual(obs[k][1], SEC_VY)
+                else:
+                    sx, sz = source_position(shots[k], params.dh)
+                    opts = dict({"src_x": sx, "src_z": sz}, **residual)
+                    mk = s.residual_ex(obs[k][0], SEC_VX, **opts) + s.residual_ex(obs[k][1], SEC_VY, **opts)
+                if misfit_shots is None or k in misfit_shots:
+                    misfit += mk
+            dn.run(ss, MODE_ADJOINT)
+            for s, k in zip(ss, part):   # stacked in shot order, batch after batch
+                if shot_taper is None and energy is None:
+                    s.accumulate_gradient()
+                else:
+                    sx, sz = source_position(shots[k], params.dh)
+                    s.accumulate_gradient_ex(energy=energy, circular_taper=None if shot_taper is None
+                                             else tuple(shot_taper) + (sx, sz))
+            for s in ss:
+                s.close()
         g = [x.astype(np.float64) for x in m.gradient()]
-        for s in ss:
-            s.close()
         m.close()
     dev = None
     if dist is not None and dist.is_initialized() and dist.get_backend() == "nccl":

@@ -51,3 +51,22 @@ def test_two_ranks_match_one(tmp_path):
     for k in range(3):
         assert O.rel_l2(a[k * n:(k + 1) * n], one[k].ravel()) < 1e-6
     assert abs(a[-1] - one[3]) <= 1e-12 * abs(one[3])
+
+
+def test_memory_batches_give_the_same_gradient(monkeypatch):
+    """A rank's shots run in batches that fit the device; forced batches of one and
+    of two shots stack the same gradient bit for bit (shot order is kept) and give
+    the same misfit as one batch."""
+    from denise_b200 import shard
+
+    p, model, shots, obs = _case()
+    one = sharded_gradient(p, model, shots, obs, None, 0)
+    assert len(shard.memory_batches(p, shots, range(len(shots)), 1, 0)) == 1   # small case: one batch
+    for size in (1, 2):
+        monkeypatch.setattr(shard, "memory_batches",
+                            lambda params, sh, idx, store, device=0, share=0.9, size=size:
+                            [list(idx)[k:k + size] for k in range(0, len(list(idx)), size)])
+        got = sharded_gradient(p, model, shots, obs, None, 0)
+        for a, b in zip(got[:3], one[:3]):
+            np.testing.assert_array_equal(a, b)
+        assert got[3] == one[3]
