@@ -38,3 +38,20 @@ def test_params_and_unsupported_switches(tmp_path, monkeypatch):
 def test_model_file_names():
     assert workflow.stage_files("m/inv", 2) == ("m/inv_vp_stage_2.bin", "m/inv_vs_stage_2.bin", "m/inv_rho_stage_2.bin")
     assert workflow.iteration_files("m/inv", 1, 3)[0] == "m/inv_vp_stage_1_it_3.bin"
+
+
+def test_memory_batches_spread_evenly(monkeypatch):
+    """Batches hold at most the shots that fit 90 % of the free memory and are
+    spread evenly; every shot appears once, in order."""
+    from denise_b200 import api, shard
+
+    shots = [(None, None, None, np.zeros(40, np.int32), None)] * 32
+    monkeypatch.setattr(api, "shot_footprint", lambda p, ntr, store: 18 << 30)
+    for free_gb, want in ((178, [8] * 4), (90, [4] * 8), (10, [1] * 32), (1000, [32])):
+        monkeypatch.setattr(api, "device_memory", lambda device=0, f=free_gb: (f << 30, 183 << 30))
+        parts = shard.memory_batches(None, shots, range(32), 1, 0)
+        assert [len(b) for b in parts] == want, free_gb
+        assert sum(parts, []) == list(range(32))
+    monkeypatch.setattr(api, "device_memory", lambda device=0: (178 << 30, 183 << 30))
+    assert [len(b) for b in shard.memory_batches(None, shots, range(30), 1, 0)] == [8, 8, 8, 6]
+    assert shard.memory_batches(None, shots, [], 1, 0) == []
