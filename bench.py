@@ -61,15 +61,29 @@ def parse():
 # ---------------------------------------------------------------------------
 # reference CPU path (oracle/_ref: the reference's own code, or the C port)
 # ---------------------------------------------------------------------------
+def _modelgen():
+    """denise_b200/modelgen.py loaded by file path: the workload's numpy model and
+    acquisition generators without importing the package (which loads the CUDA
+    library), so the reference arm runs nothing but the reference's own code."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("dn_modelgen", os.path.join(PKG, "denise_b200", "modelgen.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def _cpu_worker(args):
     """One process: one shot of the workload for `nt_sample` steps on the reference's code."""
     kind, k, nx, ny, nt_sample, seed = args
     import oracles as O
-    from denise_b200 import synth
 
-    p = synth.c1_params(nx=nx, ny=ny, nt=nt_sample)
-    model, src, rec = synth.c1_shot(p, k, seed=seed)
-    src = src + (np.ones(1, np.int32), np.zeros(1, np.float32))
+    mg = _modelgen()
+    p = mg.c1_reference_params(nx=nx, ny=ny, nt=nt_sample)
+    model = mg.base_model(nx, ny, p.dh, seed) + mg.q_model(nx, ny, seed)
+    (si, sj), rec = mg.c1_acquisition(nx, ny, p.dh, k % 64)
+    sig = mg.ricker(nt_sample, p.dt, 8.0)[None, :]
+    src = (si, sj, sig, np.ones(1, np.int32), np.zeros(1, np.float32))
     if kind == "reference":
         r = O.Reference(p, model, src, rec, mode_global=0)
         t0 = time.perf_counter()
@@ -493,7 +507,7 @@ def run_fwi_large(a, device):
     L2 = f.iterate(1)
     h = f.history[-1]
     L2_new = f.misfit((f.vp, f.vs, f.rho))
-    f.lbfgs.close()
+    f.close()
     t3 = time.perf_counter()
     cells = p.nx * p.ny * p.nt
     per_shot_grad = h["gradient_s"] / n
@@ -505,7 +519,7 @@ def run_fwi_large(a, device):
             "forward_device_s_per_shot": round(per_shot_fwd, 2),
             "forward_mcell_updates_per_s": round(cells / per_shot_fwd / 1e6, 1),
             "gradient_s": round(h["gradient_s"], 1), "gradient_s_per_shot": round(per_shot_grad, 2),
-            "lbfgs_s": round(h["lbfgs_s"], 3), "step_search_s": round(h["step_search_s"], 1),
+            "optimizer_s": round(h["optimizer_s"], 3), "step_search_s": round(h["step_search_s"], 1),
             "test_models": h["test_models"], "step_found": h["found"], "eps": h["eps"],
             "misfit_before": L2, "misfit_after": L2_new,
             "iteration_s": round(t3 - t2, 1),
@@ -579,11 +593,9 @@ def run_e2e(p, inputs, device, cells_step):
 
 
 def run_reference(a, rank, world):
-    from denise_b200 import synth
-
     if rank != 0:
         return None
-    p = synth.c1_params(nx=a.nx, ny=a.ny, nt=a.nt)
+    p = _modelgen().c1_reference_params(nx=a.nx, ny=a.ny, nt=a.nt)
     for _ in range(a.warmup):
         cpu_sample(p.nx, p.ny, max(2, a.cpu_sample_nt // 6))
     rates, secs = [], []

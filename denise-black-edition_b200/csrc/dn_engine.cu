@@ -1922,6 +1922,46 @@ extern "C" int dn_model_set_gradient(dn_model *m, const float *g_vp, const float
     return DN_OK;
 }
 
+// the stacked gradient as doubles on the device (for a collective sum over ranks) and back
+static __global__ void k_grad_export(const void *__restrict__ g, int g64, double *__restrict__ out, long long n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride)
+        out[e] = g64 ? ((const double *)g)[e] : (double)((const float *)g)[e];
+}
+static __global__ void k_grad_import(void *__restrict__ g, int g64, const double *__restrict__ in, long long n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+        if (g64)
+            ((double *)g)[e] = in[e];
+        else
+            ((float *)g)[e] = __double2float_rn(in[e]);
+    }
+}
+
+extern "C" int dn_model_gradient_to_device(const dn_model *m, double *d_out)
+{
+    if (!m || !d_out) return dn_fail(DN_EINVAL, "dn_model_gradient_to_device: null argument");
+    CU(cudaSetDevice(m->device));
+    CU(cudaDeviceSynchronize());
+    k_grad_export<<<148 * 4, 256>>>(m->dgrad, m->grad64, d_out, 3LL * m->p.nx * m->p.ny);
+    CU(cudaGetLastError());
+    CU(cudaDeviceSynchronize());
+    return DN_OK;
+}
+
+extern "C" int dn_model_gradient_from_device(dn_model *m, const double *d_in)
+{
+    if (!m || !d_in) return dn_fail(DN_EINVAL, "dn_model_gradient_from_device: null argument");
+    CU(cudaSetDevice(m->device));
+    CU(cudaDeviceSynchronize());
+    k_grad_import<<<148 * 4, 256>>>(m->dgrad, m->grad64, d_in, 3LL * m->p.nx * m->p.ny);
+    CU(cudaGetLastError());
+    CU(cudaDeviceSynchronize());
+    return DN_OK;
+}
+
 extern "C" int dn_model_view_get(dn_model *m, dn_model_view *v)
 {
     if (!m || !v) return dn_fail(DN_EINVAL, "null argument");
@@ -1932,6 +1972,8 @@ extern "C" int dn_model_view_get(dn_model *m, dn_model_view *v)
     v->grad64 = m->grad64;
     v->dgrad = m->dgrad;
     v->vs = m->field(MF_VS);
+    v->vp = m->field(MF_VP);
+    v->rho = m->field(MF_RHO);
     return DN_OK;
 }
 

@@ -18,12 +18,13 @@ int dn_visc_cell_factors(const dn_params *p, const float *vp, const float *vs, c
                          const float *qs, float *muipjp, float *tausipjp, float *mu, float *taus, float *pi,
                          float *taup);
 
-/* Device view of a model's stacked gradient and S-velocity for the
- * gradient conditioning (dn_precond.cu). */
+/* Device view of a model's stacked gradient and raw model planes for the
+ * gradient conditioning (dn_precond.cu) and the optimisers (dn_fwi.cu). */
 typedef struct {
     int nx, ny, pitch, device, grad64;
     void *dgrad;            /* 3 x nx*ny, row-major [j][i] */
-    const float *vs;        /* origin pointer: element (j, i) at vs[j * pitch + i] */
+    const float *vs;        /* origin pointers: element (j, i) at vs[j * pitch + i] */
+    const float *vp, *rho;
 } dn_model_view;
 int dn_model_view_get(dn_model *m, dn_model_view *v);
 

@@ -197,6 +197,13 @@ SIGNATURES = {
     "dn_lbfgs_push": (ctypes.c_int, [_vp, _vp, _vp]),
     "dn_lbfgs_count": (ctypes.c_int, [_vp, _c_int_p]),
     "dn_lbfgs_direction": (ctypes.c_int, [_vp, _vp, _vp]),
+    "dn_optim_create": (ctypes.c_int, [ctypes.c_int] * 6 + [_P(_vp)]),
+    "dn_optim_destroy": (ctypes.c_int, [_vp]),
+    "dn_optim_reset": (ctypes.c_int, [_vp]),
+    "dn_optim_step": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_float_p]),
+    "dn_optim_get": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p]),
+    "dn_model_gradient_to_device": (ctypes.c_int, [_vp, _vp]),
+    "dn_model_gradient_from_device": (ctypes.c_int, [_vp, _vp]),
     "dn_calc_opt_step": (ctypes.c_int, [_c_double_p, _c_float_p, _c_float_p]),
     "dn_mat_update": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [_c_float_p] * 6 + [ctypes.c_float, _c_float_p,
                                      ctypes.c_int, _c_int_p, ctypes.c_float] + [_c_float_p] * 4),

@@ -1,16 +1,16 @@
-"""FWI outer loop: L-BFGS direction (FP64, on the device), the parabolic
-step-length search of step_length_est_psv.c with calc_opt_step.c, and the
-bounded model update of calc_mat_change_test_PSV.c.
+"""FWI outer loop of FWI_PSV.c: the gradient on the device (sharded over
+ranks), the reference's optimisers (L-BFGS of store_LBFGS_PSV.c / LBFGS.c /
+extract_LBFGS_PSV.c and PCG of PCG.c on the device, float vectors with FP64
+dot products), the parabolic step-length search of step_length_est_psv.c with
+calc_opt_step.c, and the bounded model update of calc_mat_change_test_PSV.c.
 
-One iteration (FWI_PSV.c): gradient and misfit of the current model over all
-shots (batched, or sharded over ranks), search direction r = H g from the
-L-BFGS history, test models x - eps r for a bracketing sequence of eps whose
-misfits (forward runs, mode 2) fix a parabola, the model moved by its minimum.
+One iteration: gradient and misfit of the current model over all shots,
+conditioning, the search direction of the optimiser, test models m - eps d for
+a bracketing sequence of eps whose misfits (forward runs, mode 2) fix a
+parabola, the model moved by its minimum.
 
-The reference applies L-BFGS to its gradients after its normalisation steps
-(store_LBFGS_PSV.c); here the model vector is [vp; vs; rho] divided per class
-by the class maximum of the starting model, so the three classes are of the
-same order, and the direction is scaled back before the update.
+LBFGS (dn_lbfgs_*) is a general FP64 L-BFGS on device vectors; the FWI
+iteration uses Optimizer, the reference's own scheme.
 """
 import ctypes
 
@@ -49,17 +49,19 @@ def step_length(objective, L2_0, eps_scale=0.01, scalefac=2.0, stepmax=4):
     with L2(eps_3) > L2(eps_2) (or give up after stepmax tries), and return the
     parabola's minimum.  objective(eps) -> misfit of the test model.  Returns
     (eps, L2t, epst, found) with 0-based arrays (index 0 = the current model)."""
+    f32 = np.float32
+    eps_scale, scalefac = f32(eps_scale), f32(scalefac)     # float in step_length_est_psv.c
     L2t = [float(L2_0), 0.0, 0.0]
-    epst = [0.0, 0.0, 0.0]
+    epst = [f32(0.0), f32(0.0), f32(0.0)]
     step1 = step2 = 0
     countstep = 0
     itests = iteste = 1
     found = True
     while step2 != 1 or step1 != 1:
         for itest in range(itests, iteste + 1):
-            L2t[itest] = float(objective(eps_scale))
+            L2t[itest] = float(objective(float(eps_scale)))
             epst[itest] = eps_scale
-            epst[0] = 0.0
+            epst[0] = f32(0.0)
         if step1 == 0 and L2t[0] <= L2t[1]:
             eps_scale = eps_scale / scalefac
             countstep += 1
@@ -82,8 +84,8 @@ def step_length(objective, L2_0, eps_scale=0.01, scalefac=2.0, stepmax=4):
         if step1 == 1 and countstep > stepmax:
             step2 = 1          # no third step bracketing the minimum
     if step1 == 1:
-        eps_scale = calc_opt_step(L2t, epst)
-    return eps_scale, L2t, epst, found
+        eps_scale = f32(calc_opt_step(L2t, epst))
+    return float(eps_scale), L2t, [float(x) for x in epst], found
 
 
 class LBFGS:
@@ -139,24 +141,105 @@ def dot(a, b):
     return out.value
 
 
+class Optimizer:
+    """The reference's optimiser on the device (dn_optim_*): GRAD_METHOD 2,
+    L-BFGS with NLBFGS pairs, or 1, PCG with PCG_BETA (FWI_PSV.c:637-676).
+    step() replaces a Model's stacked gradient by the search direction; the
+    history persists across iterations and stages until reset() (FWI_PSV.c
+    zeroes it only when a stage ends by its abort criterion)."""
+
+    FILES = ("p", "p_u", "p_rho", "p_vp", "p_vs", "p_mrho", "c", "c_u", "c_rho")
+
+    def __init__(self, grad_method, nx, ny, nlbfgs=20, pcg_beta=2, device=0):
+        self.grad_method, self.nx, self.ny, self.device = int(grad_method), nx, ny, device
+        self.h = None
+        if self.grad_method in (1, 2):
+            self.h = ctypes.c_void_p()
+            check(lib.dn_optim_create(self.grad_method, int(nx), int(ny), int(nlbfgs), int(pcg_beta), int(device),
+                                      ctypes.byref(self.h)))
+
+    def step(self, model, it, c):
+        """Any other GRAD_METHOD leaves the conditioned gradient as the direction, as FWI_PSV.c does."""
+        if self.h is None:
+            return
+        cc = (ctypes.c_float * 3)(*[float(x) for x in c])
+        check(lib.dn_optim_step(self.h, model.handle, int(it), cc))
+
+    def reset(self):
+        if self.h is not None:
+            check(lib.dn_optim_reset(self.h))
+
+    def vector(self, which):
+        """The JACOBIAN vector `which` (0-8, FILES order) after an L-BFGS step, [nx][ny] float32."""
+        out = np.empty((self.nx, self.ny), np.float32)
+        check(lib.dn_optim_get(self.h, int(which), _lib.fptr(out)))
+        return out
+
+    def write_jacobian(self, prefix):
+        """The files extract_LBFGS_PSV.c:80-248 writes after an L-BFGS step:
+        <JACOBIAN>_{p,p_u,p_rho}.old (normalised gradients), _{p_vp,p_vs,p_mrho}.old
+        (the model), _{c,c_u,c_rho}.old (the direction), each also as the one-rank
+        part file <name>.0.0 that mergemod merges (identical on one rank)."""
+        if self.grad_method != 2:
+            return
+        for k, name in enumerate(self.FILES):
+            a = self.vector(k)
+            for path in (f"{prefix}_{name}.old.0.0", f"{prefix}_{name}.old"):
+                a.tofile(path)
+
+    def close(self):
+        if self.h:
+            lib.dn_optim_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def write_inv_model(prefix, model):
+    """The files calc_mat_change_test_PSV.c:223-243 writes with every model
+    update: <INV_MODELFILE>_{vp,vs,rho}.bin and their one-rank part files .0.0."""
+    for name, a in zip(("vp", "vs", "rho"), model):
+        a = np.ascontiguousarray(a, np.float32)
+        for path in (f"{prefix}_{name}.bin.0.0", f"{prefix}_{name}.bin"):
+            a.tofile(path)
+
+
 class FWI:
-    """FWI iterations for one grid: shots (src_i, src_j, signals, rec_i, rec_j)
-    with observed data obs[k] = (vx, vy) [ntr][nt]; `params` must store
-    snapshots.  limits: (vp_lo, vp_hi, vs_lo, vs_hi, rho_lo, rho_hi).
-    precond: a precond.PrecondConfig applied to every stacked gradient;
-    shot_taper: (srtshape, srtradius, filtsize) of the per-shot circular taper;
-    time_filter: (order, fc, fc_start) band-limiting sources and data;
-    residual: calc_res options (Shot.residual_ex keywords) for gradient and
-    misfit; energy: (C_vp, C_vs, C_rho) of the EPRECOND 1/3 scaling (params.eprecond
-    set); inv_iter: (INV_VP_ITER, INV_VS_ITER, INV_RHO_ITER); test_shots: indices of
-    the shots whose misfit is the objective and whose forward runs test the step
-    lengths (TESTSHOT_START..END by INCR, grad_obj_psv.c and step_length_est_psv.c;
-    None: all shots).  Shot tuples are (src_i, src_j, signals, rec_i, rec_j) with
-    optional src_type, src_azi and the (x, z) source position in metres."""
+    """FWI iterations of FWI_PSV.c for one grid: shots (src_i, src_j, signals,
+    rec_i, rec_j) with observed data obs[k] = (vx, vy) [ntr][nt]; `params` must
+    store snapshots.  limits: (vp_lo, vp_hi, vs_lo, vs_hi, rho_lo, rho_hi).
+
+    One iteration: the gradient of all shots (batched, sharded over the ranks of
+    `dist`, summed on the device), its conditioning (precond: smooth_grad and
+    precond_PSV), the reference's optimiser (grad_method 2 L-BFGS with nlbfgs
+    pairs, 1 PCG with pcg_beta; the gradients normalised by `averages` = C_vp,
+    C_vs, C_rho, the starting model's averages), the parabolic step search of
+    step_length_est_psv.c with mode-2 forward runs of the test shots (sharded
+    the same way), and the bounded update of calc_mat_change_test_PSV.c.
+
+    precond: a precond.PrecondConfig; shot_taper: (srtshape, srtradius,
+    filtsize) of the per-shot circular taper; time_filter: (order, fc,
+    fc_start) band-limiting sources and data; residual: calc_res options
+    (Shot.residual_ex keywords) for gradient and misfit; energy: (C_vp, C_vs,
+    C_rho) of the EPRECOND 1/3 scaling (params.eprecond set); inv_iter:
+    (INV_VP_ITER, INV_VS_ITER, INV_RHO_ITER); scalerho: SCALERHO; test_shots:
+    indices of the shots whose misfit is the objective and whose forward runs
+    test the step lengths (TESTSHOT_START..END by INCR; None: all shots);
+    optimizer: an Optimizer to continue (the workflow keeps one across stages)
+    or None for a new one; jacobian: the JACOBIAN prefix of the files
+    extract_LBFGS_PSV writes (None: none); inv_modelfile: the INV_MODELFILE
+    prefix of the files every update writes (None: none).  Shot tuples are
+    (src_i, src_j, signals, rec_i, rec_j) with optional src_type, src_azi and
+    the (x, z) source position in metres."""
 
     def __init__(self, params, model, shots, obs, limits, device=0, nlbfgs=20, eps_scale=0.01, scalefac=2.0,
                  stepmax=4, dist=None, precond=None, shot_taper=None, time_filter=None, residual=None, energy=None,
-                 inv_iter=(1, 1, 1), test_shots=None):
+                 inv_iter=(1, 1, 1), test_shots=None, grad_method=2, pcg_beta=2, averages=None, optimizer=None,
+                 jacobian=None, inv_modelfile=None, scalerho=1.0):
         self.p = params
         self.vp, self.vs, self.rho = [np.ascontiguousarray(a, np.float32) for a in model[:3]]
         if time_filter is not None:
@@ -169,13 +252,19 @@ class FWI:
                      for sh in shots]
             obs = [tuple(tdfilt(o, params.dt, order, fc, fc_start, device) for o in ob) for ob in obs]
         self.shots, self.obs, self.limits = shots, obs, limits
-        self.residual, self.energy, self.inv_iter = residual, energy, tuple(inv_iter)
+        self.residual, self.energy, self.inv_iter, self.scalerho = residual, energy, tuple(inv_iter), scalerho
         self.test_shots = None if test_shots is None else sorted(set(int(k) for k in test_shots))
         self.device, self.dist = device, dist
         self.eps_scale, self.scalefac, self.stepmax = eps_scale, scalefac, stepmax
-        self.scale = np.array([self.vp.max(), self.vs.max(), self.rho.max()], np.float64)
-        n = 3 * params.nx * params.ny
-        self.lbfgs = LBFGS(n, nlbfgs, device)
+        if averages is None:
+            from .workflow import model_averages
+
+            averages = model_averages(self.vp, self.vs, self.rho)
+        self.averages = tuple(float(x) for x in averages)
+        self.own_optimizer = optimizer is None
+        self.optimizer = optimizer or Optimizer(grad_method, params.nx, params.ny, nlbfgs, pcg_beta, device)
+        self.jacobian, self.inv_modelfile = jacobian, inv_modelfile
+        self.rank0 = dist is None or not dist.is_initialized() or dist.get_rank() == 0
         # gradient conditioning after stacking (FWI_PSV.c:628-634) and per shot
         self.shot_taper = shot_taper
         self.precond = None
@@ -183,89 +272,80 @@ class FWI:
             from .precond import PrecondPlan
 
             self.precond = PrecondPlan(params.nx, params.ny, params.dh, precond, device)
-        self.prev = None          # (x, g) of the previous iteration, scaled
         self.history = []
 
-    def _x(self):
-        return np.concatenate([(a.astype(np.float64) / s).ravel() for a, s in zip((self.vp, self.vs, self.rho),
-                                                                                   self.scale)])
-
-    def gradient(self, model=None):
-        from .shard import sharded_gradient
+    def _gradient_model(self, model=None):
+        from .shard import gradient_model
 
         m = model or (self.vp, self.vs, self.rho)
-        g_vp, g_vs, g_rho, L2 = sharded_gradient(self.p, m, self.shots, self.obs, self.dist, self.device,
-                                                 self.shot_taper, self.residual, self.energy, self.test_shots)
+        gm, L2 = gradient_model(self.p, m, self.shots, self.obs, self.dist, self.device, self.shot_taper,
+                                self.residual, self.energy, self.test_shots)
         if self.precond is not None:
-            from . import api as dn
+            self.precond.apply(gm)
+        return gm, L2
 
-            dm = dn.Model(self.p.replace(store_snapshots=0, ckpt_steps=0, L=0, fl=()), *m[:3], device=self.device)
-            dm.set_gradient(g_vp.astype(np.float32), g_vs.astype(np.float32), g_rho.astype(np.float32))
-            self.precond.apply(dm)
-            g_vp, g_vs, g_rho = [x.astype(np.float64) for x in dm.gradient()]
-            dm.close()
-        return g_vp, g_vs, g_rho, L2
+    def gradient(self, model=None):
+        """The stacked, conditioned gradient and the misfit: (g_vp, g_vs, g_rho, L2) on the host."""
+        gm, L2 = self._gradient_model(model)
+        try:
+            g = [x.astype(np.float64) for x in gm.gradient()]
+        finally:
+            gm.close()
+        return g[0], g[1], g[2], L2
 
     def misfit(self, model):
-        """mode-2 forward runs of all shots on a test model; sum of the vx and vy misfits."""
-        from . import api as dn
+        """obj_psv: the misfit of the test shots on a test model (mode-2 forward runs, sharded)."""
+        from .shard import sharded_misfit
 
-        from .shard import make_shot, source_position
-
-        from .shard import memory_batches
-
-        p = self.p.replace(store_snapshots=0, ckpt_steps=0)
-        m = dn.Model(p, *model, device=self.device)
         idx = range(len(self.shots)) if self.test_shots is None else self.test_shots
-        L2 = 0.0
-        for part in memory_batches(p, self.shots, idx, 0, self.device):
-            ss = [make_shot(m, self.shots[k]) for k in part]
-            dn.run(ss, _lib.MODE_OBJECTIVE)
-            for s, k in zip(ss, part):
-                sh, (ovx, ovy) = self.shots[k], self.obs[k]
-                if self.residual is None:
-                    L2 += s.residual(ovx, _lib.SEC_VX) + s.residual(ovy, _lib.SEC_VY)
-                else:
-                    sx, sz = source_position(sh, self.p.dh)
-                    opts = dict({"src_x": sx, "src_z": sz}, **self.residual)
-                    L2 += s.residual_ex(ovx, _lib.SEC_VX, **opts) + s.residual_ex(ovy, _lib.SEC_VY, **opts)
-            for s in ss:
-                s.close()
-        m.close()
-        return L2
+        return sharded_misfit(self.p, model, self.shots, self.obs, idx, self.dist, self.device, self.residual)
 
-    def iterate(self, it):
+    def iterate(self, it, min_iter=0):
+        """Iteration `it` (FWI_PSV.c's per-stage counter) of a stage with MIN_ITER
+        min_iter.  Returns the misfit of the current model (L2t[4])."""
         import time
 
         t0 = time.perf_counter()
-        g_vp, g_vs, g_rho, L2 = self.gradient()
-        t1 = time.perf_counter()
-        nx, ny = self.p.nx, self.p.ny
-        # gradient with respect to the scaled model x = m / scale
-        g = np.concatenate([(gc * s).ravel() for gc, s in zip((g_vp, g_vs, g_rho), self.scale)])
-        x = self._x()
-        if self.prev is not None:
-            self.lbfgs.push(x - self.prev[0], g - self.prev[1])
-        self.prev = (x, g)
-        r = self.lbfgs.direction(g)
-        d = [(r[k * nx * ny:(k + 1) * nx * ny] / self.scale[k]).reshape(nx, ny).astype(np.float32) for k in range(3)]
+        gm, L2 = self._gradient_model()
+        try:
+            t1 = time.perf_counter()
+            self.optimizer.step(gm, it, self.averages)
+            if self.jacobian is not None and self.rank0:
+                self.optimizer.write_jacobian(self.jacobian)
+            d = gm.gradient()
+        finally:
+            gm.close()
         t2 = time.perf_counter()
         ntests = [0]
 
         def objective(eps):
             ntests[0] += 1
-            vp, vs, rho, _ = mat_update(self.vp, self.vs, self.rho, *d, eps, self.limits, it, self.inv_iter)
+            vp, vs, rho, _ = mat_update(self.vp, self.vs, self.rho, *d, eps, self.limits, it, self.inv_iter,
+                                        self.scalerho)
             return self.misfit((vp, vs, rho))
 
         eps, L2t, epst, found = step_length(objective, L2, self.eps_scale, self.scalefac, self.stepmax)
-        if found:
-            self.vp, self.vs, self.rho, _ = mat_update(self.vp, self.vs, self.rho, *d, eps, self.limits, it,
-                                                       self.inv_iter)
+        # FWI_PSV.c:686-694: no update after a failed search once MIN_ITER iterations are done;
+        # before that the smallest step tried is taken
+        if it > min_iter and not found:
+            eps = 0.0
+        self.vp, self.vs, self.rho, _ = mat_update(self.vp, self.vs, self.rho, *d, eps, self.limits, it,
+                                                   self.inv_iter, self.scalerho)
+        if self.inv_modelfile is not None and self.rank0:
+            write_inv_model(self.inv_modelfile, (self.vp, self.vs, self.rho))
         t3 = time.perf_counter()
         self.history.append({"iteration": it, "misfit": L2, "eps": eps, "L2t": L2t, "epst": epst, "found": found,
-                             "gradient_s": t1 - t0, "lbfgs_s": t2 - t1, "step_search_s": t3 - t2,
+                             "gradient_s": t1 - t0, "optimizer_s": t2 - t1, "step_search_s": t3 - t2,
                              "test_models": ntests[0]})
         return L2
+
+    def close(self):
+        if self.own_optimizer and self.optimizer is not None:
+            self.optimizer.close()
+        self.optimizer = None
+        if self.precond is not None:
+            self.precond.close()
+            self.precond = None
 
 
 def rtm_image(params, model, shots, obs, device=0, batch=None):

@@ -17,16 +17,21 @@ MODE 1 is the FWI of FWI_PSV.c for the P-SV path:
 * gradient conditioning from SWS_TAPER_GRAD_VERT / _HOR / _SOURCES, GRADT1-4,
   EXP_TAPER_GRAD_HOR, the per-shot circular taper (SWS_TAPER_CIRCULAR_PER_SHOT,
   SRTSHAPE, SRTRADIUS, FILTSIZE) and the stage's SPATFILTER;
-* model bounds VP/VS/RHO UPPER/LOWERLIM, L-BFGS with NLBFGS pairs (GRAD_METHOD 2),
-  step search EPS_SCALE / STEPMAX / SCALEFAC, ITERMAX and MIN_ITER per stage;
-* outputs as FWI_PSV.c writes them: with INV_MOD_OUT 0 the model of a stage
+* model bounds VP/VS/RHO UPPER/LOWERLIM, the reference's optimisers (GRAD_METHOD
+  2: L-BFGS with NLBFGS pairs; 1: PCG with PCG_BETA) on gradients normalised by
+  the starting model's averages, step search EPS_SCALE / STEPMAX / SCALEFAC,
+  ITERMAX and MIN_ITER per stage;
+* outputs as FWI_PSV.c writes them: the model after every update,
+  INV_MODELFILE_{vp,vs,rho}.bin (calc_mat_change_test_PSV.c); after every
+  L-BFGS step the JACOBIAN files <JACOBIAN>_{p,p_u,p_rho,p_vp,p_vs,p_mrho,c,
+  c_u,c_rho}.old (extract_LBFGS_PSV.c); with INV_MOD_OUT 0 the model of a stage
   that ends by the abort criterion or a failed step search,
   INV_MODELFILE_{vp,vs,rho}_stage_<n>.bin (model_freq_out_PSV.c); with
   INV_MOD_OUT 1 the model after every iteration,
   INV_MODELFILE_{vp,vs,rho}_stage_<n>_it_<iter>.bin (model_it_out_PSV.c); and
   the MISFIT_LOG_FILE lines.
 
-Switches the GPU path does not provide raise NotImplementedError (PCG,
+Switches the GPU path does not provide raise NotImplementedError (
 SWS_TAPER_FILE, TRKILL, TIMELAPSE, gravity, and the workflow options listed in
 workflow.py).  Run as ``python -m denise_b200 <par.inp> [<workflow.inp>] [device]``.
 """
@@ -56,8 +61,6 @@ def _check_supported(inp):
         raise NotImplementedError(f"PHYSICS={inp.physics}: only 2-D P-SV (1) is built")
     if inp.readmod != 1 or inp.srcrec != 1 or inp.readrec != 1:
         raise NotImplementedError("READMOD, SRCREC and READREC must be 1 (model, source and receiver files)")
-    if inp.grad_method not in (0, 2):
-        raise NotImplementedError("PCG (GRAD_METHOD 1) is not provided: L-BFGS (GRAD_METHOD 2)")
     for key, what in (("sws_taper_file", "SWS_TAPER_FILE"), ("trkill", "TRKILL"), ("timelapse", "TIMELAPSE"),
                       ("gravity", "GRAVITY")):
         if inp.get(key):
@@ -155,7 +158,7 @@ def fwi_inp(par_path, workflow_path, device=0, snap_precision=_lib.SNAP_F32, dis
     shot_taper = (inp.srtshape, inp.srtradius, inp.filtsize) if inp.sws_taper_circular_per_shot else None
     out_prefix = inp.get("inv_modelfile") or None
     misfit_log = inp.get("misfit_log_file") or None
-    for path in (out_prefix, misfit_log):
+    for path in (out_prefix, misfit_log, inp.get("jacobian") or None):
         d = os.path.dirname(path) if path else ""
         if d:
             os.makedirs(d, exist_ok=True)
@@ -163,8 +166,9 @@ def fwi_inp(par_path, workflow_path, device=0, snap_precision=_lib.SNAP_F32, dis
                         precond_base=precond_base(inp, acq), shot_taper=shot_taper, device=device, dist=dist,
                         out_prefix=out_prefix, misfit_log=misfit_log, resume=resume, inv_mod_out=inp.inv_mod_out,
                         shots_for_stage=lambda st: [acq.shot(k, st["N_ORDER"]) for k in range(acq.nshots)],
-                        nlbfgs=inp.nlbfgs or 20, eps_scale=inp.eps_scale, scalefac=inp.scalefac, stepmax=inp.stepmax,
-                        test_shots=acq.test_shots())
+                        grad_method=inp.grad_method, nlbfgs=inp.nlbfgs or 20, pcg_beta=inp.pcg_beta or 2,
+                        jacobian=inp.get("jacobian") or None, eps_scale=inp.eps_scale, scalefac=inp.scalefac,
+                        stepmax=inp.stepmax, test_shots=acq.test_shots())
 
 
 def main(argv=None):

@@ -27,6 +27,12 @@ def assign_shots(costs, world):
     return [sorted(x) for x in out]
 
 
+def _world(dist):
+    if dist is None or not dist.is_initialized():
+        return 0, 1
+    return dist.get_rank(), dist.get_world_size()
+
+
 def allreduce_sum(arrays, dist=None, device=None):
     """Sums float arrays over all ranks (in float64) and returns them on the host.
     dist: torch.distributed (initialised) or None for a single process."""
@@ -48,6 +54,40 @@ def allreduce_sum(arrays, dist=None, device=None):
     return out
 
 
+def allreduce_scalar(x, dist=None, device=None):
+    """The sum of a float over all ranks (float64)."""
+    return float(allreduce_sum([np.array([x])], dist, device)[0][0])
+
+
+def allreduce_model_gradient(model, dist=None):
+    """Sums a model's stacked gradients over the ranks of `dist` in place, in
+    float64 on the device: the gradients are exported into a device tensor
+    (dn_model_gradient_to_device), all-reduced (NCCL on the device; gloo through
+    a host copy of that tensor) and imported back.  This replaces the
+    reference's element-wise MPI_Allreduce of the stacked gradient
+    (src/PSV/grad_obj_psv.c:371-390).  A single process does nothing."""
+    rank, world = _world(dist)
+    if world == 1:
+        return
+    import torch
+
+    from ._lib import check, lib
+
+    p = model.params
+    dev = torch.device(f"cuda:{model.device}")
+    t = torch.empty(3 * p.nx * p.ny, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    check(lib.dn_model_gradient_to_device(model.handle, t.data_ptr()))
+    if dist.get_backend() == "nccl":
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    else:
+        h = t.cpu()
+        dist.all_reduce(h, op=dist.ReduceOp.SUM)
+        t.copy_(h)
+    torch.cuda.synchronize(dev)
+    check(lib.dn_model_gradient_from_device(model.handle, t.data_ptr()))
+
+
 def make_shot(model, sh):
     """A Shot from a shot tuple (src_i, src_j, signals, rec_i, rec_j[, src_type[, src_azi[, (x, z)]]])."""
     from . import api as dn
@@ -66,7 +106,8 @@ def source_position(sh, dh):
 def memory_batches(params, shots, idx, store, device=0, share=0.9):
     """idx split into batches that fit `share` of the device's free memory (the
     library's cached blocks counted as free), spread evenly: 32 shots that fit
-    9 at a time run as 4 x 8."""
+    9 at a time run as 4 x 8.  A shot larger than the free memory raises
+    MemoryError before any batch runs."""
     from . import api as dn
 
     idx = list(idx)
@@ -75,38 +116,48 @@ def memory_batches(params, shots, idx, store, device=0, share=0.9):
     ntr = max(len(shots[k][3]) for k in idx)
     fp = dn.shot_footprint(params, ntr, store)
     free, _ = dn.device_memory(device)
+    if fp > free:
+        raise MemoryError(f"one shot needs {fp} bytes of device memory and {free} are free on device {device}")
     most = max(1, int(share * free / max(fp, 1)))
     nb = -(-len(idx) // most)
     size = -(-len(idx) // nb)
     return [idx[k:k + size] for k in range(0, len(idx), size)]
 
 
-def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_taper=None, residual=None,
-                     energy=None, misfit_shots=None):
+def shard_of(params, idx, dist=None):
+    """This rank's share of the shot indices idx (LPT over equal costs: round robin)."""
+    rank, world = _world(dist)
+    idx = list(idx)
+    costs = [params.nx * params.ny * params.nt for _ in idx]
+    return [idx[k] for k in assign_shots(costs, world)[rank]]
+
+
+def gradient_model(params, model, shots, obs, dist=None, device_index=0, shot_taper=None, residual=None,
+                   energy=None, misfit_shots=None):
     """FWI gradient of `shots` sharded over the ranks of `dist` (all ranks pass
-    the same arguments).  Each rank runs its share in batches that fit its GPU's memory:
-    forward with snapshots, device residuals against `obs`, adjoint, and stacks
-    its shots' gradients in shot order; the partial gradients and misfits are
-    then summed over ranks.  Returns (g_vp, g_vs, g_rho, misfit), float64, on
-    every rank.  shot_taper = (srtshape, srtradius, filtsize) applies the
-    per-shot circular taper (taper_grad_shot.c) around each shot's first source
-    before stacking; residual = the calc_res options of Shot.residual_ex (LNORM,
-    N_ORDER, OFFSET_MUTE, ...; None: the L2 residual); energy = (C_vp, C_vs,
-    C_rho) scales each shot's gradient by its energy weights (EPRECOND 1 or 3
-    in params); misfit_shots: the indices whose misfit is summed (the reference's
+    the same arguments), kept on the device.  Each rank runs its share in
+    batches that fit its GPU's memory: forward with snapshots, device residuals
+    against `obs`, adjoint, and stacks its shots' gradients in shot order into a
+    Model of `model`; the stacked gradients are then summed over ranks on the
+    device (allreduce_model_gradient) and the misfits as one scalar.  Returns
+    (Model, misfit): the Model holds the summed gradients (Model.gradient() reads
+    them) and is the caller's to close.
+
+    shot_taper = (srtshape, srtradius, filtsize) applies the per-shot circular
+    taper (taper_grad_shot.c) around each shot's first source before stacking;
+    residual = the calc_res options of Shot.residual_ex (LNORM, N_ORDER,
+    OFFSET_MUTE, ...; None: the L2 residual); energy = (C_vp, C_vs, C_rho)
+    scales each shot's gradient by its energy weights (EPRECOND 1 or 3 in
+    params); misfit_shots: the indices whose misfit is summed (the reference's
     test shots, TESTSHOT_START..END by INCR; None: all)."""
     from . import api as dn
     from ._lib import MODE_ADJOINT, MODE_FORWARD, SEC_VX, SEC_VY
 
-    rank = dist.get_rank() if dist is not None and dist.is_initialized() else 0
-    world = dist.get_world_size() if dist is not None and dist.is_initialized() else 1
-    costs = [params.nx * params.ny * params.nt for _ in shots]
-    mine = assign_shots(costs, world)[rank]
-    g = [np.zeros((params.nx, params.ny), np.float64) for _ in range(3)]
+    mine = shard_of(params, range(len(shots)), dist)
     misfit = 0.0
-    if mine:
-        m = dn.Model(params, *model[:3], model[3] if params.L else None, model[4] if params.L else None,
-                     device=device_index)
+    m = dn.Model(params, *model[:3], model[3] if params.L else None, model[4] if params.L else None,
+                 device=device_index)
+    try:
         for part in memory_batches(params, shots, mine, 1, device_index):
             ss = [make_shot(m, shots[k]) for k in part]
             dn.run(ss, MODE_FORWARD)
@@ -129,10 +180,58 @@ def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_
                                              else tuple(shot_taper) + (sx, sz))
             for s in ss:
                 s.close()
-        g = [x.astype(np.float64) for x in m.gradient()]
+        allreduce_model_gradient(m, dist)
+        misfit = allreduce_scalar(misfit, dist, _collective_device(dist, device_index))
+    except BaseException:
         m.close()
-    dev = None
+        raise
+    return m, misfit
+
+
+def _collective_device(dist, device_index):
     if dist is not None and dist.is_initialized() and dist.get_backend() == "nccl":
-        dev = f"cuda:{device_index}"
-    red = allreduce_sum(g + [np.array([misfit])], dist, dev)
-    return red[0], red[1], red[2], float(red[3][0])
+        return f"cuda:{device_index}"
+    return None
+
+
+def sharded_gradient(params, model, shots, obs, dist=None, device_index=0, shot_taper=None, residual=None,
+                     energy=None, misfit_shots=None):
+    """gradient_model's gradients fetched to the host: (g_vp, g_vs, g_rho,
+    misfit), float64 arrays in file order, on every rank."""
+    m, misfit = gradient_model(params, model, shots, obs, dist, device_index, shot_taper, residual, energy,
+                               misfit_shots)
+    g = [x.astype(np.float64) for x in m.gradient()]
+    m.close()
+    return g[0], g[1], g[2], misfit
+
+
+def sharded_misfit(params, model, shots, obs, idx, dist=None, device_index=0, residual=None):
+    """The objective of obj_psv.c: mode-2 forward runs of the shots idx on
+    `model`, each rank running its share (src/PSV/obj_psv.c:48 loops over its
+    own shots) in batches that fit its GPU, the vx and vy misfits summed over
+    the rank's shots and then over ranks as one scalar (obj_psv.c:233)."""
+    from . import api as dn
+    from ._lib import MODE_OBJECTIVE, SEC_VX, SEC_VY
+
+    p = params.replace(store_snapshots=0, ckpt_steps=0)
+    mine = shard_of(p, idx, dist)
+    L2 = 0.0
+    if mine:
+        m = dn.Model(p, *model[:3], model[3] if p.L else None, model[4] if p.L else None, device=device_index)
+        try:
+            for part in memory_batches(p, shots, mine, 0, device_index):
+                ss = [make_shot(m, shots[k]) for k in part]
+                dn.run(ss, MODE_OBJECTIVE)
+                for s, k in zip(ss, part):
+                    ovx, ovy = obs[k]
+                    if residual is None:
+                        L2 += s.residual(ovx, SEC_VX) + s.residual(ovy, SEC_VY)
+                    else:
+                        sx, sz = source_position(shots[k], p.dh)
+                        opts = dict({"src_x": sx, "src_z": sz}, **residual)
+                        L2 += s.residual_ex(ovx, SEC_VX, **opts) + s.residual_ex(ovy, SEC_VY, **opts)
+                for s in ss:
+                    s.close()
+        finally:
+            m.close()
+    return allreduce_scalar(L2, dist, _collective_device(dist, device_index))

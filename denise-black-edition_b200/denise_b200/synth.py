@@ -18,79 +18,8 @@ import math
 import numpy as np
 
 from .api import PsvParams, wavelet
-
-
-def _smooth(noise, sigma):
-    from scipy.ndimage import gaussian_filter
-
-    return gaussian_filter(noise, sigma=sigma, mode="nearest")
-
-
-def base_model(nx, ny, dh, seed, smooth_sigma=10.0):
-    rng = np.random.default_rng(seed)
-    z = np.arange(ny, dtype=np.float64) * dh
-    zmax = max(z[-1], dh)
-    vp1 = 1800.0 + 2700.0 * z / zmax
-    depths = rng.uniform(0.0, zmax, 6)
-    jumps = rng.uniform(-300.0, 300.0, 6)
-    for d, jmp in zip(depths, jumps):
-        vp1 = vp1 + np.where(z >= d, jmp, 0.0)
-    vp = np.broadcast_to(vp1[None, :], (nx, ny)).copy()
-    pert = _smooth(rng.standard_normal((nx, ny)), smooth_sigma)
-    pert /= max(np.abs(pert).max(), 1e-30)
-    vp = vp * (1.0 + 0.05 * pert)
-    vs = np.maximum(vp / 1.73, 1000.0)
-    rho = 310.0 * vp ** 0.25
-    return vp.astype(np.float32), vs.astype(np.float32), rho.astype(np.float32)
-
-
-def q_model(nx, ny, seed, smooth_sigma=10.0):
-    rng = np.random.default_rng(seed + 7919)
-    qp0 = rng.uniform(60.0, 120.0)
-    qs0 = rng.uniform(30.0, 60.0)
-    n = _smooth(rng.standard_normal((nx, ny)), smooth_sigma)
-    n /= max(np.abs(n).max(), 1e-30)
-    return (qp0 * (1 + 0.1 * n)).astype(np.float32), (qs0 * (1 + 0.1 * n)).astype(np.float32)
-
-
-def smoothed(a, sigma):
-    return _smooth(np.asarray(a, np.float64), sigma).astype(np.float32)
-
-
-def add_ellipse(vp, vs, rho, dh, seed, v=5500.0):
-    rng = np.random.default_rng(seed + 104729)
-    nx, ny = vp.shape
-    cx, cz = rng.uniform(0.3, 0.7) * nx, rng.uniform(0.4, 0.7) * ny
-    ax, az = rng.uniform(0.05, 0.12) * nx, rng.uniform(0.05, 0.12) * ny
-    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
-    m = ((ii - cx) / ax) ** 2 + ((jj - cz) / az) ** 2 <= 1.0
-    vp = vp.copy()
-    vp[m] = v
-    return vp, np.maximum(vp / 1.73, 1000.0).astype(np.float32), (310.0 * vp ** 0.25).astype(np.float32)
-
-
-def iround(x):
-    """fd.h:17: (int)floor(x + 0.5)."""
-    return int(math.floor(x + 0.5))
-
-
-def grid_index(x_m, dh):
-    """Grid index of a source/receiver coordinate (sources.c, splitsrc.c:27, receiver.c:55)."""
-    return iround(np.float32(x_m) / np.float32(dh))
-
-
-def receivers_line(x0, x1, n, z, dh):
-    xs = np.linspace(x0, x1, n)
-    ri = np.array([grid_index(x, dh) for x in xs], np.int32)
-    rj = np.full(n, grid_index(z, dh), np.int32)
-    # receiver.c:63-83 removes receivers sharing a grid point
-    keep, seen = [], set()
-    for k in range(n):
-        key = (int(ri[k]), int(rj[k]))
-        if key not in seen:
-            seen.add(key)
-            keep.append(k)
-    return ri[keep], rj[keep]
+from .modelgen import (_smooth, add_ellipse, base_model, c1_acquisition, grid_index, iround, q_model,  # noqa: F401
+                       receivers_line, smoothed)
 
 
 def ricker_source(p: PsvParams, fc, amp=1.0, tshift=0.0):
@@ -134,12 +63,8 @@ def c1_shot(p: PsvParams, k, nshots=64, seed=None):
     seed = k + 1 if seed is None else seed
     vp, vs, rho = base_model(p.nx, p.ny, p.dh, seed)
     qp, qs = q_model(p.nx, p.ny, seed)
-    xmax = (p.nx - 1) * p.dh
-    xs = 200.0 + (xmax - 400.0) * k / max(nshots - 1, 1)
-    si = np.array([grid_index(xs, p.dh)], np.int32)
-    sj = np.array([max(grid_index(10.0, p.dh), 1)], np.int32)
+    (si, sj), (ri, rj) = c1_acquisition(p.nx, p.ny, p.dh, k, nshots)
     sig = ricker_source(p, 8.0)[None, :]
-    ri, rj = receivers_line(100.0, xmax - 100.0, 400, 20.0, p.dh)
     return (vp, vs, rho, qp, qs), (si, sj, sig), (ri, rj)
 
 

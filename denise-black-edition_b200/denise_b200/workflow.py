@@ -100,7 +100,8 @@ def _check_supported(st, params):
 
 
 def stage_fwi(params, model, shots, obs, limits, st, averages, precond_base=None, shot_taper=None, device=0,
-              nlbfgs=20, eps_scale=0.01, scalefac=2.0, stepmax=4, dist=None, test_shots=None):
+              nlbfgs=20, eps_scale=0.01, scalefac=2.0, stepmax=4, dist=None, test_shots=None, grad_method=2,
+              pcg_beta=2, optimizer=None, jacobian=None, inv_modelfile=None):
     """An fwi.FWI configured by one workflow stage."""
     from . import fwi
     from .precond import PrecondConfig
@@ -123,7 +124,9 @@ def stage_fwi(params, model, shots, obs, limits, st, averages, precond_base=None
     return fwi.FWI(p, model, shots, obs, limits, device=device, nlbfgs=nlbfgs, eps_scale=eps_scale,
                    scalefac=scalefac, stepmax=stepmax, dist=dist, precond=precond, shot_taper=shot_taper,
                    time_filter=time_filter, residual=residual, energy=energy,
-                   inv_iter=(st["INV_VP_ITER"], st["INV_VS_ITER"], st["INV_RHO_ITER"]), test_shots=test_shots)
+                   inv_iter=(st["INV_VP_ITER"], st["INV_VS_ITER"], st["INV_RHO_ITER"]), test_shots=test_shots,
+                   grad_method=grad_method, pcg_beta=pcg_beta, averages=averages, optimizer=optimizer,
+                   jacobian=jacobian, inv_modelfile=inv_modelfile, scalerho=st["SCALERHO"])
 
 
 def stage_files(prefix, stage):
@@ -136,7 +139,7 @@ def _write_log(path, f, st, stage):
     """The misfit log line of FWI_PSV.c:734-743 (MISFIT_LOG_FILE): opteps, epst1[1..3],
     L2t[1..4] and the stage, with FC_START and FC before the stage when TIME_FILT is set."""
     h = f.history[-1]
-    eps = h["eps"] if h["found"] else 0.0
+    eps = h["eps"]          # opteps_vp: the step taken (0 after a failed search past MIN_ITER)
     L2t = list(h["L2t"]) + [h["misfit"]]
     epst = list(h["epst"])
     v = (eps, epst[0], epst[1], epst[2], L2t[0], L2t[1], L2t[2], L2t[3])
@@ -161,21 +164,35 @@ def _write_model(files, model):
 
 def run_workflow(params, model, shots, obs, limits, stages, itermax, min_iter=0, precond_base=None,
                  shot_taper=None, device=0, dist=None, out_prefix=None, misfit_log=None, resume=False,
-                 shots_for_stage=None, inv_mod_out=None, **fwi_kw):
+                 shots_for_stage=None, inv_mod_out=None, grad_method=2, nlbfgs=20, pcg_beta=2, jacobian=None,
+                 **fwi_kw):
     """Runs the stages in order from the starting model; returns (vp, vs, rho, [StageResult]).
+
+    The loop is FWI_PSV.c:398-840: the model averages C_vp, C_vs, C_rho of the
+    starting model normalise the gradients of every stage; one optimiser
+    (grad_method 2: L-BFGS with nlbfgs pairs, 1: PCG with pcg_beta) serves all
+    stages and is reset only when a stage ends by its abort criterion; a stage
+    ends after ITERMAX iterations or, once MIN_ITER iterations are done, when
+    the misfit changed by at most PRO over two iterations or the step search
+    failed (a failed search moves the model by 0 after MIN_ITER iterations and
+    by the smallest step tried before).
 
     shots_for_stage: a function of the stage's dict returning its shots, for
     wavelets that depend on the stage (wavelet.c integrates N_ORDER times);
     otherwise every stage uses `shots`.
 
-    out_prefix: write each stage's final model as stage_files(out_prefix, stage) (rank 0 of dist).
+    out_prefix: the INV_MODELFILE prefix: each update writes <prefix>_{vp,vs,rho}.bin
+    (calc_mat_change_test_PSV) and the stage models as below (rank 0 of dist).
     inv_mod_out: None writes every stage's final model; 0 or 1 follow FWI_PSV.c: 0 writes
     a stage's model only when the stage ends by the abort criterion or a failed step
     search (model_freq_out_PSV), 1 writes the model after every iteration
     (iteration_files, model_it_out_PSV) and no stage files.
+    jacobian: the JACOBIAN prefix of the L-BFGS files (extract_LBFGS_PSV).
     misfit_log: append one line per iteration in the reference's misfit-log format.
     resume: start after the last stage whose three model files exist, from that model (the
     reference's restart from its last written model)."""
+    from .fwi import Optimizer
+
     vp, vs, rho = [np.ascontiguousarray(a, np.float32) for a in model[:3]]
     averages = model_averages(vp, vs, rho)          # of the starting model (iter_true == 1)
     nx, ny = params.nx, params.ny
@@ -193,36 +210,43 @@ def run_workflow(params, model, shots, obs, limits, stages, itermax, min_iter=0,
                 results = [StageResult(j, 0, [], "resumed") for j in range(1, k + 1)]
                 first = k + 1
                 break
-    for k in range(first, len(stages) + 1):
-        st = stages[k - 1]
-        sh = shots_for_stage(st) if shots_for_stage is not None else shots
-        f = stage_fwi(params, (vp, vs, rho), sh, obs, limits, st, averages, precond_base, shot_taper, device,
-                      dist=dist, **fwi_kw)
-        misfits, reason, it = [], "ITERMAX", 0
-        try:
-            for it in range(1, itermax + 1):
-                misfits.append(f.iterate(it))
-                if misfit_log is not None and rank0:
-                    _write_log(misfit_log, f, st, k)
-                found = f.history[-1]["found"]
-                stop = None
-                if it > min_iter and it >= 3 and abs(misfits[-3] - misfits[-1]) / misfits[-3] <= st["PRO"]:
-                    stop = "PRO"
-                elif not found:
-                    stop = "step search failed"
-                if stop is not None:
-                    reason = stop
-                    if out_prefix is not None and rank0 and inv_mod_out == 0:
-                        _write_model(stage_files(out_prefix, k), (f.vp, f.vs, f.rho))
-                    break
-                if out_prefix is not None and rank0 and inv_mod_out == 1:
-                    _write_model(iteration_files(out_prefix, k, it), (f.vp, f.vs, f.rho))
-        finally:
-            f.lbfgs.close()
-            if f.precond is not None:
-                f.precond.close()
-        vp, vs, rho = f.vp, f.vs, f.rho
-        if out_prefix is not None and rank0 and inv_mod_out is None:
-            _write_model(stage_files(out_prefix, k), (vp, vs, rho))
-        results.append(StageResult(k, it, misfits, reason))
+    optimizer = Optimizer(grad_method, nx, ny, nlbfgs, pcg_beta, device)
+    try:
+        for k in range(first, len(stages) + 1):
+            st = stages[k - 1]
+            sh = shots_for_stage(st) if shots_for_stage is not None else shots
+            f = stage_fwi(params, (vp, vs, rho), sh, obs, limits, st, averages, precond_base, shot_taper, device,
+                          dist=dist, nlbfgs=nlbfgs, grad_method=grad_method, pcg_beta=pcg_beta,
+                          optimizer=optimizer, jacobian=jacobian, inv_modelfile=out_prefix, **fwi_kw)
+            misfits, reason, it = [], "ITERMAX", 0
+            try:
+                for it in range(1, itermax + 1):
+                    misfits.append(f.iterate(it, min_iter))
+                    if misfit_log is not None and rank0:
+                        _write_log(misfit_log, f, st, k)
+                    found = f.history[-1]["found"]
+                    stop = None
+                    # FWI_PSV.c:782-832 (the reference reads L2_hist[iter - 2] before it exists in
+                    # iterations 1 and 2, where the criterion cannot hold)
+                    if it > min_iter:
+                        if it >= 3 and abs(misfits[-3] - misfits[-1]) / misfits[-3] <= st["PRO"]:
+                            stop = "PRO"
+                        elif not found:
+                            stop = "step search failed"
+                    if stop is not None:
+                        reason = stop
+                        if out_prefix is not None and rank0 and inv_mod_out == 0:
+                            _write_model(stage_files(out_prefix, k), (f.vp, f.vs, f.rho))
+                        optimizer.reset()
+                        break
+                    if out_prefix is not None and rank0 and inv_mod_out == 1:
+                        _write_model(iteration_files(out_prefix, k, it), (f.vp, f.vs, f.rho))
+            finally:
+                f.close()
+            vp, vs, rho = f.vp, f.vs, f.rho
+            if out_prefix is not None and rank0 and inv_mod_out is None:
+                _write_model(stage_files(out_prefix, k), (vp, vs, rho))
+            results.append(StageResult(k, it, misfits, reason))
+    finally:
+        optimizer.close()
     return vp, vs, rho, results

@@ -239,6 +239,14 @@ int dn_model_zero_gradient(dn_model *m);
  * is), e.g. with the sum over ranks before the conditioning below. */
 int dn_model_set_gradient(dn_model *m, const float *g_vp, const float *g_vs, const float *g_rho);
 
+/* The model's stacked gradients as one vector of 3 nx ny doubles in device
+ * memory of the model's device (classes vp, vs, rho, each row-major [j][i]),
+ * e.g. for an all-reduce sum over ranks in place of grad_obj_psv.c:371-390's
+ * element-wise MPI_Allreduce, and back (rounded to the model's accumulator
+ * type).  Both wait for the device's pending work first. */
+int dn_model_gradient_to_device(const dn_model *m, double *d_out);
+int dn_model_gradient_from_device(dn_model *m, const double *d_in);
+
 /* ---- gradient conditioning ------------------------------------------------
  * smooth_grad (src/smooth_grad.c) of the three stacked gradients followed by
  * precond_PSV (src/PSV/precond_PSV.c), FWI_PSV.c:628-634, and the per-shot
@@ -428,6 +436,36 @@ int dn_lbfgs_push(dn_lbfgs *L, const double *d_s, const double *d_y);
 int dn_lbfgs_count(const dn_lbfgs *L, int *count);
 /* r = H g (device vectors); the model update is x - eps r */
 int dn_lbfgs_direction(dn_lbfgs *L, const double *d_g, double *d_r);
+
+/* The reference's optimisers, FWI_PSV.c:637-676, on a model's stacked and
+ * conditioned gradient, which the call replaces by the search direction that
+ * calc_mat_change_test_PSV then applies (dn_mat_update):
+ *  - grad_method 2, L-BFGS with nlbfgs pairs: the LBFGS_pointer rule of
+ *    FWI_PSV.c:452-466, store_LBFGS_PSV (src/PSV/store_LBFGS_PSV.c: gradients
+ *    normalised by c = {C_vp, C_vs, C_rho}, the model averages of the starting
+ *    model; y and s against the previous call's normalised gradient and model),
+ *    LBFGS (src/LBFGS.c) and extract_LBFGS_PSV (src/PSV/extract_LBFGS_PSV.c:
+ *    the direction times c; in iteration 1 the normalised gradient);
+ *  - grad_method 1, PCG with PCG_BETA pcg_beta (1 Fletcher-Reeves, 2
+ *    Polak-Ribiere, 3 Hestenes-Stiefel, 4 Dai-Yuan): descent, store_PCG_PSV,
+ *    PCG (src/PCG.c), extract_PCG_PSV, descent.
+ * iter is FWI_PSV.c's per-stage iteration counter (1 at a stage's start).  The
+ * vectors are float as in the reference; the dot products are summed in FP64.
+ * The history lives on `device` (2 nlbfgs + 5 vectors of 3 nx ny floats for
+ * L-BFGS, 3 for PCG).  The model (vp, vs, rho) of the step is the model `m`
+ * was created from. */
+typedef struct dn_optim dn_optim;
+int dn_optim_create(int grad_method, int nx, int ny, int nlbfgs, int pcg_beta, int device, dn_optim **out);
+int dn_optim_destroy(dn_optim *o);
+/* zero_LBFGS / zero_PCG and LBFGS_pointer = 1 at a stage change (FWI_PSV.c:800-811) */
+int dn_optim_reset(dn_optim *o);
+int dn_optim_step(dn_optim *o, dn_model *m, int iter, const float c[3]);
+/* After an L-BFGS step, the vectors extract_LBFGS_PSV writes as the JACOBIAN
+ * files, in file order: which 0, 1, 2 = the normalised gradients
+ * (<JACOBIAN>_p.old, _p_u.old, _p_rho.old), 3, 4, 5 = the model
+ * (_p_vp.old, _p_vs.old, _p_mrho.old), 6, 7, 8 = the direction (_c.old,
+ * _c_u.old, _c_rho.old).  out holds nx*ny floats. */
+int dn_optim_get(const dn_optim *o, int which, float *out);
 
 /* calc_opt_step (src/calc_opt_step.c): the step length at the extremum of the
  * parabola through (epst[k], L2t[k]), k = 0..2, with the reference's clamping

@@ -1,6 +1,9 @@
 /*
  * ORACLE / TEST INFRASTRUCTURE - body of the CPU restatement, included twice
  * by psv_oracle.c with REAL = float (suffix _f) and REAL = double (_d).
+ * The per-cell loops of the updates, the snapshot store and the correlation
+ * run in parallel over rows (OpenMP): every iteration writes only its own
+ * cells, so the results do not depend on the thread count.
  * Variables the reference declares `float` are REAL here; every double
  * literal and double intermediate of the reference is kept, so the _f build
  * reproduces the reference's rounding and the _d build is an FP64 scheme.
@@ -323,6 +326,7 @@ static void FN(or_update_v)(CTX *c, int nt, int sw)
 {
     const int R = c->R, nx = c->nx, ny = c->ny, FW = c->fw;
     const REAL *hc = c->hc;
+#pragma omp parallel for schedule(static)
     for (int j = 1; j <= ny; j++)
         for (int i = 1; i <= nx; i++) {
             REAL sxx_x = hc[1] * (AT(c->sxx, j, i + 1) - AT(c->sxx, j, i));
@@ -453,6 +457,7 @@ static void FN(or_vderiv)(CTX *c, int j, int i, REAL dhi, REAL *pvxx, REAL *pvyx
 static void FN(or_update_s_el)(CTX *c)
 {
     REAL dhi = c->dt / c->dh;
+#pragma omp parallel for schedule(static)
     for (int j = 1; j <= c->ny; j++)
         for (int i = 1; i <= c->nx; i++) {
             REAL vxx, vyx, vxy, vyy;
@@ -472,6 +477,7 @@ static void FN(or_update_s_vi)(CTX *c)
     const int L = c->L;
     REAL dhi = 1.0 / c->dh;
     REAL dthalbe = c->dt / 2.0;
+#pragma omp parallel for schedule(static)
     for (int j = 1; j <= c->ny; j++)
         for (int i = 1; i <= c->nx; i++) {
             REAL vxx, vyx, vxy, vyy;
@@ -639,6 +645,7 @@ static void FN(or_store)(CTX *c, int k)
     size_t n = (size_t)c->nx * c->ny;
     REAL *dst = c->snap + (size_t)k * 5 * n;
     REAL *src[5] = {c->vxp1, c->vyp1, c->sxx, c->syy, c->sxy};
+#pragma omp parallel for schedule(static) collapse(2)
     for (int f = 0; f < 5; f++)
         for (int i = 1; i <= c->nx; i++)
             for (int j = 1; j <= c->ny; j++) dst[f * n + FO(i, j)] = AT(src[f], j, i);
@@ -653,6 +660,7 @@ static void FN(or_correlate)(CTX *c, int k)
 {
     size_t n = (size_t)c->nx * c->ny;
     const REAL *s = c->snap + (size_t)k * 5 * n;
+#pragma omp parallel for schedule(static)
     for (int i = 1; i <= c->nx; i++)
         for (int j = 1; j <= c->ny; j++) {
             size_t o = FO(i, j);

@@ -829,3 +829,94 @@ int refh_read_par_fwi(const char *path, int *iv, float *fv, char *strs)
     }
     return 0;
 }
+
+/* ---- the reference's optimisers: FWI_PSV.c:637-676 -------------------------
+ * GRAD_METHOD 2: the LBFGS_pointer rule of FWI_PSV.c:452-466, store_LBFGS_PSV,
+ * LBFGS, extract_LBFGS_PSV (which keep the previous gradient and model in the
+ * JACOBIAN files, here under `jacobian`); GRAD_METHOD 1: descent, store_PCG_PSV,
+ * PCG, extract_PCG_PSV, store_PCG_PSV, descent.  Models and gradients cross in
+ * file order; the gradients are replaced by the search direction.  The vectors
+ * persist between calls like FWI_PSV.c's; refh_optim_reset is zero_LBFGS /
+ * zero_PCG with LBFGS_pointer = 1 (FWI_PSV.c:800-811). */
+static int o_method = 0, o_nlbfgs = 0, o_ptr = 1, o_vec = 0;
+static float *o_y, *o_s, *o_q, *o_r, *o_rho, *o_alpha, *o_beta, *o_new, *o_old, *o_dir;
+
+int refh_optim_init(int method, int nx, int ny, int nlbfgs, int pcg_beta, const char *jacobian)
+{
+    FP = stderr;
+    NX = NXG = nx;
+    NY = NYG = ny;
+    IDX = IDY = 1;
+    MYID = MYID_SHOT = 0;
+    POS[1] = POS[2] = 0;
+    NPROCX = NPROCY = 1;
+    NPROC = NP = 1;
+    PCG_BETA = pcg_beta;
+    strncpy(JACOBIAN, jacobian, STRING_SIZE - 1);
+    o_method = method;
+    o_nlbfgs = nlbfgs;
+    o_ptr = 1;
+    o_vec = 3 * nx * ny;
+    if (method == 2) {
+        o_y = vector(1, o_vec * nlbfgs);
+        o_s = vector(1, o_vec * nlbfgs);
+        o_q = vector(1, o_vec);
+        o_r = vector(1, o_vec);
+        o_rho = vector(1, nlbfgs);
+        o_alpha = vector(1, nlbfgs);
+        o_beta = vector(1, nlbfgs);
+    } else {
+        o_old = vector(1, o_vec);
+        o_new = vector(1, o_vec);
+        o_dir = vector(1, o_vec);
+    }
+    return 0;
+}
+
+int refh_optim_reset(void)
+{
+    if (o_method == 2) {
+        zero_LBFGS(o_nlbfgs, o_vec, o_y, o_s, o_q, o_r, o_alpha, o_beta, o_rho);
+        o_ptr = 1;
+    } else {
+        zero_PCG(o_old, o_new, o_dir, o_vec);
+    }
+    return 0;
+}
+
+int refh_optim_step(int iter, const float *c3, const float *vp, const float *vs, const float *rho, float *gvp,
+                    float *gvs, float *grho)
+{
+    const int nx = NX, ny = NY;
+    C_vp = c3[0];
+    C_vs = c3[1];
+    C_rho = c3[2];
+    float **P = grad_in(nx, ny, vp), **U = grad_in(nx, ny, vs), **R = grad_in(nx, ny, rho);
+    float **G = grad_in(nx, ny, gvp), **Gu = grad_in(nx, ny, gvs), **Gr = grad_in(nx, ny, grho);
+    float **Gp = grad_in(nx, ny, gvp), **Gpu = grad_in(nx, ny, gvs), **Gpr = grad_in(nx, ny, grho);
+    if (o_method == 2) {
+        if (iter > 2) o_ptr++;
+        if (o_ptr > o_nlbfgs) o_ptr = 1;
+        store_LBFGS_PSV(NULL, 0, NULL, NULL, 0, iter, G, Gp, Gu, Gpu, Gr, Gpr, o_y, o_s, o_q, P, U, R, nx * ny,
+                        o_ptr, o_nlbfgs, o_vec);
+        LBFGS(iter, o_y, o_s, o_rho, o_alpha, o_q, o_r, o_beta, o_ptr, o_nlbfgs, o_vec);
+        extract_LBFGS_PSV(iter, G, Gp, Gu, Gpu, Gr, Gpr, P, U, R, o_r);
+    } else {
+        descent(G, Gp);
+        descent(Gu, Gpu);
+        descent(Gr, Gpr);
+        store_PCG_PSV(o_new, Gp, Gpu, Gpr);
+        PCG(o_new, o_old, o_dir, 3);
+        extract_PCG_PSV(o_dir, G, Gu, Gr);
+        store_PCG_PSV(o_old, Gp, Gpu, Gpr);
+        descent(G, G);
+        descent(Gu, Gu);
+        descent(Gr, Gr);
+    }
+    grad_out(nx, ny, G, gvp);
+    grad_out(nx, ny, Gu, gvs);
+    grad_out(nx, ny, Gr, grho);
+    float **ms[6] = {P, U, R, Gp, Gpu, Gpr};   /* grad_out freed G, Gu, Gr */
+    for (int k = 0; k < 6; k++) free_matrix(ms[k], -REFH_PAD, ny + REFH_PAD, -REFH_PAD, nx + REFH_PAD);
+    return o_ptr;
+}

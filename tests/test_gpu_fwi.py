@@ -80,7 +80,7 @@ def test_two_fwi_iterations_lower_the_misfit():
     L2 = f.misfit((f.vp, f.vs, f.rho))
     assert all(h["found"] for h in f.history), f.history
     assert L1 < L0 and L2 < L1, (L0, L1, L2)
-    f.lbfgs.close()
+    f.close()
 
 
 def test_fwi_with_gradient_conditioning():
@@ -123,7 +123,7 @@ def test_fwi_with_gradient_conditioning():
     L1 = f.iterate(2)
     assert all(h["found"] for h in f.history), f.history
     assert L1 < L0, (L0, L1)
-    f.lbfgs.close()
+    f.close()
 
 
 def test_fwi_with_time_filter():
@@ -148,7 +148,7 @@ def test_fwi_with_time_filter():
     np.testing.assert_array_equal(f.obs[1][0], dn.tdfilt(obs[1][0], p.dt, 4, 30.0, 2.0))
     L0 = f.iterate(1)
     assert np.isfinite(L0) and f.history[0]["found"]
-    f.lbfgs.close()
+    f.close()
 
 
 def test_workflow_two_stages(tmp_path):

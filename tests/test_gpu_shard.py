@@ -70,3 +70,37 @@ def test_memory_batches_give_the_same_gradient(monkeypatch):
         for a, b in zip(got[:3], one[:3]):
             np.testing.assert_array_equal(a, b)
         assert got[3] == one[3]
+
+
+def _misfit_worker(rank, world, port, out_dir):
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from denise_b200 import shard
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    p, model, shots, obs = _case()
+    ran = []
+    make = shard.make_shot
+    shard.make_shot = lambda m, sh: (ran.append(next(k for k, x in enumerate(shots) if x is sh)), make(m, sh))[1]
+    L2 = shard.sharded_misfit(p, model, shots, obs, range(len(shots)), dist, 0)
+    np.save(os.path.join(out_dir, f"m{rank}.npy"), np.array(ran + [-1, L2]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_step_search_misfit_two_ranks(tmp_path):
+    """obj_psv.c on two ranks: each rank runs the mode-2 forwards of its own test
+    shots only, and the all-reduced misfit equals the single-process one."""
+    from denise_b200.shard import sharded_misfit
+
+    p, model, shots, obs = _case()
+    one = sharded_misfit(p, model, shots, obs, range(len(shots)), None, 0)
+    mp.spawn(_misfit_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
+    r = [np.load(tmp_path / f"m{k}.npy") for k in range(2)]
+    ran = [sorted(x[:-2].astype(int)) for x in r]
+    assert sorted(ran[0] + ran[1]) == list(range(len(shots))) and ran[0] and ran[1]
+    assert r[0][-1] == r[1][-1]
+    assert abs(r[0][-1] - one) <= 1e-12 * abs(one)

@@ -29,7 +29,7 @@ def test_params_and_unsupported_switches(tmp_path, monkeypatch):
     assert p.nt == io.inp_nt(inp) and len(p.fl) == 2
     assert np.float32(p.ts) == np.float32(acq.ts)
     inversion._check_supported(inp)
-    for key in ("GRAD_METHOD", "SWS_TAPER_FILE", "TRKILL", "TIMELAPSE", "GRAVITY"):
+    for key in ("SWS_TAPER_FILE", "TRKILL", "TIMELAPSE", "GRAVITY"):
         inp_case.write_case(str(tmp_path), nshots=2, MODE=1, **{key: 1})
         with pytest.raises(NotImplementedError):
             inversion._check_supported(io.read_inp(str(tmp_path / "case.inp")))
@@ -47,7 +47,7 @@ def test_memory_batches_spread_evenly(monkeypatch):
 
     shots = [(None, None, None, np.zeros(40, np.int32), None)] * 32
     monkeypatch.setattr(api, "shot_footprint", lambda p, ntr, store: 18 << 30)
-    for free_gb, want in ((178, [8] * 4), (90, [4] * 8), (10, [1] * 32), (1000, [32])):
+    for free_gb, want in ((178, [8] * 4), (90, [4] * 8), (19, [1] * 32), (1000, [32])):
         monkeypatch.setattr(api, "device_memory", lambda device=0, f=free_gb: (f << 30, 183 << 30))
         parts = shard.memory_batches(None, shots, range(32), 1, 0)
         assert [len(b) for b in parts] == want, free_gb
@@ -55,3 +55,7 @@ def test_memory_batches_spread_evenly(monkeypatch):
     monkeypatch.setattr(api, "device_memory", lambda device=0: (178 << 30, 183 << 30))
     assert [len(b) for b in shard.memory_batches(None, shots, range(30), 1, 0)] == [8, 8, 8, 6]
     assert shard.memory_batches(None, shots, [], 1, 0) == []
+    # a shot larger than the free memory is refused before anything runs
+    monkeypatch.setattr(api, "device_memory", lambda device=0: (10 << 30, 183 << 30))
+    with pytest.raises(MemoryError):
+        shard.memory_batches(None, shots, range(32), 1, 0)

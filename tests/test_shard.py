@@ -84,3 +84,39 @@ def test_single_process_sum_is_identity():
     out = allreduce_sum(a, None)
     np.testing.assert_array_equal(out[0], a[0])
     np.testing.assert_array_equal(out[1], a[1])
+
+
+def _misfit_worker(rank, world, port, ntest, out_dir):
+    """Each rank takes its share of the test shots (shard_of, as sharded_misfit
+    does) and adds up stand-in misfits; one scalar all-reduce gives the total."""
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from denise_b200.api import PsvParams
+    from denise_b200.shard import allreduce_scalar, shard_of
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    p = PsvParams(nx=40, ny=30, dh=5.0, dt=1e-3, nt=100)
+    test_idx = list(range(1, 2 * ntest, 2))          # TESTSHOT_START 2 .. by INCR 2 (0-based 1, 3, ...)
+    mine = shard_of(p, test_idx, dist)
+    total = allreduce_scalar(sum(_partial(k, (1, 1))[1] for k in mine), dist)
+    np.save(os.path.join(out_dir, f"m{rank}.npy"), np.array(mine + [-1, total]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("ntest", [5, 1])
+def test_step_search_misfit_shards_test_shots(tmp_path, ntest):
+    """The step-length forwards (obj_psv.c:48) run each test shot on one rank only,
+    and the summed misfit is the serial one."""
+    mp.spawn(_misfit_worker, args=(2, _free_port(), ntest, str(tmp_path)), nprocs=2, join=True)
+    r = [np.load(tmp_path / f"m{k}.npy") for k in range(2)]
+    shares = [list(x[:-2].astype(int)) for x in r]
+    test_idx = list(range(1, 2 * ntest, 2))
+    assert sorted(shares[0] + shares[1]) == test_idx        # every test shot on exactly one rank
+    assert abs(len(shares[0]) - len(shares[1])) <= 1
+    want = sum(_partial(k, (1, 1))[1] for k in test_idx)
+    assert r[0][-1] == r[1][-1]
+    assert abs(r[0][-1] - want) <= 1e-12 * want
