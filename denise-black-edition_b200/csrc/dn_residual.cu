@@ -195,12 +195,23 @@ __global__ void k_residual(const float *__restrict__ syn, const float *__restric
     part[l] = L2;
 }
 
-__global__ void k_sum_partials(const double *__restrict__ part, int n, double *__restrict__ out)
+// The misfit: the per-trace double sums added in a fixed order by one block of
+// SUM_THREADS threads (thread t adds traces t, t + SUM_THREADS, ... in order, then a
+// shared-memory tree), so repeated calls give the same bits.
+constexpr int SUM_THREADS = 1024;
+__global__ void __launch_bounds__(SUM_THREADS) k_sum_partials(const double *__restrict__ part, int n,
+                                                              double *__restrict__ out)
 {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    __shared__ double sh[SUM_THREADS];
     double s = 0.0;
-    for (int l = 0; l < n; l++) s = __dadd_rn(s, part[l]);
-    *out = s;
+    for (int l = threadIdx.x; l < n; l += SUM_THREADS) s = __dadd_rn(s, part[l]);
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = SUM_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) sh[threadIdx.x] = __dadd_rn(sh[threadIdx.x], sh[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
 }
 
 }   // namespace
@@ -258,7 +269,7 @@ extern "C" int dn_residual_launch_ex(const float *syn_tm, const float *obs, floa
     a.s1 = s1;
     a.s2 = s2;
     k_residual<<<(ntr + 127) / 128, 128, 0, stream>>>(syn_tm, obs, res, ntr, nt, a, scratch);
-    k_sum_partials<<<1, 1, 0, stream>>>(scratch, ntr, scratch + ntr);
+    k_sum_partials<<<1, SUM_THREADS, 0, stream>>>(scratch, ntr, scratch + ntr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "residual kernels: %s", cudaGetErrorString(e));
     return DN_OK;
@@ -386,7 +397,13 @@ extern "C" int dn_residual_l2(const float *syn_tm, const float *obs, float *res,
 //
 // Set-up: the first call on each device looks up the array's address with that
 // device current (cudaGetSymbolAddress, which may load this module on the
-// device) and caches it; make that first call before any stream capture.
+// device) and caches it; make that first call before any stream capture.  The
+// cached address belongs to the device's current context: after a
+// cudaDeviceReset of that device it would point at freed memory, so a device
+// reset between calls is not supported (as for every other object of this
+// library).  The kernels run on the legacy default stream, which does not wait
+// for work on non-blocking streams: the caller makes sure the producers of
+// syn_tm and obs have finished (e.g. synchronises their stream) before the call.
 // Nothing in the scratch has to start at zero: k_residual writes every
 // partial sum k_sum_partials reads, and the misfit slot is written, not added
 // to.  There is one scratch array per device, so calls that overlap on the

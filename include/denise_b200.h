@@ -324,7 +324,11 @@ int dn_last_run_stats(double *device_ms, long long *launches);
  * source [ntr][nt], time-reversed, first observed sample replaced by the
  * synthetic one, time-integrated when grad_form == 1; l2 (out, host): the misfit
  * 0.5*sum(res^2) accumulated in double.  All arrays are device pointers; the
- * call allocates ntr+1 doubles of device scratch for the per-trace sums. */
+ * call allocates ntr+1 doubles of device scratch for the per-trace sums.  The
+ * kernels run on the legacy default stream, which does not wait for work on
+ * non-blocking streams: the producers of syn_tm and obs must have finished
+ * (e.g. their stream synchronised) before the call; it returns after the misfit
+ * has been read back. */
 int dn_residual_l2(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt, int grad_form,
                    double *l2);
 /* dn_residual_l2 for callers that cannot allocate device memory during the
@@ -334,8 +338,10 @@ int dn_residual_l2(const float *syn_tm, const float *obs, float *res, int ntr, i
  * on host arrays.  Same arguments and results as dn_residual_l2, but the
  * per-trace sums use a static device array, so ntr <= 16384 (DN_EINVAL
  * beyond).  The first call on each device (with that device current) looks up
- * the array and should come before any stream capture.  Calls that overlap on
- * one device share that array and race; serialise them. */
+ * the array and should come before any stream capture; the address it keeps
+ * does not survive a cudaDeviceReset of the device (not supported between
+ * calls).  Calls that overlap on one device share that array and race;
+ * serialise them.  Inputs must be complete as for dn_residual_l2. */
 int dn_residual_l2_noalloc(const float *syn_tm, const float *obs, float *res, int ntr, int nt, float dt,
                            int grad_form, double *l2);
 /* The same for a shot after its forward run: obs [ntr][nt] in host memory,
