@@ -1099,33 +1099,53 @@ static Inst make_inst_state2(const dn_shot *s, int mode)
     return I;
 }
 
-static int run_ckpt(dn_shot *s, int mode, double &ms_total, long long &nl)
+// Checkpointed shots (params.ckpt_steps > 0) of one batch: they share NT, DTINV and
+// the segment length, so the segments line up and every launch covers all of them.
+// Forward (mode 0/2): before each segment every shot's full state is copied to its
+// checkpoint slot, then the segment's steps run for the whole batch.  Adjoint: the
+// segments from last to first; per segment every shot's state is restored from its
+// checkpoint, the segment is recomputed for the batch with its snapshots into the
+// one-segment buffers, and the adjoint steps that correlate with it run for the batch.
+static int run_ckpt(dn_shot *const *shots, int n, int mode, double &ms_total, long long &nl)
 {
-    dn_shot *arr[1] = {s};
     LaunchCfg c, cf;
-    int st = check_batch(arr, 1, mode, c);
-    if (!st && mode == 1) st = check_batch(arr, 1, 0, cf);
+    int st = check_batch(shots, n, mode, c);
+    if (!st && mode == 1) st = check_batch(shots, n, 0, cf);
     if (st) return st;
+    const dn_shot *s0 = shots[0];
+    for (int k = 1; k < n; k++)
+        if (shots[k]->p.nt != s0->p.nt || shots[k]->p.ckpt_steps != s0->p.ckpt_steps ||
+            shots[k]->p.dtinv != s0->p.dtinv || shots[k]->nseg != s0->nseg || shots[k]->nsnap != s0->nsnap)
+            return dn_fail(DN_EINVAL, "dn_run: checkpointed shots of one batch must share NT, DTINV and ckpt_steps");
     DevState *ds;
-    st = dev_state(s->m->device, &ds);
+    st = dev_state(s0->m->device, &ds);
     if (st) return st;
-    CU(cudaSetDevice(s->m->device));
+    CU(cudaSetDevice(s0->m->device));
     st = prepare_launch(c);
     if (st) return st;
-    const int Ls = s->p.ckpt_steps, nt = s->p.nt, nseg = s->nseg, per = Ls / s->p.dtinv;
-    const size_t sb = s->state_bytes;
+    const int Ls = s0->p.ckpt_steps, nt = s0->p.nt, nseg = s0->nseg, per = Ls / s0->p.dtinv;
     cudaStream_t sm = ds->stream;
     std::vector<Inst> h;
     if (mode != 1) {
-        h.push_back(make_inst(s, mode));
-        h[0].store = 0;
+        for (int k = 0; k < n; k++) {
+            h.push_back(make_inst(shots[k], mode));
+            h.back().store = 0;
+        }
     } else {
+        // segment g: n recompute instances, then n adjoint instances
         for (int g = 0; g < nseg; g++) {
-            Inst f = make_inst(s, 0), a = make_inst_state2(s, 1);
-            f.snap_base = a.snap_base = g * per;
-            f.nsnap = a.nsnap = s->nsnap;   // the segment buffer's slots (fewer than per when NT < ckpt_steps)
-            h.push_back(f);
-            h.push_back(a);
+            for (int k = 0; k < n; k++) {
+                Inst f = make_inst(shots[k], 0);
+                f.snap_base = g * per;
+                f.nsnap = shots[k]->nsnap;   // the segment buffer's slots (fewer than per when NT < ckpt_steps)
+                h.push_back(f);
+            }
+            for (int k = 0; k < n; k++) {
+                Inst a = make_inst_state2(shots[k], 1);
+                a.snap_base = g * per;
+                a.nsnap = shots[k]->nsnap;
+                h.push_back(a);
+            }
         }
     }
     Inst *d = nullptr;
@@ -1136,11 +1156,14 @@ static int run_ckpt(dn_shot *s, int mode, double &ms_total, long long &nl)
         dn_free(d);
         return dn_fail(DN_EDEVICE, "checkpointed run: %s", cudaGetErrorString(e));
     }
-    if (mode != 1) {
-        st = zero_for_run(s, mode, sm);
-    } else if (cudaMemsetAsync(s->dstate2, 0, sb, sm) != cudaSuccess ||
-               cudaMemsetAsync(s->d_flag, 0, 4, sm) != cudaSuccess) {
-        st = dn_fail(DN_EDEVICE, "checkpointed adjoint: state reset failed");
+    for (int k = 0; k < n && !st; k++) {
+        dn_shot *s = shots[k];
+        if (mode != 1) {
+            st = zero_for_run(s, mode, sm);
+        } else if (cudaMemsetAsync(s->dstate2, 0, s->state_bytes, sm) != cudaSuccess ||
+                   cudaMemsetAsync(s->d_flag, 0, 4, sm) != cudaSuccess) {
+            st = dn_fail(DN_EDEVICE, "checkpointed adjoint: state reset failed");
+        }
     }
     if (st) {
         dn_free(d);
@@ -1149,20 +1172,26 @@ static int run_ckpt(dn_shot *s, int mode, double &ms_total, long long &nl)
     cudaEventRecord(ds->ev0, sm);
     if (mode != 1) {
         for (int g = 0; g < nseg; g++) {
-            if (mode == 0) cudaMemcpyAsync(s->dckpt + sb * g, s->dstate, sb, cudaMemcpyDeviceToDevice, sm);
-            for (int k = g * Ls + 1; k <= std::min((g + 1) * Ls, nt); k++) launch_step(c, sm, d, ds->d_zero, k, nl);
+            if (mode == 0)
+                for (int k = 0; k < n; k++)
+                    cudaMemcpyAsync(shots[k]->dckpt + shots[k]->state_bytes * g, shots[k]->dstate,
+                                    shots[k]->state_bytes, cudaMemcpyDeviceToDevice, sm);
+            for (int t = g * Ls + 1; t <= std::min((g + 1) * Ls, nt); t++) launch_step(c, sm, d, ds->d_zero, t, nl);
         }
     } else {
         for (int g = nseg - 1; g >= 0; g--) {
             const int a = g * Ls + 1, b = std::min((g + 1) * Ls, nt);
-            cudaMemcpyAsync(s->dstate, s->dckpt + sb * g, sb, cudaMemcpyDeviceToDevice, sm);
-            for (int k = a; k <= b; k++) launch_step(cf, sm, d + 2 * g, ds->d_zero, k, nl);
-            for (int k = nt - b + 1; k <= nt - a + 1; k++) launch_step(c, sm, d + 2 * g + 1, ds->d_zero, k, nl);
+            for (int k = 0; k < n; k++)
+                cudaMemcpyAsync(shots[k]->dstate, shots[k]->dckpt + shots[k]->state_bytes * g, shots[k]->state_bytes,
+                                cudaMemcpyDeviceToDevice, sm);
+            for (int t = a; t <= b; t++) launch_step(cf, sm, d + (size_t)2 * n * g, ds->d_zero, t, nl);
+            for (int t = nt - b + 1; t <= nt - a + 1; t++)
+                launch_step(c, sm, d + (size_t)2 * n * g + n, ds->d_zero, t, nl);
         }
     }
     cudaEventRecord(ds->ev1, sm);
     cudaError_t le = cudaGetLastError();
-    st = finish_run(arr, 1, mode, sm);
+    st = finish_run(shots, n, mode, sm);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, ds->ev0, ds->ev1);
     ms_total += ms;
@@ -1175,15 +1204,14 @@ extern "C" int dn_run(dn_shot *const *shots, int n, int mode)
 {
     DnRange range(mode == 0 ? "dn_run forward" : mode == 1 ? "dn_run adjoint" : "dn_run objective");
     if (shots && n > 0 && shots[0] && shots[0]->nseg > 0) {
-        // checkpointed shots run one after the other
+        // checkpointed shots run as one batch
         double ms = 0.0;
         long long nl = 0;
-        for (int k = 0; k < n; k++) {
+        for (int k = 0; k < n; k++)
             if (!shots[k] || shots[k]->nseg == 0)
                 return dn_fail(DN_EINVAL, "dn_run: checkpointed and stored-snapshot shots cannot share a batch");
-            int st = run_ckpt(shots[k], mode, ms, nl);
-            if (st) return st;
-        }
+        int st = run_ckpt(shots, n, mode, ms, nl);
+        if (st) return st;
         g_last_ms = ms;
         g_last_launches = nl;
         return DN_OK;
