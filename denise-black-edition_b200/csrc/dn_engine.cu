@@ -916,8 +916,25 @@ static int set_smem_attrs_X(int R)
     }
 }
 
+template <bool X>
+static int set_vpipe_attr_X(int R)
+{
+    switch (R) {
+    case 1: return set_vpipe_attr_R<1, X>();
+    case 2: return set_vpipe_attr_R<2, X>();
+    case 3: return set_vpipe_attr_R<3, X>();
+    case 4: return set_vpipe_attr_R<4, X>();
+    case 5: return set_vpipe_attr_R<5, X>();
+    default: return set_vpipe_attr_R<6, X>();
+    }
+}
+
 static int prepare_launch(const LaunchCfg &c)
 {
+    if (c.vpipe) {
+        int e = c.exact ? set_vpipe_attr_X<true>(c.R) : set_vpipe_attr_X<false>(c.R);
+        if (e) return dn_fail(DN_EDEVICE, "cudaFuncSetAttribute (dynamic shared memory) failed");
+    }
     if (!c.tma) return DN_OK;
     int e = c.exact ? set_smem_attrs_X<true>(c.R) : set_smem_attrs_X<false>(c.R);
     if (e) return dn_fail(DN_EDEVICE, "cudaFuncSetAttribute (dynamic shared memory) failed");
@@ -1029,6 +1046,27 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c, con
         if (m == 1) c.any_adj = true;
     }
     c.tile_grid = dim3(maxtiles, n);
+    // pipelined velocity kernel (DN_VPIPE=1): strips of VP_W columns, about four CTAs per
+    // resident slot (148 SMs x 3) over the batch, at least 32 rows tall (DN_VPIPE_ROWS sets it)
+    const char *vp = getenv("DN_VPIPE");
+    c.vpipe = vp && strcmp(vp, "1") == 0;
+    c.vsh = 0;
+    c.vgrid = dim3(1, n);
+    if (c.vpipe) {
+        int sum_tx = 0, maxny = 1;
+        for (int k = 0; k < n; k++) {
+            sum_tx += (shots[k]->p.nx + VP_W - 1) / VP_W;
+            maxny = std::max(maxny, shots[k]->p.ny);
+        }
+        const int strips = std::max(1, (4 * 148 * 3 + sum_tx - 1) / sum_tx);
+        c.vsh = std::max(32, (maxny + strips - 1) / strips);
+        const char *vr = getenv("DN_VPIPE_ROWS");
+        if (vr && atoi(vr) > 0) c.vsh = atoi(vr);
+        int maxc = 1;
+        for (int k = 0; k < n; k++)
+            maxc = std::max(maxc, ((shots[k]->p.nx + VP_W - 1) / VP_W) * ((shots[k]->p.ny + c.vsh - 1) / c.vsh));
+        c.vgrid = dim3(maxc, n);
+    }
     c.src_grid = dim3((maxsrc + 127) / 128, n);
     c.surf_grid = dim3((maxnx + 127) / 128, n);
     c.rec_grid = dim3((maxtr + 127) / 128, n);

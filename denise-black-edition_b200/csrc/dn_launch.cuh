@@ -5,6 +5,7 @@
 #pragma once
 
 #include "dn_kernels_tma.cuh"
+#include "dn_kernels_vpipe.cuh"
 
 namespace dn {
 
@@ -15,6 +16,9 @@ struct LaunchCfg {
     bool exact;
     bool tma;   // stencil kernels fed by the bulk-copy row pipeline
     bool pack;  // paired-column (FP32x2) stencil kernels, bx / 2 threads per tile
+    bool vpipe; // velocity update by the warp-specialised copy pipeline (k_update_v_pipe)
+    dim3 vgrid; // its grid: strips of VP_W columns x vsh rows per instance
+    int vsh;
     bool any_surf, any_src_s, any_store, any_adj, any_rec;
 };
 
@@ -32,5 +36,7 @@ void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int
 // opts the bulk-copy pipeline kernels of order R into their dynamic shared memory
 template <int R, bool X>
 int set_smem_attrs_R();
+template <int R, bool X>
+int set_vpipe_attr_R();
 
 }   // namespace dn

@@ -11,7 +11,8 @@ void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int
                           cudaEvent_t *marks)
 {
     MARK(0);
-    if (c.tma) k_update_v_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QV>(slot_floats_v()), st>>>(d, ntb, off);
+    if (c.vpipe) k_update_v_pipe<R, X><<<c.vgrid, VP_THREADS, vpipe_smem_bytes(), st>>>(d, ntb, off, c.vsh);
+    else if (c.tma) k_update_v_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QV>(slot_floats_v()), st>>>(d, ntb, off);
     else if (c.pack) k_update_v2<R, X><<<c.tile_grid, c.bx / 2, 0, st>>>(d, ntb, off);
     else k_update_v<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
     MARK(1);
@@ -101,6 +102,13 @@ int set_smem_attrs_R()
     return e == cudaSuccess ? 0 : -1;
 }
 
+template <int R, bool X>
+int set_vpipe_attr_R()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_update_v_pipe<R, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)vpipe_smem_bytes());
+    return e == cudaSuccess ? 0 : -1;
+}
 
 #ifdef DN_R
 template void launch_step_R<DN_R, true>(const LaunchCfg &, cudaStream_t, const Inst *, const int *, int, long long &,
@@ -109,6 +117,8 @@ template void launch_step_R<DN_R, false>(const LaunchCfg &, cudaStream_t, const 
                                          cudaEvent_t *);
 template int set_smem_attrs_R<DN_R, true>();
 template int set_smem_attrs_R<DN_R, false>();
+template int set_vpipe_attr_R<DN_R, true>();
+template int set_vpipe_attr_R<DN_R, false>();
 #endif
 
 }   // namespace dn

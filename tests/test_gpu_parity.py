@@ -344,15 +344,18 @@ def test_energy_preconditioned_gradient_matches_reference(ep):
             assert O.rel_l2(a, b) < 1e-6, (n, O.rel_l2(a, b))
 
 
-@pytest.mark.parametrize("kernels", ["one-column", "tma"])
+@pytest.mark.parametrize("kernels", ["one-column", "tma", "vpipe"])
 @pytest.mark.parametrize("case", [dict(L=0, fdorder=8, nx=63), dict(L=3, fdorder=8), dict(L=0, fdorder=12, free_surf=0)],
                          ids=["elastic8-odd", "visco8", "elastic12-nofs"])
 def test_alternative_kernels_bitexact(monkeypatch, kernels, case):
-    """The kernels kept beside the default paired-column ones: the one-column
-    register-streaming kernels (DN_PACK=0) and the bulk-copy row pipeline
-    (DN_KERNEL=tma), both bit-identical to the reference."""
+    """The kernels beside the default paired-column ones: the one-column
+    register-streaming kernels (DN_PACK=0), the bulk-copy row pipeline
+    (DN_KERNEL=tma) and the warp-specialised velocity pipeline (DN_VPIPE=1),
+    all bit-identical to the reference."""
     if kernels == "one-column":
         monkeypatch.setenv("DN_PACK", "0")
+    elif kernels == "vpipe":
+        monkeypatch.setenv("DN_VPIPE", "1")
     else:
         monkeypatch.setenv("DN_KERNEL", "tma")
     p, model, src, rec = small_case(**case)
@@ -363,3 +366,64 @@ def test_alternative_kernels_bitexact(monkeypatch, kernels, case):
     for comp in range(2):
         np.testing.assert_array_equal(s.sections(comp), ref.sections(comp), err_msg=f"section {comp}")
     np.testing.assert_array_equal(s.field(2), ref.field(2))
+
+
+@pytest.mark.parametrize("L,ckpt", [(0, 39), (2, 27)], ids=["elastic", "visco-odd-segments"])
+def test_checkpointed_batch_equals_single_shots(L, ckpt):
+    """Checkpointed shots run as one batch (segments of all shots in the same
+    launches; different models and source positions) give, shot for shot, the
+    bit-identical sections and gradients of stored-snapshot runs of each shot alone."""
+    cases = [small_case(L=L, store_snapshots=1, nt=300, seed=sd, nx=72) for sd in (3, 4, 6)]
+    cases = [(p, model, (src[0] + 5 * k,) + tuple(src[1:]), rec) for k, (p, model, src, rec) in enumerate(cases)]
+    want = []
+    for p, model, src, rec in cases:
+        m, s = gpu_shot(p, model, src, rec)
+        dn.run([s], dn.MODE_FORWARD)
+        syn = [s.sections(c) for c in (0, 1)]
+        rvx, rvy = _residuals(p, syn[0], syn[1])
+        s.set_residuals(rvx, rvy, None)
+        dn.run([s], dn.MODE_ADJOINT)
+        s.accumulate_gradient()
+        want.append((syn, m.gradient(), (rvx, rvy)))
+        s.close()
+        m.close()
+    pairs = [gpu_shot(p.replace(ckpt_steps=ckpt), model, src, rec) for p, model, src, rec in cases]
+    shots = [s for _, s in pairs]
+    dn.run(shots, dn.MODE_FORWARD)
+    for (m, s), (syn, _, (rvx, rvy)) in zip(pairs, want):
+        for c in (0, 1):
+            np.testing.assert_array_equal(s.sections(c), syn[c])
+        s.set_residuals(rvx, rvy, None)
+    dn.run(shots, dn.MODE_ADJOINT)
+    for (m, s), (_, g, _) in zip(pairs, want):
+        s.accumulate_gradient()
+        for x, y in zip(m.gradient(), g):
+            np.testing.assert_array_equal(x, y)
+        s.close()
+        m.close()
+
+
+@pytest.mark.parametrize("rows", [0, 7, 32])
+@pytest.mark.parametrize("fdorder,nx,ny", [(8, 300, 70), (12, 257, 41), (2, 131, 33), (6, 64, 48)])
+def test_vpipe_forward_and_gradient_bitexact(monkeypatch, rows, fdorder, nx, ny):
+    """The warp-specialised velocity pipeline over strip heights (automatic, 7 and
+    32 rows: strips that end inside the grid, one strip taller than the grid),
+    several tiles across (nx > 256, odd nx) and every stencil reach: forward
+    sections and the adjoint's gradient bit-identical to the oracle."""
+    monkeypatch.setenv("DN_VPIPE", "1")
+    if rows:
+        monkeypatch.setenv("DN_VPIPE_ROWS", str(rows))
+    p, model, src, rec = small_case(fdorder=fdorder, nx=nx, ny=ny, nt=200, store_snapshots=1)
+    ref = O.Restatement(p, model, src, rec, "f")
+    ref.forward(store=True)
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run([s], dn.MODE_FORWARD)
+    for comp in range(2):
+        np.testing.assert_array_equal(s.sections(comp), ref.sections(comp), err_msg=f"section {comp}")
+    rvx, rvy = _residuals(p, s.sections(0), s.sections(1))
+    s.set_residuals(rvx, rvy, None)
+    ref.adjoint(rvx, rvy, None)
+    dn.run([s], dn.MODE_ADJOINT)
+    s.accumulate_gradient()
+    for a, b in zip(m.gradient(), ref.gradient()):
+        np.testing.assert_array_equal(a, b)
