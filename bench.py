@@ -7,6 +7,17 @@ graph-replayed launch per operation.  Metric: Mcell-updates/s = shots x NX x
 NZ x NT / time.  Inputs (~15 GB resident) are larger than L2, so no flush is
 needed between timed steps.
 
+Beside the headline the JSON line carries the other workloads: `c0` (the
+plain single-shot elastic forward, 600 x 300, NT 5000: batched and plain
+paths, end to end, the reference's own full run on one core and a bitwise
+comparison with it), `elastic` (the 2000 x 600 grid of 64 shots, elastic, NT
+6000), `gradient` (the 1700 x 500, NT 4000, 32-shot FWI gradient with FP16
+snapshots, and on one of its shots the errors of the FP32 gradient against the
+reference's and of the FP16 gradient against the FP64 restatement, both timed
+on the host as CPU baselines), `serving` (the mixed request stream with its
+load calibrated to the measured capacity of the mix) and `fwi_large` (shots of
+the 8000 x 2000, NT 12000 FWI iteration with batched checkpointed adjoints).
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Under torchrun every rank runs its own 64-shot batch (shots are independent:
@@ -46,15 +57,20 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--plain-shots", type=int, default=4)
     ap.add_argument("--cpu-sample-nt", type=int, default=60)
-    ap.add_argument("--serve-requests", type=int, default=32,
+    ap.add_argument("--serve-requests", type=int, default=500,
                     help="requests of the serving workload run after the batch measurement (0: skip)")
+    ap.add_argument("--serve-calibration", type=int, default=48,
+                    help="requests of the closed-loop run that measures the serving capacity of the mix")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="shrinks NX, NZ and NT of served requests")
     ap.add_argument("--gradient-shots", type=int, default=32,
                     help="shots of the FWI-gradient measurement (1700x500, NT 4000, FP16 snapshots; 0: skip)")
-    ap.add_argument("--fwi-large-shots", type=int, default=0,
+    ap.add_argument("--fwi-large-shots", type=int, default=4,
                     help="shots of a sample of the 8000x2000, NT 12000 FWI iteration (0: skip)")
-    ap.add_argument("--elastic-nt", type=int, default=1000,
+    ap.add_argument("--elastic-nt", type=int, default=6000,
                     help="NT of the elastic batch measured beside the viscoelastic one (0: skip)")
+    ap.add_argument("--no-c0", action="store_true", help="skip the plain single-shot elastic workload")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the host runs of the reference and the FP64 restatement beside the GPU work")
     return ap.parse_args()
 
 
@@ -208,6 +224,104 @@ def workload_config(a, p, world):
             "parallelism": f"shots-dp{world}"}
 
 
+class HostJobs:
+    """CPU runs beside the GPU work, in spawned processes started before the
+    timed regions need the host: the reference's own full C0 run (the C0 CPU
+    baseline and its bitwise comparison) and, on one shot of the FWI-gradient
+    workload, the reference's gradient (grad_obj_psv's shot loop: forward with
+    snapshots, calc_res, adjoint, ass_gradPSV) and then the FP64 restatement's
+    gradient with the GPU's adjoint sources.  The C2 runs hold 34 GB (reference)
+    and 68 GB (FP64) of host snapshot arrays one after the other; they are
+    skipped when the host has less memory free."""
+
+    def __init__(self):
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+
+        self.ex = ProcessPoolExecutor(max_workers=2, mp_context=mp.get_context("spawn"))
+        self.futs = {}
+        self.notes = {}
+        self._chain = None
+
+    def c0(self, p, model, src, rec):
+        import config_cases as CC
+
+        self.futs["c0"] = self.ex.submit(CC.ref_forward, p, model, src, rec)
+
+    def c2(self, p, start, shot, obs, residual):
+        import config_cases as CC
+
+        need_ref, need_64 = CC.snapshot_bytes(p, 4), CC.snapshot_bytes(p, 8)
+        avail = CC.available_memory()
+        if avail < 1.3 * need_ref:
+            self.notes["c2"] = f"skipped: {avail / 1e9:.0f} GB of host memory free"
+            return
+        self.futs["c2_ref"] = self.ex.submit(CC.ref_gradient_shot, p, start, shot, obs[0], obs[1])
+
+        def chain():
+            try:
+                self.futs["c2_ref"].result()
+            except Exception:
+                return
+            if CC.available_memory() < 1.3 * need_64:
+                self.notes["c2_fp64"] = "skipped: host memory"
+                return
+            self.futs["c2_fp64"] = self.ex.submit(CC.fp64_gradient, p, start, [shot], [residual], 8)
+
+        self._chain = threading.Thread(target=chain, daemon=True)
+        self._chain.start()
+
+    def result(self, key, timeout=3600):
+        if key == "c2_fp64" and self._chain is not None:
+            self._chain.join(timeout)
+        f = self.futs.get(key)
+        if f is None:
+            return None
+        try:
+            return f.result(timeout=timeout)
+        except Exception as e:      # a failed host run is reported, not fatal
+            self.notes[key] = f"failed: {type(e).__name__}: {e}"[:300]
+            return None
+
+    def close(self):
+        self.ex.shutdown(wait=True, cancel_futures=True)
+
+
+def c2_parity_inputs(device):
+    """Shot 0 of the FWI-gradient workload: observed data of the true model, and the
+    GPU's FP32 and FP16-snapshot gradients with the L2 adjoint sources of its
+    own FP32 forward run (calc_res, oracle/residual_oracle.py, equal to the device
+    residual bit for bit)."""
+    import denise_b200 as dn
+
+    import config_cases as CC
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import residual_oracle as ro
+
+    p, true, start, shots = CC.c2_case()
+    sh = shots[0]
+    mt = dn.Model(p.replace(store_snapshots=0), *true, device=device)
+    s = dn.Shot(mt, *sh)
+    dn.run([s])
+    obs = (s.sections(dn.SEC_VX), s.sections(dn.SEC_VY))
+    s.close()
+    mt.close()
+    grads, res = {}, None
+    for prec in (dn.SNAP_F32, dn.SNAP_F16):
+        m = dn.Model(p.replace(snap_precision=prec), *start, device=device)
+        s = dn.Shot(m, *sh)
+        dn.run([s], dn.MODE_FORWARD)
+        if res is None:
+            res = (ro.calc_res(obs[0], s.sections(dn.SEC_VX), p.dt)[0], ro.calc_res(obs[1], s.sections(dn.SEC_VY), p.dt)[0])
+        s.set_residuals(res[0], res[1], None)
+        dn.run([s], dn.MODE_ADJOINT)
+        s.accumulate_gradient()
+        grads[prec] = m.gradient()
+        s.close()
+        m.close()
+    return p, start, sh, obs, res, grads
+
+
 def run_ours(a, rank, world, local_rank):
     import denise_b200 as dn
     from denise_b200 import synth
@@ -224,13 +338,24 @@ def run_ours(a, rank, world, local_rank):
     device = local_rank
     p = synth.c1_params(nx=a.nx, ny=a.ny, nt=a.nt)
     cells_step = a.shots * p.nx * p.ny * p.nt
+    side = rank == 0 and world == 1      # the side workloads and host baselines: one GPU, rank 0
 
     cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu:
+    if side and not a.no_cpu:
         rate, cores, kind, secs, wall = cpu_sample(p.nx, p.ny, a.cpu_sample_nt)
         cpu = {"value": round(rate, 3), "unit": UNIT, "cores": cores, "kind": kind,
                "sample": f"{cores} concurrent single-rank shots of the {p.nx}x{p.ny} L=3 FDORDER 8 workload, "
                          f"{a.cpu_sample_nt} time steps each ({secs:.1f} s)"}
+
+    jobs, c0case, c2in = None, None, None
+    if side and not a.no_parity:
+        jobs = HostJobs()
+        if not a.no_c0:
+            c0case = synth.c0_case(seed=0)
+            jobs.c0(*c0case)
+        if a.gradient_shots > 0:
+            c2in = c2_parity_inputs(device)
+            jobs.c2(c2in[0], c2in[1], c2in[2], c2in[3], c2in[4])
 
     inputs = build_inputs(p, a.shots, rank * a.shots)
     pairs = create_batch(p, inputs, device)
@@ -296,30 +421,27 @@ def run_ours(a, rank, world, local_rank):
             tp += dn.last_run_stats()[0] / 1e3
         plain_sps = len(plain_shots) / tp
         batched_sps = a.shots * a.steps / t_dev
-        elastic = None
-        if a.elastic_nt > 0:
-            elastic = run_elastic(a, inputs, device, peak)
-        gradient = None
-        if a.gradient_shots > 0:
-            for m_, s_ in pairs:       # the gradient batches need the HBM
-                s_.close()
-                m_.close()
-            gradient = run_gradient(a, device)
-        fwi_large = None
-        if a.fwi_large_shots > 0:
-            for m_, s_ in pairs:
-                s_.close()
-                m_.close()
-            fwi_large = run_fwi_large(a, device)
-        serving = None
-        if a.serve_requests > 0:
-            for m_, s_ in pairs:       # free the batch's HBM for the served requests
-                s_.close()
-                m_.close()
-            serving = run_serving(a, device, value)
         e2e = None
         if not a.no_e2e:
             e2e = run_e2e(p, inputs, device, cells_step)
+        blocks = {}
+        if side:
+            if not a.no_c0:
+                blocks["c0"] = run_c0(a, device, peak, c0case, jobs)
+            if a.elastic_nt > 0:
+                blocks["elastic"] = run_elastic(a, inputs, device, peak)
+            for m_, s_ in pairs:       # the remaining workloads need the HBM
+                s_.close()
+                m_.close()
+            pairs = []
+            if a.gradient_shots > 0:
+                blocks["gradient"] = run_gradient(a, device, c2in, jobs)
+            if a.fwi_large_shots > 0:
+                blocks["fwi_large"] = run_fwi_large(a, device)
+            if a.serve_requests > 0:
+                blocks["serving"] = run_serving(a, device, peak)
+        if jobs is not None:
+            jobs.close()
         result = {
             "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(ms_step, 2), "higher_is_better": True, "scaling": "weak",
@@ -333,14 +455,7 @@ def run_ours(a, rank, world, local_rank):
             "clocks": clk.summary(),
             "wall_s_timed": round(wall, 3),
         }
-        if elastic:
-            result["elastic"] = elastic
-        if serving:
-            result["serving"] = serving
-        if gradient:
-            result["gradient"] = gradient
-        if fwi_large:
-            result["fwi_large"] = fwi_large
+        result.update(blocks)
         if e2e:
             result["e2e"] = e2e
         if cpu:
@@ -354,9 +469,77 @@ def run_ours(a, rank, world, local_rank):
     return result
 
 
+def run_c0(a, device, peak, case, jobs):
+    """The plain elastic forward of one shot: 600 x 300, DH 5 m, DT 0.4 ms, NT 5000,
+    FDORDER 8, CPML 20, free surface, explosive Ricker 10 Hz at (1500 m, 10 m), 120
+    receivers at z = 20 m.  Device time of the batched (graph-replayed) and of the
+    plain (one launch per operation) path, the same end to end through the public
+    API from host arrays, and the reference's own full run on one host core, whose
+    sections the GPU's must equal bit for bit."""
+    import denise_b200 as dn
+    import torch
+    from denise_b200 import synth
+
+    p, model, src, rec = case if case is not None else synth.c0_case(seed=0)
+    cells = p.nx * p.ny * p.nt
+    m = dn.Model(p, *model, device=device)
+    s = dn.Shot(m, *src, *rec)
+    dn.run([s])
+    torch.cuda.synchronize(device)
+    ms = []
+    for _ in range(3):
+        dn.run([s])
+        ms.append(dn.last_run_stats()[0])
+    batched_ms = float(np.median(ms))
+    secs = (s.sections(dn.SEC_VX), s.sections(dn.SEC_VY))
+    pl = []
+    for _ in range(2):
+        dn.run_plain(s)
+        pl.append(dn.last_run_stats()[0])
+    plain_ms = float(np.median(pl))
+    prof = dn.api.profile_steps([s], dn.MODE_FORWARD, nsteps=50)
+    s.close()
+    m.close()
+    # end to end: host set-up and upload, the run, sections read back
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    m = dn.Model(p, *model, device=device)
+    s = dn.Shot(m, *src, *rec)
+    dn.run([s])
+    out = (s.sections(dn.SEC_VX), s.sections(dn.SEC_VY))
+    s.close()
+    m.close()
+    torch.cuda.synchronize(device)
+    e2e_s = time.perf_counter() - t0
+    h2d = 3 * model[0].nbytes + src[2].nbytes + 8 * len(rec[0])
+    d2h = out[0].nbytes + out[1].nbytes
+    blk = {"workload": f"plain elastic forward: one shot, {p.nx}x{p.ny} grid, DH {p.dh} m, DT {p.dt} s, NT {p.nt}, "
+                       "FDORDER 8, FW 20, free surface, 120 receivers",
+           "value": round(cells / (batched_ms * 1e-3) / 1e6, 1), "unit": UNIT,
+           "ms_per_shot": round(batched_ms, 2),
+           "plain_ms_per_shot": round(plain_ms, 2),
+           "plain_value": round(cells / (plain_ms * 1e-3) / 1e6, 1),
+           "shots_per_s": {"batched": round(1e3 / batched_ms, 3), "plain": round(1e3 / plain_ms, 3)},
+           "whole_step_gbs_direct": round(80 * p.nx * p.ny / (sum(prof.values()) * 1e-3) / 1e9, 1),
+           "e2e": {"value": round(cells / e2e_s / 1e6, 1), "unit": UNIT, "seconds": round(e2e_s, 3),
+                   "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}}
+    blk["whole_step_frac"] = round(blk["whole_step_gbs_direct"] / peak, 4)
+    ref = jobs.result("c0") if jobs is not None else None
+    if ref is not None:
+        rvx, rvy, rsec = ref
+        blk["cpu_baseline"] = {"value": round(cells / rsec / 1e6, 3), "unit": UNIT, "cores": 1, "kind": "reference",
+                               "sample": "the reference's own full run of this shot (NT 5000) in one single-rank "
+                                         f"process ({rsec:.1f} s, set-up included)"}
+        blk["sections_bitwise_equal_reference"] = bool(np.array_equal(secs[0], rvx) and np.array_equal(secs[1], rvy))
+    elif jobs is not None and "c0" in jobs.notes:
+        blk["cpu_baseline"] = {"unavailable": jobs.notes["c0"]}
+    return blk
+
+
 def run_elastic(a, inputs, device, peak):
-    """The same shots with the elastic propagator (vp, vs, rho of each model, L = 0) at NT = a.elastic_nt:
-    device time of the batched run, and the elastic step's per-kernel roofline."""
+    """The same 64 shots (the 2000 x 600 grid of the batched workload) with the elastic
+    propagator (vp, vs, rho of each model, L = 0) over the full NT = a.elastic_nt:
+    device time of the batched run and the elastic step's per-kernel roofline."""
     import denise_b200 as dn
     import torch
     from denise_b200 import synth
@@ -370,74 +553,64 @@ def run_elastic(a, inputs, device, peak):
     shots = [s for _, s in pairs]
     dn.run(shots)
     torch.cuda.synchronize(device)
-    ms = 0.0
+    ms = []
     for _ in range(2):
         dn.run(shots)
-        ms += dn.last_run_stats()[0]
-    ms /= 2
+        ms.append(dn.last_run_stats()[0])
+    ms = float(np.mean(ms))
     cells = len(shots) * p.nx * p.ny
     prof = dn.api.profile_steps(shots, dn.MODE_FORWARD, nsteps=20)
     step_ms = sum(prof.values())
-    out = {"value": round(cells * p.nt / (ms * 1e-3) / 1e6, 1), "unit": UNIT, "shots": len(shots), "nt": p.nt,
+    out = {"workload": f"batched elastic forward: {len(shots)} shots x {p.nx}x{p.ny} grid, NT={p.nt}, FDORDER 8, "
+                       "FW 20, free surface, 400 receivers/shot (the models of the batched workload, L = 0)",
+           "value": round(cells * p.nt / (ms * 1e-3) / 1e6, 1), "unit": UNIT, "shots": len(shots), "nt": p.nt,
            "ms_per_run": round(ms, 2),
            "v_kernel_gbs": round(36 * cells / (prof["update_v"] * 1e-3) / 1e9, 1),
            "s_kernel_gbs": round(44 * cells / (prof["update_s"] * 1e-3) / 1e9, 1),
-           "whole_step_gbs_direct": round(80 * cells / (step_ms * 1e-3) / 1e9, 1)}
+           "whole_step_gbs_direct": round(80 * cells / (step_ms * 1e-3) / 1e9, 1),
+           "kernel_ms": {k: round(v, 4) for k, v in prof.items()}}
     out["whole_step_frac"] = round(out["whole_step_gbs_direct"] / peak, 4)
+    out["v_kernel_frac"] = round(out["v_kernel_gbs"] / peak, 4)
     for m, s in pairs:
         s.close()
         m.close()
     return out
 
 
-def run_gradient(a, device):
+def run_gradient(a, device, c2in, jobs):
     """FWI gradient (forward with snapshots + adjoint) of the 1700 x 500 elastic workload:
     true model = the seeded family (seed 2), starting model = it smoothed with sigma 25
     cells, observed data synthesised on the GPU from the true model; FP16 snapshots
-    every 2 steps; shots streamed through HBM in batches that fit."""
-    import ctypes
-
+    every 2 steps; shots streamed through HBM in the batches shard.memory_batches
+    gives (as many as 90 % of the free HBM holds, spread evenly).  On shot 0: the
+    errors of the GPU's FP32 gradient against the reference's own and of its
+    FP16-snapshot gradient against the FP64 restatement, both host runs timed."""
     import denise_b200 as dn
     import torch
-    from denise_b200 import synth
+    from denise_b200 import shard
 
+    import config_cases as CC
     import oracles as O
 
-    p = synth.c2_params(snap_precision=dn.SNAP_F16)
     n = a.gradient_shots
-    vpt, vst, rhot = synth.base_model(p.nx, p.ny, p.dh, 2)
-    start = tuple(synth.smoothed(x, 25.0) for x in (vpt, vst, rhot))
-    xmax = (p.nx - 1) * p.dh
-    sig = synth.ricker_source(p, 8.0)[None, :]
-    ri, rj = synth.receivers_line(100.0, xmax - 100.0, 400, 20.0, p.dh)
-    shots = [(np.array([synth.grid_index(200.0 + (xmax - 400.0) * k / max(n - 1, 1), p.dh)], np.int32),
-              np.array([max(synth.grid_index(10.0, p.dh), 1)], np.int32), sig, ri, rj) for k in range(n)]
-    # observed data from the true model (batched forward, no snapshots)
-    mt = dn.Model(p.replace(store_snapshots=0), vpt, vst, rhot, device=device)
+    p, true, start, shots = CC.c2_case(nshots=n, snap_precision=dn.SNAP_F16)
+    mt = dn.Model(p.replace(store_snapshots=0), *true, device=device)
     st_ = [dn.Shot(mt, *sh) for sh in shots]
     dn.run(st_)
     obs = [(s.sections(dn.SEC_VX), s.sections(dn.SEC_VY)) for s in st_]
     for s in st_:
         s.close()
     mt.close()
-    fp = ctypes.c_size_t()
-    pc = p.to_c()
-    dn._lib.check(dn._lib.lib.dn_shot_footprint(ctypes.byref(pc), len(ri), 1, ctypes.byref(fp)))
-    free, total = dn.device_memory(device)
-    # as many shots per batch as 90 % of the free HBM holds, spread evenly over the
-    # batches (32 shots: 4 x 8 rather than 4 x 7 + 4; larger batches run faster per shot)
-    most = max(1, min(n, int(0.9 * free / fp.value)))
-    nbatch = -(-n // most)
-    batch = -(-n // nbatch)
 
     def grad(params, idx):
         m = dn.Model(params, *start, device=device)
-        L2, dev_ms = 0.0, 0.0
-        for b0 in range(0, len(idx), batch):
-            ss = [dn.Shot(m, *shots[k]) for k in idx[b0:b0 + batch]]
+        L2, dev_ms, nb = 0.0, 0.0, []
+        for part in shard.memory_batches(params, shots, idx, 1, device):
+            nb.append(len(part))
+            ss = [dn.Shot(m, *shots[k]) for k in part]
             dn.run(ss, dn.MODE_FORWARD)
             dev_ms += dn.last_run_stats()[0]
-            for s, k in zip(ss, idx[b0:b0 + batch]):
+            for s, k in zip(ss, part):
                 L2 += s.residual(obs[k][0], dn.SEC_VX) + s.residual(obs[k][1], dn.SEC_VY)
             dn.run(ss, dn.MODE_ADJOINT)
             dev_ms += dn.last_run_stats()[0]
@@ -446,25 +619,50 @@ def run_gradient(a, device):
                 s.close()
         g = m.gradient()
         m.close()
-        return g, L2, dev_ms
+        return g, L2, dev_ms, nb
 
     grad(p, [0])                                   # warm-up (graphs, module load)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
-    g16, L2, dev_ms = grad(p, list(range(n)))
+    g16, L2, dev_ms, nb = grad(p, list(range(n)))
     torch.cuda.synchronize(device)
     wall = time.perf_counter() - t0
     cells = n * p.nx * p.ny * p.nt * 2
-    g32, _, _ = grad(p.replace(snap_precision=dn.SNAP_F32), [0, n // 2])
-    g16s, _, _ = grad(p, [0, n // 2])
+    g32, _, _, _ = grad(p.replace(snap_precision=dn.SNAP_F32), [0, n // 2])
+    g16s, _, _, _ = grad(p, [0, n // 2])
     err = max(O.rel_l2(x, y) for x, y in zip(g16s, g32))
-    return {"workload": f"FWI gradient, elastic {p.nx}x{p.ny}, DH {p.dh} m, DT {p.dt} s, NT {p.nt}, FDORDER 8, "
-                        f"{n} shots x 400 receivers, FP16 snapshots every DTINV={p.dtinv} steps, "
-                        "starting model smoothed sigma 25 cells, observed data synthesised on the GPU",
-            "shots": n, "batch_shots": batch, "seconds": round(wall, 2),
-            "device_ms": round(dev_ms, 1), "shots_per_s": round(n / wall, 3),
-            "mcell_updates_per_s": round(cells / wall / 1e6, 1),
-            "misfit": L2, "fp16_vs_fp32_gradient_rel_l2": float(err)}
+    out = {"workload": f"FWI gradient, elastic {p.nx}x{p.ny}, DH {p.dh} m, DT {p.dt} s, NT {p.nt}, FDORDER 8, "
+                       f"{n} shots x 400 receivers, FP16 snapshots every DTINV={p.dtinv} steps, "
+                       "starting model smoothed sigma 25 cells, observed data synthesised on the GPU",
+           "shots": n, "batches": nb, "seconds": round(wall, 2),
+           "device_ms": round(dev_ms, 1), "shots_per_s": round(n / wall, 3),
+           "mcell_updates_per_s": round(cells / wall / 1e6, 1),
+           "misfit": L2, "fp16_vs_fp32_gradient_rel_l2": float(err)}
+    if c2in is not None and jobs is not None:
+        grads = c2in[5]
+        cs = p.nx * p.ny * p.nt * 2
+        ref = jobs.result("c2_ref")
+        base = []
+        if ref is not None:
+            out["fp32_vs_reference_rel_l2"] = float(max(O.rel_l2(x, y) for x, y in zip(grads[dn.SNAP_F32], ref[:3])))
+            out["fp32_bitwise_equal_reference"] = bool(all(np.array_equal(x, y)
+                                                            for x, y in zip(grads[dn.SNAP_F32], ref[:3])))
+            base.append({"value": round(cs / ref[4] / 1e6, 3), "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": "the reference's own gradient of shot 0 of this workload (forward with "
+                                   f"snapshots, calc_res, adjoint, ass_gradPSV) in one process, {ref[4]:.0f} s"})
+        f64 = jobs.result("c2_fp64")
+        if f64 is not None:
+            out["fp16_vs_fp64_oracle_rel_l2"] = float(max(O.rel_l2(x, y) for x, y in zip(grads[dn.SNAP_F16], f64[:3])))
+            out["fp32_vs_fp64_oracle_rel_l2"] = float(max(O.rel_l2(x, y) for x, y in zip(grads[dn.SNAP_F32], f64[:3])))
+            base.append({"value": round(cs / f64[3] / 1e6, 3), "unit": UNIT, "cores": 8, "kind": "port",
+                         "sample": "the FP64 restatement of the scheme (oracle/psv_oracle) on shot 0, 8 threads, "
+                                   f"{f64[3]:.0f} s"})
+        if base:
+            out["cpu_baseline"] = base
+        for k in ("c2", "c2_ref", "c2_fp64"):
+            if k in jobs.notes:
+                out.setdefault("host_runs", {})[k] = jobs.notes[k]
+    return out
 
 
 def run_fwi_large(a, device):
@@ -473,7 +671,8 @@ def run_fwi_large(a, device):
     96-shot line with 1600 receivers; true model = the seeded family (seed 4) plus a
     5500 m/s ellipse, starting model smoothed with sigma 25 cells; one FWI iteration
     with FP16 snapshots every 4 steps and checkpointed adjoints (segments of 400
-    steps), the FP64 L-BFGS direction, the parabolic step search and the update."""
+    steps) run as one batch, the reference's L-BFGS, the parabolic step search
+    and the update."""
     import denise_b200 as dn
     from denise_b200 import fwi, synth
     from denise_b200.api import PsvParams
@@ -513,12 +712,13 @@ def run_fwi_large(a, device):
     per_shot_grad = h["gradient_s"] / n
     per_shot_fwd = fwd_ms / 1e3 / n
     return {"workload": "FWI iteration sample: elastic 8000x2000, DH 2.5 m, DT 0.2 ms, NT 12000, FDORDER 8, "
-                        f"{n} of 96 shots x 1600 receivers, FP16 snapshots every 4 steps, checkpointed adjoint "
-                        "(400-step segments), FP64 L-BFGS, parabolic step search",
+                        f"{n} of 96 shots x 1600 receivers in one batch, FP16 snapshots every 4 steps, checkpointed "
+                        "adjoint (400-step segments), the reference's L-BFGS, parabolic step search",
             "shots": n, "setup_s": round(t1 - t0, 1), "observed_data_s": round(t2 - t1, 1),
             "forward_device_s_per_shot": round(per_shot_fwd, 2),
             "forward_mcell_updates_per_s": round(cells / per_shot_fwd / 1e6, 1),
             "gradient_s": round(h["gradient_s"], 1), "gradient_s_per_shot": round(per_shot_grad, 2),
+            "gradient_mcell_updates_per_s": round(2 * cells * n / h["gradient_s"] / 1e6, 1),
             "optimizer_s": round(h["optimizer_s"], 3), "step_search_s": round(h["step_search_s"], 1),
             "test_models": h["test_models"], "step_found": h["found"], "eps": h["eps"],
             "misfit_before": L2, "misfit_after": L2_new,
@@ -526,47 +726,85 @@ def run_fwi_large(a, device):
             "iteration_96_shots_estimate_s": round(96 * per_shot_grad + h["test_models"] * 96 * per_shot_fwd, 0)}
 
 
-def run_serving(a, device, mcells_per_s):
-    """The serving workload: requests arrive as a Poisson process at 1.2x the
-    capacity implied by the batched throughput just measured; the server admits
-    them by HBM footprint into its run queues.  Latency = scheduled arrival ->
-    result on the host."""
+def _request_bytes(kind, p, nshots):
+    """Algorithmic HBM bytes of a request: 80 B per elastic and (23 + 6L) 4 B per
+    viscoelastic cell-update; a gradient adds its adjoint (96 B per cell-update)
+    and per snapshot 5 s_b (store) plus 5 s_b + 8 + 6 g_b (correlation) bytes per
+    cell, FP16 snapshots (s_b = 2) and float accumulators (g_b = 4)."""
+    c = p.nx * p.ny
+    fwd = (80 if p.L == 0 else (23 + 6 * p.L) * 4) * c * p.nt
+    if kind != "gradient":
+        return fwd * nshots
+    nsnap = -(-p.nt // max(p.dtinv, 1))
+    return (fwd + c * (96 * p.nt + nsnap * (10 + 10 + 8 + 24))) * nshots
+
+
+def run_serving(a, device, peak):
+    """The serving workload (2000 requests in the full stream; a.serve_requests of
+    it here): requests of the mix arrive as a Poisson process at 1.2x the
+    capacity of that mix, measured first by a closed-loop run of
+    a.serve_calibration requests of another seed (all submitted at once); the
+    server admits them by HBM footprint into its run queues.  Latency =
+    scheduled arrival -> result on the host.  The HBM fraction is the mix's
+    algorithmic bytes over the wall time of the stream."""
+    from concurrent.futures import ThreadPoolExecutor
+
     from denise_b200 import serve, synth
 
-    reqs = synth.serve_requests(a.serve_requests, seed=3, scale=a.serve_scale)
-    work = []
-    for kind, p, model, shots, obs in reqs:
-        w = p.nx * p.ny * p.nt * len(shots)
-        work.append(2 * w if kind == "gradient" else w)
-    rate = 1.2 * mcells_per_s * 1e6 / float(np.mean(work))      # requests per second
+    def make(n, seed):
+        # the models of the stream are drawn in parallel threads (scipy releases the GIL)
+        chunks = [(k, min(k + 16, n)) for k in range(0, n, 16)]
+        with ThreadPoolExecutor(max_workers=8) as ex:
+            parts = list(ex.map(lambda c: synth.serve_requests(n, seed=seed, scale=a.serve_scale, first=c[0],
+                                                                 last=c[1]), chunks))
+        return [r for part in parts for r in part]
+
+    def drive(reqs, arrivals):
+        srv = serve.Server(device=device, chunk=50)
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(reqs) or not srv.idle():
+            now = time.perf_counter() - t0
+            while i < len(reqs) and arrivals[i] <= now:
+                kind, p, model, shots, obs = reqs[i]
+                srv.submit(serve.Request(kind, p, model, shots, obs, rid=i), now=t0 + arrivals[i])
+                i += 1
+            if srv.idle():
+                time.sleep(max(0.0, min(0.05, arrivals[i] - (time.perf_counter() - t0))))
+                continue
+            srv.step()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        bad = sum(1 for r in srv.results if r.status != 0)
+        return wall, st, bad
+
+    cal = make(a.serve_calibration, 33)
+    cal_wall, _, _ = drive(cal, np.zeros(len(cal)))
+    capacity = len(cal) / cal_wall                                    # requests per second, closed loop
+    cal_bytes = sum(_request_bytes(k, p, len(sh)) for k, p, _, sh, _ in cal)
+    del cal
+    reqs = make(a.serve_requests, 3)
+    work = [p.nx * p.ny * p.nt * len(sh) * (2 if k == "gradient" else 1) for k, p, _, sh, _ in reqs]
+    nbytes = sum(_request_bytes(k, p, len(sh)) for k, p, _, sh, _ in reqs)
+    rate = 1.2 * capacity
     rng = np.random.default_rng(3)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
-    srv = serve.Server(device=device, chunk=50)
-    t0 = time.perf_counter()
-    i = 0
-    while i < len(reqs) or not srv.idle():
-        now = time.perf_counter() - t0
-        while i < len(reqs) and arrivals[i] <= now:
-            kind, p, model, shots, obs = reqs[i]
-            srv.submit(serve.Request(kind, p, model, shots, obs, rid=i), now=t0 + arrivals[i])
-            i += 1
-        if srv.idle():
-            time.sleep(max(0.0, min(0.05, arrivals[i] - (time.perf_counter() - t0))))
-            continue
-        srv.step()
-    wall = time.perf_counter() - t0
-    st = srv.stats()
-    srv.close()
-    bad = sum(1 for r in srv.results if r.status != 0)
+    wall, st, bad = drive(reqs, arrivals)
     return {"requests": len(reqs), "failed": bad, "p50_latency_s": round(st["p50_s"], 3),
             "p99_latency_s": round(st["p99_s"], 3), "shots_per_s": round(st["shots_done_total"] / wall, 3),
             "mcell_updates_per_s": round(sum(work) / wall / 1e6, 1), "wall_s": round(wall, 2),
-            "arrival_rate_per_s": round(rate, 3), "max_running_shots": st["max_running_shots"],
-            "joins_while_running": st["joins_while_running"],
+            "hbm_gbs": round(nbytes / wall / 1e9, 1), "hbm_frac": round(nbytes / wall / 1e9 / peak, 4),
+            "arrival_rate_per_s": round(rate, 3),
+            "capacity": {"requests_per_s": round(capacity, 3), "requests": a.serve_calibration,
+                         "wall_s": round(cal_wall, 2), "hbm_frac": round(cal_bytes / cal_wall / 1e9 / peak, 4),
+                         "how": "closed loop: all requests of a seed-33 stream submitted at once"},
+            "max_running_shots": st["max_running_shots"], "joins_while_running": st["joins_while_running"],
             "workload": "seeded serving mix: 70% elastic forward, 20% visco L=3 forward, 10% elastic FWI gradient "
                         "(FP16 snapshots); NX 300-3000, NZ 150-1000, NT 2000-8000 (x scale "
                         f"{a.serve_scale}), FDORDER 4/8/12, 1-4 shots, 50-500 receivers; Poisson arrivals at 1.2x "
-                        "the batched capacity"}
+                        "the measured capacity of the mix; the first "
+                        f"{a.serve_requests} of the 2000-request stream"}
 
 
 def run_e2e(p, inputs, device, cells_step):

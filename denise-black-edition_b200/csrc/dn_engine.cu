@@ -167,6 +167,7 @@ struct dn_shot {
     void *d_snap = nullptr;
     float *d_snap_scale = nullptr;
     int nsnap = 0, zch = 16, bx = 128, tiles_x = 0, tiles = 0;
+    int kern = DN_KERN_PAIRED;     // stencil kernel variant (the batch runs its first shot's)
     void *d_acc = nullptr;         // wc, wcu, wcrho (float or double) + Ws, Wr
     int acc64;
     int *d_flag = nullptr;
@@ -472,14 +473,17 @@ struct TileRule {
     int fdorder, L;
     long long cells_min, cells_max;
     int bx, zch;
+    int store;     // -1: any shot; 0 / 1: shots that do not / do store snapshots
+    int variant;   // DN_KERN_* stencil kernels (register blocking); -1: the default
 };
 static std::mutex g_tile_mu;
 static std::vector<TileRule> g_tile_rules;
 
 static bool tile_ok(int bx, int zch) { return bx >= 32 && bx <= 256 && (bx % 32) == 0 && zch >= 1 && zch <= 256; }
 
-static void tile_shape(const dn_params *p, int &bx, int &zch)
+static void tile_choice(const dn_params *p, int &bx, int &zch, int &variant)
 {
+    variant = DN_KERN_PAIRED;
     // default tiles: 128 x 8 for forward runs; 128 x 4 for shots that store
     // snapshots (more blocks for the gradient's smaller batches: the 7-shot
     // 1700 x 500 FP16 forward + adjoint ran 449 ms per 1000 steps at 128 x 8 and
@@ -490,9 +494,11 @@ static void tile_shape(const dn_params *p, int &bx, int &zch)
     {
         std::lock_guard<std::mutex> lk(g_tile_mu);
         for (const TileRule &r : g_tile_rules)
-            if (r.fdorder == p->fdorder && r.L == p->L && cells >= r.cells_min && cells <= r.cells_max) {
+            if (r.fdorder == p->fdorder && r.L == p->L && cells >= r.cells_min && cells <= r.cells_max &&
+                (r.store < 0 || r.store == (p->store_snapshots ? 1 : 0))) {
                 bx = r.bx;
                 zch = r.zch;
+                if (r.variant >= 0) variant = r.variant;
             }
     }
     const char *ev = getenv("DN_TILE");
@@ -505,21 +511,38 @@ static void tile_shape(const dn_params *p, int &bx, int &zch)
     }
 }
 
-extern "C" int dn_set_tile_shape(int fdorder, int L, long long cells_min, long long cells_max, int bx, int zch)
+static void tile_shape(const dn_params *p, int &bx, int &zch)
 {
-    if (fdorder < 2 || fdorder > 12 || (fdorder % 2) || L < 0 || L > DN_MAX_L || cells_min > cells_max)
-        return dn_fail(DN_EINVAL, "dn_set_tile_shape: bad class");
+    int v;
+    tile_choice(p, bx, zch, v);
+}
+
+extern "C" int dn_set_kernel_rule(int fdorder, int L, int store, long long cells_min, long long cells_max, int bx,
+                                  int zch, int variant)
+{
+    if (fdorder < 2 || fdorder > 12 || (fdorder % 2) || L < 0 || L > DN_MAX_L || cells_min > cells_max ||
+        store < -1 || store > 1)
+        return dn_fail(DN_EINVAL, "dn_set_kernel_rule: bad class");
     if (!tile_ok(bx, zch))
-        return dn_fail(DN_EINVAL, "dn_set_tile_shape: %d x %d (width a multiple of 32 up to 256, 1-256 rows)", bx, zch);
+        return dn_fail(DN_EINVAL, "dn_set_kernel_rule: %d x %d (width a multiple of 32 up to 256, 1-256 rows)", bx,
+                       zch);
+    if (variant < -1 || variant > DN_KERN_VPIPE) return dn_fail(DN_EINVAL, "dn_set_kernel_rule: variant %d", variant);
     std::lock_guard<std::mutex> lk(g_tile_mu);
     for (TileRule &r : g_tile_rules)
-        if (r.fdorder == fdorder && r.L == L && r.cells_min == cells_min && r.cells_max == cells_max) {
+        if (r.fdorder == fdorder && r.L == L && r.cells_min == cells_min && r.cells_max == cells_max &&
+            r.store == store) {
             r.bx = bx;
             r.zch = zch;
+            r.variant = variant;
             return DN_OK;
         }
-    g_tile_rules.push_back({fdorder, L, cells_min, cells_max, bx, zch});
+    g_tile_rules.push_back({fdorder, L, cells_min, cells_max, bx, zch, store, variant});
     return DN_OK;
+}
+
+extern "C" int dn_set_tile_shape(int fdorder, int L, long long cells_min, long long cells_max, int bx, int zch)
+{
+    return dn_set_kernel_rule(fdorder, L, -1, cells_min, cells_max, bx, zch, -1);
 }
 
 extern "C" int dn_clear_tile_shapes(void)
@@ -533,6 +556,13 @@ extern "C" int dn_get_tile_shape(const dn_params *p, int *bx, int *zch)
 {
     if (!p || !bx || !zch) return dn_fail(DN_EINVAL, "dn_get_tile_shape: null argument");
     tile_shape(p, *bx, *zch);
+    return DN_OK;
+}
+
+extern "C" int dn_get_kernel_choice(const dn_params *p, int *bx, int *zch, int *variant)
+{
+    if (!p || !bx || !zch || !variant) return dn_fail(DN_EINVAL, "dn_get_kernel_choice: null argument");
+    tile_choice(p, *bx, *zch, *variant);
     return DN_OK;
 }
 
@@ -618,7 +648,7 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
     s->rec_i.assign(acq->rec_i, acq->rec_i + acq->ntr);
     s->rec_j.assign(acq->rec_j, acq->rec_j + acq->ntr);
     s->quelltyp_last = acq->nsrc > 0 ? s->src_type[acq->nsrc - 1] : 0;
-    tile_shape(p, s->bx, s->zch);
+    tile_choice(p, s->bx, s->zch, s->kern);
     shot_counts(p, s->bx, s->zch, s->tiles_x, s->tiles, s->nsnap);
     s->acc64 = p->grad_accum == DN_ACC_F64;
 
@@ -1012,13 +1042,15 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c, con
     c.L = p0.L;
     c.exact = p0.arith == DN_ARITH_EXACT;
     c.bx = shots[0]->bx;
-    // stencil kernels: register streaming (default, fastest measured on B200) or, with
-    // DN_KERNEL=tma, the bulk-copy row pipeline of dn_kernels_tma.cuh
+    // stencil kernels of the batch: the variant of its first shot (tile rules, measured by
+    // the autotuner; results do not depend on it); environment overrides: DN_KERNEL=tma the
+    // bulk-copy row pipeline of dn_kernels_tma.cuh, DN_PACK=0 the one-column kernels,
+    // DN_VPIPE=1 / 0 the pipelined velocity kernel on / off
     const char *kern = getenv("DN_KERNEL");
     c.tma = c.bx == TMA_W && kern && strcmp(kern, "tma") == 0;
-    // paired-column FP32x2 kernels (default; DN_PACK=0 selects the one-column kernels)
     const char *pk = getenv("DN_PACK");
-    c.pack = !c.tma && !(pk && strcmp(pk, "0") == 0);
+    c.pack = !c.tma && shots[0]->kern != DN_KERN_COLUMN;
+    if (pk) c.pack = !c.tma && strcmp(pk, "0") != 0;
     c.any_surf = c.any_src_s = c.any_store = c.any_adj = c.any_rec = false;
     int maxtiles = 0, maxsrc = 1, maxnx = 1, maxtr = 1;
     for (int k = 0; k < n; k++) {
@@ -1049,7 +1081,8 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c, con
     // pipelined velocity kernel (DN_VPIPE=1): strips of VP_W columns, about four CTAs per
     // resident slot (148 SMs x 3) over the batch, at least 32 rows tall (DN_VPIPE_ROWS sets it)
     const char *vp = getenv("DN_VPIPE");
-    c.vpipe = vp && strcmp(vp, "1") == 0;
+    c.vpipe = !c.tma && shots[0]->kern == DN_KERN_VPIPE;
+    if (vp) c.vpipe = !c.tma && strcmp(vp, "1") == 0;
     c.vsh = 0;
     c.vgrid = dim3(1, n);
     if (c.vpipe) {

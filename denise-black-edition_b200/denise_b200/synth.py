@@ -83,7 +83,7 @@ def c2_params(**kw):
 SERVE_MIX = (("forward", 0, 0.7), ("forward", 3, 0.2), ("gradient", 0, 0.1))   # kind, L, share
 
 
-def serve_requests(n, seed=3, scale=1.0, snap_budget=16e9):
+def serve_requests(n, seed=3, scale=1.0, snap_budget=16e9, first=0, last=None):
     """n requests: 70 % elastic forward, 20 % viscoelastic (L = 3) forward, 10 %
     elastic FWI gradients; NX in U[300, 3000], NZ in U[150, 1000], DH in U[5, 10],
     NT in U[2000, 8000], FDORDER in {4, 8, 12}, 1-4 shots and 50-500 receivers
@@ -92,12 +92,15 @@ def serve_requests(n, seed=3, scale=1.0, snap_budget=16e9):
     runs.  Gradient requests store FP16 snapshots every DTINV steps, DTINV the
     smallest even interval that keeps one shot's snapshots under snap_budget
     bytes; their observed data are zero traces.  Returns (kind, params, model,
-    shots, obs) tuples; shots are (src_i, src_j, signals, rec_i, rec_j)."""
+    shots, obs) tuples; shots are (src_i, src_j, signals, rec_i, rec_j).
+    first, last: build only requests first .. last - 1 of the n-request stream
+    (the same requests as in the whole stream), e.g. to build it in parallel."""
     from .api import cfl_limit
 
     rng = np.random.default_rng(seed)
     kinds = rng.choice(len(SERVE_MIX), size=n, p=[m[2] for m in SERVE_MIX])
     out = []
+    last = n if last is None else min(last, n)
     for k in range(n):
         kind, L, _ = SERVE_MIX[kinds[k]]
         nx = max(60, int(rng.integers(300, 3001) * scale))
@@ -107,6 +110,8 @@ def serve_requests(n, seed=3, scale=1.0, snap_budget=16e9):
         fdorder = int(rng.choice([4, 8, 12]))
         nshots = int(rng.integers(1, 5))
         nrec = int(rng.integers(50, 501))
+        if not first <= k < last:
+            continue
         vp, vs, rho = base_model(nx, ny, dh, 1000 + k, smooth_sigma=4.0)
         model = (vp, vs, rho)
         kw = dict(nx=nx, ny=ny, dh=dh, nt=nt, fdorder=fdorder, maxrelerror=1, free_surf=1, fw=20,

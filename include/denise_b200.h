@@ -427,6 +427,18 @@ int dn_set_tile_shape(int fdorder, int L, long long cells_min, long long cells_m
 int dn_clear_tile_shapes(void);
 /* the tile shape a new shot with these parameters gets */
 int dn_get_tile_shape(const dn_params *p, int *bx, int *zch);
+/* Stencil kernel variants (the register blocking of the stencil kernels; no
+ * counterpart in the reference, whose loops have one form): */
+#define DN_KERN_PAIRED 0   /* two adjacent columns per thread, packed FP32x2 arithmetic (default) */
+#define DN_KERN_COLUMN 1   /* one column per thread, z stencils in register windows */
+#define DN_KERN_VPIPE 2    /* paired, with the velocity update fed by a warp-specialised copy pipeline */
+/* A rule as dn_set_tile_shape's, for shots that store snapshots (store 1), that
+ * do not (0) or both (-1), which also picks the kernel variant (-1: default).
+ * A batch runs the variant of its first shot. */
+int dn_set_kernel_rule(int fdorder, int L, int store, long long cells_min, long long cells_max, int bx, int zch,
+                       int variant);
+/* the tile shape and kernel variant a new shot with these parameters gets */
+int dn_get_kernel_choice(const dn_params *p, int *bx, int *zch, int *variant);
 
 /* ---- FWI outer loop (FP64) ------------------------------------------------- */
 /* Deterministic FP64 dot product of two device vectors (fixed reduction order). */
