@@ -21,6 +21,8 @@ BUILD = os.path.join(HERE, "_build")
 INC = os.path.join(ROOT, "include")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+# extra nvcc flags, e.g. a kernel tuning macro for a measurement build (-DDN_PF2_ROWS=4)
+EXTRA_NVCC = os.environ.get("DN_NVCC_FLAGS", "").split()
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_CFLAGS = ["-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-Wno-unused-function"]
 
@@ -55,7 +57,7 @@ def build(verbose=True):
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if _newer(o, [s] + headers):
-            jobs.append([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
+            jobs.append([NVCC] + ARCH + EXTRA_NVCC + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
                                          "-I", INC, "-I", CSRC, "-c", s, "-o", o])
         objs.append(o)
     # the CUDA translation units are independent: compile them concurrently

@@ -7,7 +7,9 @@
  * TS = 1 / max fc) and the receiver table; one shot per line of the source
  * table, firing that source (RUN_MULTIPLE_SHOTS = 1) or all of them; a wavelet per
  * source (wavelet.c); the shot run; the seismograms written as
- * saveseis_glob.c names them.  The difference is that the shots run as
+ * saveseis_glob.c names them, in SEIS_FORMAT 1 (SU), 2 (ASCII) or 3 (binary);
+ * receivers from REC_FILE.dat, or per shot from REC_FILE_shot_<n>.dat with
+ * READREC 2 (receiver.c:32-41).  The difference is that the shots run as
  * batches through one launch sequence, as many per batch as the device's free
  * memory holds.
  */
@@ -33,6 +35,18 @@ static void free_src(shot_src *s)
     free(s->azi);
     free(s->sig);
     memset(s, 0, sizeof(*s));
+}
+
+/* receivers of shot `ishot` (1-based): REC_FILE.dat for READREC 1, REC_FILE_shot_<ishot>.dat
+ * for READREC 2 (receiver.c:32-41) */
+static int read_shot_receivers(const dn_inp *in, int ishot, int *ntr, int **ri, int **rj)
+{
+    char rpath[2 * DN_STR + 32];
+    if (in->readrec == 2)
+        snprintf(rpath, sizeof(rpath), "%s_shot_%i.dat", in->rec_file, ishot);
+    else
+        snprintf(rpath, sizeof(rpath), "%s.dat", in->rec_file);
+    return dn_read_receivers(rpath, in->refrec, in->dh, ntr, ri, rj);
 }
 
 /* sources of shot `k` (0-based) in grid indices, with their wavelets (wavelet.c;
@@ -124,8 +138,8 @@ static int write_shot(const dn_inp *in, const dn_params *p, dn_shot *shot, int i
         snprintf(path, sizeof(path), "%s.shot%d", base, ishot);
         int st = dn_shot_get_sections(shot, COMPS[c].comp, buf);
         if (!st)
-            st = dn_write_su(path, buf, ntr, p->nt, in->ndt > 0 ? in->ndt : 1, p->dt, in->time, p->dh, ri, rj,
-                             in->refrec, src->xs, src->ys);
+            st = dn_write_seis(path, in->seis_format, buf, ntr, p->nt, in->ndt > 0 ? in->ndt : 1, p->dt, in->time,
+                               p->dh, ri, rj, in->refrec, src->xs, src->ys);
         if (st) return st;
     }
     return DN_OK;
@@ -139,11 +153,14 @@ int dn_forward_inp(const char *inp_path, int device)
     if (in.physics != 1) return dn_fail(DN_ENOTSUP, "PHYSICS=%d: only 2-D P-SV (1) is built", in.physics);
     if (in.readmod != 1) return dn_fail(DN_ENOTSUP, "READMOD=%d: models are read from MFILE (READMOD=1)", in.readmod);
     if (in.srcrec != 1) return dn_fail(DN_ENOTSUP, "SRCREC=%d: sources are read from SOURCE_FILE (SRCREC=1)", in.srcrec);
-    if (in.readrec != 1) return dn_fail(DN_ENOTSUP, "READREC=%d: receivers are read from one REC_FILE (READREC=1)", in.readrec);
-    if (in.seis_format != 1) return dn_fail(DN_ENOTSUP, "SEIS_FORMAT=%d: SU output (1) is built", in.seis_format);
+    if (in.readrec != 1 && in.readrec != 2)
+        return dn_fail(DN_ENOTSUP, "READREC=%d: receivers are read from REC_FILE (1) or per shot (2)", in.readrec);
+    if (in.seis_format < 1 || in.seis_format > 3)
+        return dn_fail(DN_EINVAL, "SEIS_FORMAT=%d: SU (1), ASCII (2) or binary (3)", in.seis_format);
     if (in.seismo < 1 || in.seismo > 4) return dn_fail(DN_EINVAL, "SEISMO=%d: nothing to record", in.seismo);
 
-    int nsrc = 0, ntr = 0, *ri = NULL, *rj = NULL;
+    int nsrc = 0, ntr = 0, *ri = NULL, *rj = NULL, maxtr = 0;
+    int *sntr = NULL, **sri = NULL, **srj = NULL;   /* per-shot receivers (READREC 2) */
     float *srcpos = NULL, ts = in.ts;
     float *mod[5] = {NULL, NULL, NULL, NULL, NULL};
     dn_model *model = NULL;
@@ -153,9 +170,18 @@ int dn_forward_inp(const char *inp_path, int device)
     int nshots = 0;
 
     st = dn_read_sources(in.source_file, &nsrc, &srcpos, &ts);
-    char rpath[2 * DN_STR];
-    snprintf(rpath, sizeof(rpath), "%s.dat", in.rec_file);
-    if (!st) st = dn_read_receivers(rpath, in.refrec, in.dh, &ntr, &ri, &rj);
+    if (!st && in.readrec == 1) st = read_shot_receivers(&in, 1, &ntr, &ri, &rj);
+    maxtr = ntr;
+    if (!st && in.readrec == 2) {
+        sntr = (int *)calloc((size_t)(nsrc > 0 ? nsrc : 1), sizeof(int));
+        sri = (int **)calloc((size_t)(nsrc > 0 ? nsrc : 1), sizeof(int *));
+        srj = (int **)calloc((size_t)(nsrc > 0 ? nsrc : 1), sizeof(int *));
+        if (!sntr || !sri || !srj) st = dn_fail(DN_ENOMEM, "driver: out of memory");
+        for (int k = 0; k < nsrc && !st; k++) {
+            st = read_shot_receivers(&in, k + 1, &sntr[k], &sri[k], &srj[k]);
+            if (!st && sntr[k] > maxtr) maxtr = sntr[k];
+        }
+    }
     dn_params p;
     if (!st) st = dn_inp_params(&in, ts, &p);
     if (!st) {
@@ -179,14 +205,14 @@ int dn_forward_inp(const char *inp_path, int device)
         nshots = nsrc;
         shots = (dn_shot **)calloc((size_t)nshots, sizeof(dn_shot *));
         srcs = (shot_src *)calloc((size_t)nshots, sizeof(shot_src));
-        buf = (float *)malloc(sizeof(float) * (size_t)(ntr > 0 ? ntr : 1) * p.nt);
+        buf = (float *)malloc(sizeof(float) * (size_t)(maxtr > 0 ? maxtr : 1) * p.nt);
         if (!shots || !srcs || !buf) st = dn_fail(DN_ENOMEM, "driver: out of memory");
     }
     /* shots per batch: what the free device memory holds */
     int per_batch = nshots;
     if (!st) {
         size_t fp = 0, free_b = 0, total_b = 0;
-        if (dn_shot_footprint(&p, ntr, 0, &fp) == DN_OK && dn_device_memory(device, &free_b, &total_b) == DN_OK &&
+        if (dn_shot_footprint(&p, maxtr, 0, &fp) == DN_OK && dn_device_memory(device, &free_b, &total_b) == DN_OK &&
             fp > 0) {
             const size_t fit = (size_t)(0.85 * (double)free_b) / fp;
             per_batch = fit < 1 ? 1 : (fit < (size_t)nshots ? (int)fit : nshots);
@@ -197,11 +223,15 @@ int dn_forward_inp(const char *inp_path, int device)
         for (int k = b0; k < b1 && !st; k++) {
             st = build_sources(&in, &p, srcpos, nsrc, k, !in.run_multiple_shots, ts, device, &srcs[k]);
             if (st) break;
-            dn_acq a = {srcs[k].nsrc, srcs[k].si, srcs[k].sj, srcs[k].type, srcs[k].azi, srcs[k].sig, ntr, ri, rj};
+            const int kt = in.readrec == 2 ? sntr[k] : ntr;
+            dn_acq a = {srcs[k].nsrc, srcs[k].si, srcs[k].sj, srcs[k].type, srcs[k].azi, srcs[k].sig, kt,
+                        in.readrec == 2 ? sri[k] : ri, in.readrec == 2 ? srj[k] : rj};
             st = dn_shot_create(model, &a, &shots[k]);
         }
         if (!st) st = dn_run(shots + b0, b1 - b0, DN_MODE_FORWARD);
-        for (int k = b0; k < b1 && !st; k++) st = write_shot(&in, &p, shots[k], k + 1, ntr, ri, rj, &srcs[k], buf);
+        for (int k = b0; k < b1 && !st; k++)
+            st = in.readrec == 2 ? write_shot(&in, &p, shots[k], k + 1, sntr[k], sri[k], srj[k], &srcs[k], buf)
+                                 : write_shot(&in, &p, shots[k], k + 1, ntr, ri, rj, &srcs[k], buf);
         for (int k = b0; k < b1; k++) {
             if (shots[k]) dn_shot_destroy(shots[k]);
             shots[k] = NULL;
@@ -213,6 +243,13 @@ int dn_forward_inp(const char *inp_path, int device)
     free(srcpos);
     free(ri);
     free(rj);
+    for (int k = 0; sri && k < nsrc; k++) {
+        free(sri[k]);
+        free(srj[k]);
+    }
+    free(sntr);
+    free(sri);
+    free(srj);
     free(shots);
     free(srcs);
     free(buf);

@@ -390,6 +390,34 @@ int dn_write_su(const char *path, const float *section, int ntr, int nt, int ndt
     return st;
 }
 
+int dn_write_seis(const char *path, int format, const float *section, int ntr, int nt, int ndt, float dt, float time,
+                  float dh, const int *rec_i, const int *rec_j, const float refrec[4], float xs, float ys)
+{
+    if (format == 1) return dn_write_su(path, section, ntr, nt, ndt, dt, time, dh, rec_i, rec_j, refrec, xs, ys);
+    if (format != 2 && format != 3) return dn_fail(DN_EINVAL, "SEIS_FORMAT=%d: 1 (SU), 2 (ASCII) or 3 (binary)", format);
+    if (!path || !section || ntr < 1 || nt < 1 || ndt < 1) return dn_fail(DN_EINVAL, "dn_write_seis: bad arguments");
+    /* outseis_glob.c:26-33 with sws = 1 (saveseis_glob.c): ns2 = iround(NT / NDT), samples NDT, 2 NDT, ... */
+    const int ntt = iround_d(time / dt);
+    const int ns2 = ntt / ndt;
+    if ((long long)ns2 * ndt > nt) return dn_fail(DN_EINVAL, "dn_write_seis: section shorter than TIME/DT");
+    FILE *f = fopen(path, format == 3 ? "wb" : "w");
+    if (!f) return dn_fail(DN_EIO, "cannot write %s", path);
+    int st = DN_OK;
+    for (int k = 0; k < ntr && st == DN_OK; k++) {
+        const float *tr = section + (size_t)k * nt;
+        for (int j = 1; j <= ns2; j++) {
+            const float v = tr[(size_t)j * ndt - 1];
+            /* outseis_glob.c:268-295: ASCII one value per line ("%e"), or raw native floats */
+            if (format == 2 ? fprintf(f, "%e\n", v) < 0 : fwrite(&v, sizeof(float), 1, f) != 1) {
+                st = dn_fail(DN_EIO, "write error on %s", path);
+                break;
+            }
+        }
+    }
+    if (fclose(f) != 0 && st == DN_OK) st = dn_fail(DN_EIO, "write error on %s", path);
+    return st;
+}
+
 int dn_read_su(const char *path, int ntr, int ns, float *section)
 {
     if (!path || !section || ntr < 1 || ns < 1) return dn_fail(DN_EINVAL, "dn_read_su: bad arguments");

@@ -136,6 +136,11 @@ int dn_read_receivers(const char *path, const float refrec[4], float dh, int *nt
  * unassigned (210-239) are written as zero. */
 int dn_write_su(const char *path, const float *section, int ntr, int nt, int ndt, float dt, float time, float dh,
                 const int *rec_i, const int *rec_j, const float refrec[4], float xs, float ys);
+/* The seismogram file of one component in SEIS_FORMAT `format` (outseis_glob.c):
+ * 1 SU (dn_write_su), 2 ASCII one value per line ("%e"), 3 raw native float32,
+ * trace after trace; the same NDT-decimated samples in every format. */
+int dn_write_seis(const char *path, int format, const float *section, int ntr, int nt, int ndt, float dt, float time,
+                  float dh, const int *rec_i, const int *rec_j, const float refrec[4], float xs, float ys);
 
 /* SU reader for observed data (inseis.c): ntr traces of ns samples each. */
 int dn_read_su(const char *path, int ntr, int ns, float *section);

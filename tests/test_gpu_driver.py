@@ -29,6 +29,9 @@ CASES = {
     "spike-low-pass-quellart6": dict(QUELLART=6, FC_SPIKE_1=-5.0, FC_SPIKE_2=30.0, ORDER_SPIKE=5),
     "wavelet-file-quellart3": dict(QUELLART=3, SIGNAL_FILE="wavelet/sig", wavelet_files=True),
     "klauder-quellart7": dict(QUELLART=7, FC_SPIKE_1=7.0, FC_SPIKE_2=45.0),
+    "seis-format-ascii": dict(SEIS_FORMAT=2, SEISMO=4, NDT=3),
+    "seis-format-binary": dict(SEIS_FORMAT=3, SEISMO=1),
+    "receivers-per-shot-readrec2": dict(READREC=2, per_shot_receivers=True),
 }
 
 
@@ -48,7 +51,13 @@ def _make(root, kw):
     nshots = kw.pop("nshots", 3)
     styp = kw.pop("src_type", 1)
     wavelet_files = kw.pop("wavelet_files", False)
+    per_shot = kw.pop("per_shot_receivers", False)
     inp = inp_case.write_case(root, nshots=nshots, **kw)
+    if per_shot:   # READREC 2: "<REC_FILE>_shot_<n>.dat", a different line of receivers per shot
+        lines = open(os.path.join(root, "receiver", "receivers.dat")).read().splitlines()
+        for k in range(1, nshots + 1):
+            with open(os.path.join(root, "receiver", f"receivers_shot_{k}.dat"), "w") as f:
+                f.write("".join(ln + "\n" for ln in lines[k - 1: len(lines) - 2 * k]))
     if wavelet_files:   # QUELLART 3: "<SIGNAL_FILE>_shot_<n>.dat", one sample per line
         os.makedirs(os.path.join(root, "wavelet"), exist_ok=True)
         nt = io.inp_nt(io.read_inp(inp))
@@ -93,9 +102,14 @@ def test_driver_matches_reference_program(tmp_path, name):
     ref_files = sorted(f for f in os.listdir(os.path.join(ref_dir, "su")) if ".shot" in f)
     assert ref_files
     inp = io.read_inp(os.path.join(ref_dir, "case.inp"))
-    ri, _ = io.read_receivers(os.path.join(ref_dir, "receiver", "receivers.dat"), inp.refrec, inp.dh)
     for f in ref_files:
+        shot = int(f.rsplit(".shot", 1)[1])
+        rec = "receivers_shot_%d.dat" % shot if inp.readrec == 2 else "receivers.dat"
+        ri, _ = io.read_receivers(os.path.join(ref_dir, "receiver", rec), inp.refrec, inp.dh)
         for d in (our_dir, cli_dir):
-            _su_equal(os.path.join(d, "su", f), os.path.join(ref_dir, "su", f), len(ri))
+            if inp.seis_format == 1:
+                _su_equal(os.path.join(d, "su", f), os.path.join(ref_dir, "su", f), len(ri))
+            else:   # ASCII or raw floats: the whole file
+                assert open(os.path.join(d, "su", f), "rb").read() == open(os.path.join(ref_dir, "su", f), "rb").read(), f
     ours = sorted(f for f in os.listdir(os.path.join(our_dir, "su")) if ".shot" in f)
     assert ours == ref_files
