@@ -226,6 +226,9 @@ SIGNATURES = {
     "dn_write_su": (ctypes.c_int, [ctypes.c_char_p, _c_float_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_float, ctypes.c_float, ctypes.c_float, _P(ctypes.c_int),
                                    _P(ctypes.c_int), _c_float_p, ctypes.c_float, ctypes.c_float]),
+    "dn_write_seis": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _c_float_p, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, _P(ctypes.c_int),
+                                     _P(ctypes.c_int), _c_float_p, ctypes.c_float, ctypes.c_float]),
     "dn_read_su": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _c_float_p]),
     "dn_forward_inp": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "dn_residual_l2_noalloc": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,

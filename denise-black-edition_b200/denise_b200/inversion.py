@@ -59,8 +59,9 @@ def params_from_inp(inp, ts, **kw):
 def _check_supported(inp):
     if inp.physics != 1:
         raise NotImplementedError(f"PHYSICS={inp.physics}: only 2-D P-SV (1) is built")
-    if inp.readmod != 1 or inp.srcrec != 1 or inp.readrec != 1:
-        raise NotImplementedError("READMOD, SRCREC and READREC must be 1 (model, source and receiver files)")
+    if inp.readmod != 1 or inp.srcrec != 1 or inp.readrec not in (1, 2):
+        raise NotImplementedError("READMOD and SRCREC must be 1 (model and source files), READREC 1 or 2 "
+                                  "(one receiver file or one per shot)")
     for key, what in (("sws_taper_file", "SWS_TAPER_FILE"), ("trkill", "TRKILL"), ("timelapse", "TIMELAPSE"),
                       ("gravity", "GRAVITY")):
         if inp.get(key):
@@ -74,7 +75,9 @@ class Acquisition:
         self.inp = inp
         self.device = device
         self.srcpos, self.ts = io.read_sources(inp.get("source_file"))
-        self.rec_i, self.rec_j = io.read_receivers(inp.get("rec_file") + ".dat", list(inp.refrec), inp.dh)
+        self.rec_i, self.rec_j = io.read_receivers(inp.get("rec_file") + ".dat", list(inp.refrec), inp.dh) \
+            if inp.readrec != 2 else (None, None)
+        self.shot_receivers = {}
         self.nt = io.inp_nt(inp)
         self.nshots = len(self.srcpos)
         self.file_signals = {}
@@ -106,8 +109,19 @@ class Acquisition:
         if inp.quellart == 6:
             signals = tdfilt(signals, inp.dt, inp.order_spike, inp.fc_spike_2, inp.fc_spike_1, self.device)
         s0 = self.srcpos[k]
-        return (np.array(si, np.int32), np.array(sj, np.int32), signals, self.rec_i, self.rec_j,
+        ri, rj = self.receivers(k)
+        return (np.array(si, np.int32), np.array(sj, np.int32), signals, ri, rj,
                 np.array(types, np.int32), np.array(azi, np.float32), (float(s0[0]), float(s0[1])))
+
+    def receivers(self, k):
+        """Receivers of shot k (0-based): REC_FILE.dat, or REC_FILE_shot_<k+1>.dat with
+        READREC 2 (receiver.c:32-41, read per shot by grad_obj_psv.c and obj_psv.c)."""
+        if self.inp.readrec != 2:
+            return self.rec_i, self.rec_j
+        if k not in self.shot_receivers:
+            self.shot_receivers[k] = io.read_receivers(f"{self.inp.get('rec_file')}_shot_{k + 1}.dat",
+                                                       list(self.inp.refrec), self.inp.dh)
+        return self.shot_receivers[k]
 
     def test_shots(self):
         """0-based indices of TESTSHOT_START .. TESTSHOT_END by TESTSHOT_INCR."""
@@ -116,9 +130,11 @@ class Acquisition:
 
 
 def read_observed(inp, nshots, ntr, nt):
-    """DATA_DIR_x.su.shot<n> and DATA_DIR_y.su.shot<n> (inseis.c) of every shot."""
+    """DATA_DIR_x.su.shot<n> and DATA_DIR_y.su.shot<n> (inseis.c) of every shot; ntr is
+    the receiver count, or a function of the 0-based shot giving it (READREC 2)."""
     base = inp.get("data_dir")
-    return [(io.read_su(f"{base}_x.su.shot{k}", ntr, nt), io.read_su(f"{base}_y.su.shot{k}", ntr, nt))
+    count = ntr if callable(ntr) else (lambda k: ntr)
+    return [(io.read_su(f"{base}_x.su.shot{k}", count(k - 1), nt), io.read_su(f"{base}_y.su.shot{k}", count(k - 1), nt))
             for k in range(1, nshots + 1)]
 
 
@@ -133,7 +149,9 @@ def precond_base(inp, acq):
                          exp_taper_grad_hor=inp.exp_taper_grad_hor, srtshape=inp.srtshape, srtradius=inp.srtradius,
                          filtsize=inp.filtsize,
                          sources=[(float(s[0]), float(s[1])) for s in acq.srcpos],
-                         receivers=list(zip(acq.rec_i.tolist(), acq.rec_j.tolist())))
+                         receivers=list(zip(*[np.concatenate([acq.receivers(k)[c] for k in range(acq.nshots)]).tolist()
+                                              for c in (0, 1)])) if inp.readrec == 2
+                         else list(zip(acq.rec_i.tolist(), acq.rec_j.tolist())))
 
 
 def fwi_inp(par_path, workflow_path, device=0, snap_precision=_lib.SNAP_F32, dist=None, resume=False):
@@ -152,7 +170,7 @@ def fwi_inp(par_path, workflow_path, device=0, snap_precision=_lib.SNAP_F32, dis
     model = [io.read_model_file(f"{inp.get('mfile')}.{ext}", nx, ny) for ext in ("vp", "vs", "rho")]
     if p.L:
         model += [io.read_model_file(f"{inp.get('mfile')}.{ext}", nx, ny) for ext in ("qp", "qs")]
-    obs = read_observed(inp, acq.nshots, len(acq.rec_i), p.nt)
+    obs = read_observed(inp, acq.nshots, lambda k: len(acq.receivers(k)[0]), p.nt)
     stages = read_workflow(workflow_path)
     limits = (inp.vplowerlim, inp.vpupperlim, inp.vslowerlim, inp.vsupperlim, inp.rholowerlim, inp.rhoupperlim)
     shot_taper = (inp.srtshape, inp.srtradius, inp.filtsize) if inp.sws_taper_circular_per_shot else None

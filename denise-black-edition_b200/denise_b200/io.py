@@ -139,6 +139,18 @@ def write_su(path, section, ndt, dt, time, dh, rec_i, rec_j, refrec, xs, ys):
                           rr.ctypes.data_as(_lib._c_float_p), ctypes.c_float(xs), ctypes.c_float(ys)))
 
 
+def write_seis(path, fmt, section, ndt, dt, time, dh, rec_i, rec_j, refrec, xs, ys):
+    """dn_write_seis: SEIS_FORMAT fmt 1 (SU), 2 (ASCII) or 3 (binary float32)."""
+    sec = np.ascontiguousarray(section, np.float32)
+    ri = np.ascontiguousarray(rec_i, np.int32)
+    rj = np.ascontiguousarray(rec_j, np.int32)
+    rr = np.asarray(refrec, np.float32)
+    check(lib.dn_write_seis(str(path).encode(), int(fmt), sec.ctypes.data_as(_lib._c_float_p), sec.shape[0],
+                            sec.shape[1], ndt, ctypes.c_float(dt), ctypes.c_float(time), ctypes.c_float(dh),
+                            ri.ctypes.data_as(_lib._c_int_p), rj.ctypes.data_as(_lib._c_int_p),
+                            rr.ctypes.data_as(_lib._c_float_p), ctypes.c_float(xs), ctypes.c_float(ys)))
+
+
 def read_su(path, ntr, ns):
     out = np.empty((ntr, ns), np.float32)
     check(lib.dn_read_su(str(path).encode(), ntr, ns, out.ctypes.data_as(_lib._c_float_p)))

@@ -417,8 +417,19 @@ int refh_receivers(const char *base, float refx, float refy, float dh, int *ntr,
 }
 
 /* outseis_glob() SEIS_FORMAT 1 of a section [ntr][ns] (ns = NT samples) */
+int refh_outseis_fmt(const char *path, int format, const float *section, int ntr, int ns, const int *ri,
+                     const int *rj, float xs, float ys, int ndt, float time, float dt, float dh, float refx,
+                     float refy);
 int refh_outseis(const char *path, const float *section, int ntr, int ns, const int *ri, const int *rj, float xs,
                  float ys, int ndt, float time, float dt, float dh, float refx, float refy)
+{
+    return refh_outseis_fmt(path, 1, section, ntr, ns, ri, rj, xs, ys, ndt, time, dt, dh, refx, refy);
+}
+
+/* outseis_glob() with SEIS_FORMAT `format` (1 SU, 2 ASCII, 3 binary), as saveseis_glob.c calls it */
+int refh_outseis_fmt(const char *path, int format, const float *section, int ntr, int ns, const int *ri,
+                     const int *rj, float xs, float ys, int ndt, float time, float dt, float dh, float refx,
+                     float refy)
 {
     float **sec = matrix(1, ntr, 1, ns);
     int **rp = imatrix(1, 3, 1, ntr);
@@ -439,7 +450,7 @@ int refh_outseis(const char *path, const float *section, int ntr, int ns, const 
     REFREC[2] = refy;
     FILE *f = fopen(path, "w");
     if (!f) return -1;
-    outseis_glob(null_log(), f, 1, sec, rp, rp, ntr, sp, 1, ns, 1, 1, 1);
+    outseis_glob(null_log(), f, 1, sec, rp, rp, ntr, sp, 1, ns, format, 1, 1);
     free_matrix(sec, 1, ntr, 1, ns);
     free_imatrix(rp, 1, 3, 1, ntr);
     free_matrix(sp, 1, 8, 1, 1);

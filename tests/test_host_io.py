@@ -222,6 +222,34 @@ def test_su_writer_matches_outseis_glob(tmp_path, ndt):
     np.testing.assert_array_equal(back, sec[:, ndt - 1::ndt][:, :ns])
 
 
+def _ref_outseis_fmt(path, fmt, sec, ri, rj, xs, ys, ndt, time, dt, dh, refx, refy):
+    lib = ctypes.CDLL(O.REF_SO)
+    sec = np.ascontiguousarray(sec, np.float32)
+    ri = np.ascontiguousarray(ri, np.int32)
+    rj = np.ascontiguousarray(rj, np.int32)
+    f = ctypes.c_float
+    assert lib.refh_outseis_fmt(path.encode(), fmt, O._fp(sec), sec.shape[0], sec.shape[1], O._ip(ri), O._ip(rj),
+                                f(xs), f(ys), ndt, f(time), f(dt), f(dh), f(refx), f(refy)) == 0
+
+
+@needs_ref
+@pytest.mark.parametrize("fmt", [2, 3])
+@pytest.mark.parametrize("ndt", [1, 3])
+def test_ascii_and_binary_seismograms_match_outseis_glob(tmp_path, fmt, ndt):
+    """SEIS_FORMAT 2 (one "%e" per line) and 3 (native floats), trace after trace,
+    NDT-decimated: byte for byte the files of the reference's outseis_glob."""
+    rng = np.random.default_rng(fmt + 10 * ndt)
+    ntr, nt, dt, dh = 11, 200, 4e-4, 5.0
+    time = np.float32(nt * dt)
+    sec = (rng.standard_normal((ntr, nt)) * 10.0 ** rng.integers(-12, 3, (ntr, 1))).astype(np.float32)
+    ri = np.arange(4, 4 + 3 * ntr, 3).astype(np.int32)
+    rj = np.full(ntr, 5, np.int32)
+    ours, ref = str(tmp_path / "ours"), str(tmp_path / "ref")
+    io.write_seis(ours, fmt, sec, ndt, dt, time, dh, ri, rj, [0.0, 2.0, 1.0, 0.0], 312.5, 10.0)
+    O.run_isolated(_ref_outseis_fmt, ref, fmt, sec, ri, rj, 312.5, 10.0, ndt, time, dt, dh, 2.0, 1.0)
+    assert open(ours, "rb").read() == open(ref, "rb").read()
+
+
 def test_model_file_roundtrip_and_short_file(tmp_path):
     a = np.random.default_rng(0).standard_normal((12, 7)).astype(np.float32)
     p = str(tmp_path / "m.vp")
