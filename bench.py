@@ -215,11 +215,24 @@ def create_batch(p, inputs, device):
         return list(ex.map(mk, inputs))
 
 
+def kernel_choice(p):
+    """The tile and stencil-kernel variant the library's rules give this workload."""
+    try:
+        from denise_b200 import tune
+
+        bx, zch, v = tune.choice_for(p)
+        return {"tile": f"{bx}x{zch}", "variant": {0: "paired-column FP32x2", 1: "one-column",
+                                                   2: "paired, pipelined velocity"}.get(v, str(v)),
+                "rule": "built-in table measured by denise_b200.tune (denise_b200/tiles_b200.json)"}
+    except Exception:
+        return None
+
+
 def workload_config(a, p, world):
     return {"workload": f"batched viscoelastic forward: {a.shots} shots x {p.nx}x{p.ny} grid, NT={p.nt}, "
                         f"L=3, FDORDER 8, FW 20, free surface, 400 receivers/shot",
             "shots_per_gpu": a.shots, "nx": p.nx, "nz": p.ny, "nt": p.nt, "fdorder": p.fdorder, "L": p.L,
-            "arith": "exact (bit-identical to the reference)",
+            "arith": "exact (bit-identical to the reference)", "kernels": kernel_choice(p),
             "l2_flush": "inputs larger than L2 (resident state ~15 GB)",
             "parallelism": f"shots-dp{world}"}
 

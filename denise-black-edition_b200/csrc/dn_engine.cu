@@ -465,10 +465,10 @@ extern "C" int dn_model_params(const dn_model *m, dn_params *out)
 // ---------------------------------------------------------------------------
 // shots
 // ---------------------------------------------------------------------------
-// Tile shapes of new shots: rules set by dn_set_tile_shape (the autotuner of
-// denise_b200/tune.py measures them per FDORDER, L and grid size on the device),
-// the last matching rule winning; DN_TILE="WxZ" overrides everything; else the
-// 128 x 8 tile measured best for the 2000 x 600 batched workload (4-32 rows swept).
+// Tile shapes and kernel variants of new shots: rules set by dn_set_tile_shape /
+// dn_set_kernel_rule (the autotuner of denise_b200/tune.py measures them per
+// FDORDER, L, snapshot class and grid size on the device) after the built-in
+// ones below, the last matching rule winning; DN_TILE="WxZ" overrides the tile.
 struct TileRule {
     int fdorder, L;
     long long cells_min, cells_max;
@@ -477,19 +477,26 @@ struct TileRule {
     int variant;   // DN_KERN_* stencil kernels (register blocking); -1: the default
 };
 static std::mutex g_tile_mu;
-static std::vector<TileRule> g_tile_rules;
+// Built-in rules, from the table denise_b200.tune measured on a B200
+// (denise_b200/tiles_b200.json: FDORDER 4, 8, 12 x L 0, 3 x snapshot class x grids
+// of 0.18 M and 1.2 M cells, 8 shots each): the default 128 x 4 tile is the best
+// or within 1.3 % of the best in every class; the one-column kernels beat the
+// paired ones on FDORDER 8 elastic forward grids up to 470 k cells.
+static std::vector<TileRule> g_tile_rules = {
+    {8, 0, 0, 470000, 128, 4, 0, DN_KERN_COLUMN},
+};
 
 static bool tile_ok(int bx, int zch) { return bx >= 32 && bx <= 256 && (bx % 32) == 0 && zch >= 1 && zch <= 256; }
 
 static void tile_choice(const dn_params *p, int &bx, int &zch, int &variant)
 {
     variant = DN_KERN_PAIRED;
-    // default tiles: 128 x 8 for forward runs; 128 x 4 for shots that store
-    // snapshots (more blocks for the gradient's smaller batches: the 7-shot
-    // 1700 x 500 FP16 forward + adjoint ran 449 ms per 1000 steps at 128 x 8 and
-    // 416 ms at 128 x 4, while 64-shot forward batches gain nothing from it)
+    // default tiles: 128 x 4 (the autotuner's table: 1.7-11 % faster than 128 x 8
+    // for forward runs of 8 shots, 3.5 % on the 2000 x 600 viscoelastic grid; the
+    // 7-shot 1700 x 500 FP16 forward + adjoint ran 449 ms per 1000 steps at
+    // 128 x 8 and 416 ms at 128 x 4)
     bx = 128;
-    zch = p->store_snapshots ? 4 : 8;
+    zch = 4;
     const long long cells = (long long)p->nx * p->ny;
     {
         std::lock_guard<std::mutex> lk(g_tile_mu);

@@ -333,12 +333,6 @@ __device__ __forceinline__ void pf_l1(const float *p) { asm volatile("prefetch.g
 #ifndef DN_PF_ROWS
 #define DN_PF_ROWS 1
 #endif
-// rows ahead of the L2 prefetch of the paired kernels (0: none); capped at HZ - R so
-// that every prefetched address stays inside the padded planes
-#ifndef DN_PF2_ROWS
-#define DN_PF2_ROWS 0
-#endif
-__device__ __forceinline__ void pf_l2(const float *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 
 // float2 store of a lane pair, or lane 0 alone for the last column of an odd nx
@@ -400,16 +394,6 @@ __global__ void __launch_bounds__(128, 8) k_update_v2(const Inst *__restrict__ i
             pf_l1(I.rjp + o + D * P);
             pf_l1(I.vx + o + D * P);
             pf_l1(I.vy + o + D * P);
-            constexpr int D2 = DN_PF2_ROWS < DN_HZ - R ? DN_PF2_ROWS : DN_HZ - R;
-            if (D2 > D) {
-                pf_l2(I.syy + o + (R + D2) * P);
-                pf_l2(I.sxy + o + (R - 1 + D2) * P);
-                pf_l2(I.sxx + o + D2 * P);
-                pf_l2(I.rip + o + D2 * P);
-                pf_l2(I.rjp + o + D2 * P);
-                pf_l2(I.vx + o + D2 * P);
-                pf_l2(I.vy + o + D2 * P);
-            }
         }
         // sxx x stencil of lane 0: columns i0-R+1 .. i0+R (A[k], k = 0..2R); pairs (A[k], A[k+1]);
         // column i0-R+1+k is odd when k - R is odd
@@ -857,17 +841,6 @@ __global__ void __launch_bounds__(128, 8) k_update_s_el2(const Inst *__restrict_
             pf_l1(I.sxx + o + D * P);
             pf_l1(I.syy + o + D * P);
             pf_l1(I.sxy + o + D * P);
-            constexpr int D2 = DN_PF2_ROWS < DN_HZ - R ? DN_PF2_ROWS : DN_HZ - R;
-            if (D2 > D) {
-                pf_l2(I.vx + o + (R + D2) * P);
-                pf_l2(I.vy + o + (R - 1 + D2) * P);
-                pf_l2(I.uipjp + o + D2 * P);
-                pf_l2(I.mu + o + D2 * P);
-                pf_l2(I.lam + o + D2 * P);
-                pf_l2(I.sxx + o + D2 * P);
-                pf_l2(I.syy + o + D2 * P);
-                pf_l2(I.sxy + o + D2 * P);
-            }
         }
         float2 vxx, vyx, vxy, vyy;
         vderiv2<R, X>(I, hc, i0, j, o, P, dhi, vxx, vyx, vxy, vyy);
