@@ -228,11 +228,11 @@ def kernel_choice(p):
         return None
 
 
-def workload_config(a, p, world):
+def workload_config(a, p, world, ours=True):
     return {"workload": f"batched viscoelastic forward: {a.shots} shots x {p.nx}x{p.ny} grid, NT={p.nt}, "
                         f"L=3, FDORDER 8, FW 20, free surface, 400 receivers/shot",
             "shots_per_gpu": a.shots, "nx": p.nx, "nz": p.ny, "nt": p.nt, "fdorder": p.fdorder, "L": p.L,
-            "arith": "exact (bit-identical to the reference)", "kernels": kernel_choice(p),
+            "arith": "exact (bit-identical to the reference)", "kernels": kernel_choice(p) if ours else None,
             "l2_flush": "inputs larger than L2 (resident state ~15 GB)",
             "parallelism": f"shots-dp{world}"}
 
@@ -861,7 +861,7 @@ def run_reference(a, rank, world):
     return {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(ms, 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": dict(workload_config(a, p, world), parallelism="host processes",
+            "config": dict(workload_config(a, p, world, ours=False), parallelism="host processes",
                            sample="bounded: one single-rank process per host core, each on its own shot of this "
                                   f"workload for {a.cpu_sample_nt} time steps"),
             "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
