@@ -477,26 +477,27 @@ struct TileRule {
     int variant;   // DN_KERN_* stencil kernels (register blocking); -1: the default
 };
 static std::mutex g_tile_mu;
-// Built-in rules, from the table denise_b200.tune measured on a B200
-// (denise_b200/tiles_b200.json: FDORDER 4, 8, 12 x L 0, 3 x snapshot class x grids
-// of 0.18 M and 1.2 M cells, 8 shots each): the default 128 x 4 tile is the best
-// or within 1.3 % of the best in every class; the one-column kernels beat the
-// paired ones on FDORDER 8 elastic forward grids up to 470 k cells.
-static std::vector<TileRule> g_tile_rules = {
-    {8, 0, 0, 470000, 128, 4, 0, DN_KERN_COLUMN},
-};
+// Built-in rules: none.  The table denise_b200.tune measured on a B200
+// (denise_b200/tiles_b200.json: FDORDER 4, 8, 12 x L 0, 3 x snapshot class x
+// grids of 0.18 M and 1.2 M cells; forward batches of 32 shots, storing batches
+// of 8) picks the default of tile_choice in 16 of its 18 classes and beats it by
+// 1.0 % and 0.4 % in the other two, within the run-to-run spread.
+static std::vector<TileRule> g_tile_rules;
 
 static bool tile_ok(int bx, int zch) { return bx >= 32 && bx <= 256 && (bx % 32) == 0 && zch >= 1 && zch <= 256; }
 
 static void tile_choice(const dn_params *p, int &bx, int &zch, int &variant)
 {
     variant = DN_KERN_PAIRED;
-    // default tiles: 128 x 4 (the autotuner's table: 1.7-11 % faster than 128 x 8
-    // for forward runs of 8 shots, 3.5 % on the 2000 x 600 viscoelastic grid; the
-    // 7-shot 1700 x 500 FP16 forward + adjoint ran 449 ms per 1000 steps at
-    // 128 x 8 and 416 ms at 128 x 4)
+    // default tiles: 128 x 8 for forward shots of 480 k cells and more (batches
+    // of 32 and 64 shots of 2000 x 600 cells step 2.3-4.1 % faster than at
+    // 128 x 4), 128 x 4 for smaller forward grids (32 shots of 600 x 300: 3-8 %
+    // faster than 128 x 8 for FDORDER 4, 8, 12 and L 0, 3) and for
+    // snapshot-storing shots, whose batches the snapshots keep small (the 7-shot
+    // 1700 x 500 FP16 forward + adjoint ran 449 ms per 1000 steps at 128 x 8 and
+    // 416 ms at 128 x 4)
     bx = 128;
-    zch = 4;
+    zch = (p->store_snapshots || (long long)p->nx * p->ny < 480000) ? 4 : 8;
     const long long cells = (long long)p->nx * p->ny;
     {
         std::lock_guard<std::mutex> lk(g_tile_mu);

@@ -7,13 +7,18 @@ from denise_b200 import _lib, synth, tune
 def test_rules_pick_the_last_match_and_respect_the_class(tmp_path):
     tune.clear_rules()
     p = synth.c0_params(nx=400, ny=200)
-    assert tune.tile_for(p) == (128, 4)
+    big = p.replace(nx=2000, ny=600)
+    assert tune.tile_for(p) == (128, 4)                   # forward default below 480 k cells
+    assert tune.tile_for(big) == (128, 8)                 # forward default from 480 k cells
+    assert tune.tile_for(big.replace(store_snapshots=1)) == (128, 4)   # snapshot-storing default
     tune.set_rule(8, 0, 50_000, 100_000, 64, 16)
     assert tune.tile_for(p) == (64, 16)
     tune.set_rule(8, 0, 80_000, 80_000, 256, 4)           # later and narrower: wins for this grid
     assert tune.tile_for(p) == (256, 4)
     assert tune.tile_for(p.replace(fdorder=4)) == (128, 4)  # other FDORDER: default
     assert tune.tile_for(p.replace(nx=1000)) == (128, 4)    # outside the ranges
+    assert tune.default_choice(400 * 200, 0) == (128, 4, _lib.KERN_PAIRED)
+    assert tune.default_choice(2000 * 600, 0) == (128, 8, _lib.KERN_PAIRED)
     rules = [(8, 0, 50_000, 100_000, 64, 16), (8, 0, 80_000, 80_000, 256, 4)]
     tune.save(tmp_path / "t.json", rules)
     tune.clear_rules()
