@@ -222,8 +222,10 @@ def kernel_choice(p):
 
         bx, zch, v = tune.choice_for(p)
         return {"tile": f"{bx}x{zch}", "variant": {0: "paired-column FP32x2", 1: "one-column",
-                                                   2: "paired, pipelined velocity"}.get(v, str(v)),
-                "rule": "built-in table measured by denise_b200.tune (denise_b200/tiles_b200.json)"}
+                                                   2: "paired, pipelined velocity",
+                                                   3: "fused elastic step"}.get(v, str(v)),
+                "rule": "the library's default (tile_choice), which the table measured by denise_b200.tune "
+                        "(denise_b200/tiles_b200.json) confirms"}
     except Exception:
         return None
 
@@ -567,9 +569,10 @@ def run_elastic(a, inputs, device, peak):
     dn.run(shots)
     torch.cuda.synchronize(device)
     ms = []
-    for _ in range(2):
-        dn.run(shots)
-        ms.append(dn.last_run_stats()[0])
+    with ClockSampler(device) as clk:
+        for _ in range(2):
+            dn.run(shots)
+            ms.append(dn.last_run_stats()[0])
     ms = float(np.mean(ms))
     cells = len(shots) * p.nx * p.ny
     prof = dn.api.profile_steps(shots, dn.MODE_FORWARD, nsteps=20)
@@ -581,7 +584,8 @@ def run_elastic(a, inputs, device, peak):
            "v_kernel_gbs": round(36 * cells / (prof["update_v"] * 1e-3) / 1e9, 1),
            "s_kernel_gbs": round(44 * cells / (prof["update_s"] * 1e-3) / 1e9, 1),
            "whole_step_gbs_direct": round(80 * cells / (step_ms * 1e-3) / 1e9, 1),
-           "kernel_ms": {k: round(v, 4) for k, v in prof.items()}}
+           "kernel_ms": {k: round(v, 4) for k, v in prof.items()},
+           "clocks": clk.summary()}
     out["whole_step_frac"] = round(out["whole_step_gbs_direct"] / peak, 4)
     out["v_kernel_frac"] = round(out["v_kernel_gbs"] / peak, 4)
     for m, s in pairs:

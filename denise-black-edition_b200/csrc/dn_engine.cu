@@ -168,6 +168,12 @@ struct dn_shot {
     float *d_snap_scale = nullptr;
     int nsnap = 0, zch = 16, bx = 128, tiles_x = 0, tiles = 0;
     int kern = DN_KERN_PAIRED;     // stencil kernel variant (the batch runs its first shot's)
+    // fused elastic step (DN_KERN_FUSED on an eligible shot): the second set of fields and
+    // velocity CPML memory (inside dstate, so zeroed with it) and the tile rows
+    bool fz = false;
+    int fzc = 0;
+    float *fb[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    float *fpsi[4] = {nullptr, nullptr, nullptr, nullptr};
     void *d_acc = nullptr;         // wc, wcu, wcrho (float or double) + Ws, Wr
     int acc64;
     int *d_flag = nullptr;
@@ -534,7 +540,7 @@ extern "C" int dn_set_kernel_rule(int fdorder, int L, int store, long long cells
     if (!tile_ok(bx, zch))
         return dn_fail(DN_EINVAL, "dn_set_kernel_rule: %d x %d (width a multiple of 32 up to 256, 1-256 rows)", bx,
                        zch);
-    if (variant < -1 || variant > DN_KERN_VPIPE) return dn_fail(DN_EINVAL, "dn_set_kernel_rule: variant %d", variant);
+    if (variant < -1 || variant > DN_KERN_FUSED) return dn_fail(DN_EINVAL, "dn_set_kernel_rule: variant %d", variant);
     std::lock_guard<std::mutex> lk(g_tile_mu);
     for (TileRule &r : g_tile_rules)
         if (r.fdorder == fdorder && r.L == L && r.cells_min == cells_min && r.cells_max == cells_max &&
@@ -583,6 +589,27 @@ static int shot_counts(const dn_params *p, int bx, int zch, int &tiles_x, int &t
     return DN_OK;
 }
 
+// shots of this class run the fused elastic step (k_step_el_fused) in their forward runs:
+// elastic, no snapshots, variant DN_KERN_FUSED (a rule, or DN_FUSED=1 / 0 in the environment)
+static bool fused_class(const dn_params *p, int variant)
+{
+    if (p->L != 0 || p->store_snapshots) return false;
+    const char *ev = getenv("DN_FUSED");
+    if (ev) return strcmp(ev, "0") != 0;
+    return variant == DN_KERN_FUSED;
+}
+
+// rows per tile of the fused step: about DN_FUSED_ROWS (default 96) in equal chunks,
+// at least R + 1 so that the top tile holds the rows the free surface reads
+static int fused_rows(const dn_params *p)
+{
+    const char *ev = getenv("DN_FUSED_ROWS");
+    int z = ev && atoi(ev) > 0 ? atoi(ev) : 96;
+    z = std::max(z, p->fdorder / 2 + 1);
+    const int chunks = std::max(1, (p->ny + z - 1) / z);
+    return std::max((p->ny + chunks - 1) / chunks, std::min(p->ny, p->fdorder / 2 + 1));
+}
+
 extern "C" int dn_shot_footprint(const dn_params *p, int ntr, int store, size_t *bytes)
 {
     int st = validate_params(p);
@@ -603,6 +630,10 @@ extern "C" int dn_shot_footprint(const dn_params *p, int ntr, int store, size_t 
                            std::max(p->nx, p->ny) * 4);
     }
     b += (size_t)p->nx * p->ny * (3 * (p->grad_accum == DN_ACC_F64 ? 8 : 4) + 8);
+    int variant;
+    tile_choice(&q, bx, zch, variant);
+    if (fused_class(&q, variant))   // the fused step's second set of fields and CPML memory
+        b += (size_t)5 * L.plane * 4 + (size_t)4 * 2 * std::max(p->fw, 1) * std::max(p->nx, p->ny) * 4;
     if (bytes) *bytes = b;
     return DN_OK;
 }
@@ -690,6 +721,14 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
     const int fw = p->fw;
     const size_t xf = (size_t)p->ny * 2 * std::max(fw, 1), zf = (size_t)2 * std::max(fw, 1) * p->nx;
     s->state_bytes = carve_size(L.plane, 4) * (7 + 3 * p->L) + carve_size(xf, 4) * 5 + carve_size(zf, 4) * 4;
+    // the fused step takes shots with at most FZ_MAXSRC source cells and no moment-tensor source
+    s->fz = fused_class(p, s->kern) && s->nsrc_cells <= FZ_MAXSRC;
+    for (int l = 0; l < acq->nsrc; l++)
+        if (s->src_type[l] == 5) s->fz = false;
+    if (s->fz) {
+        s->fzc = fused_rows(p);
+        s->state_bytes += carve_size(L.plane, 4) * 5 + carve_size(xf, 4) * 2 + carve_size(zf, 4) * 2;
+    }
     size_t acq_bytes = carve_size(std::max((size_t)s->nsrc_cells, (size_t)1), 4) * 4 +
                        carve_size(std::max((size_t)acq->nsrc, (size_t)1), 4) * 2 +
                        carve_size(std::max((size_t)acq->ntr, (size_t)1), 4) * 2 +
@@ -734,6 +773,11 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
     }
     for (int k = 0; k < 5; k++) s->psi[k] = carve<float>(cur, xf);
     for (int k = 5; k < 9; k++) s->psi[k] = carve<float>(cur, zf);
+    if (s->fz) {
+        for (int k = 0; k < 5; k++) s->fb[k] = carve<float>(cur, L.plane) + L.origin;
+        for (int k = 0; k < 2; k++) s->fpsi[k] = carve<float>(cur, xf);
+        for (int k = 2; k < 4; k++) s->fpsi[k] = carve<float>(cur, zf);
+    }
     // (the visco planes were carved with their full size)
     char *ac = s->dacq;
     s->d_cell_i = carve<int>(ac, std::max(s->nsrc_cells, 1));
@@ -778,6 +822,14 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
     return DN_OK;
 }
 
+extern "C" int dn_shot_kernel(const dn_shot *s, int *variant, int *fused)
+{
+    if (!s || !variant || !fused) return dn_fail(DN_EINVAL, "dn_shot_kernel: null argument");
+    *variant = s->kern;
+    *fused = s->fz ? 1 : 0;
+    return DN_OK;
+}
+
 static void forget_shot(const dn_shot *s);
 
 extern "C" int dn_shot_destroy(dn_shot *s)
@@ -809,6 +861,9 @@ static void *acc_ptr(const dn_shot *s, int k)
     if (k < 3) return b + k * a;
     return b + 3 * a + (k - 3) * w;
 }
+
+// a forward run (mode 0 or 2) of a shot with the second field set takes the fused step
+static bool runs_fused(const dn_shot *s, int mode) { return s->fz && (mode == 0 || mode == 2); }
 
 static Inst make_inst(const dn_shot *s, int mode)
 {
@@ -935,6 +990,23 @@ static Inst make_inst(const dn_shot *s, int mode)
     I.Ws = (float *)acc_ptr(s, 3);
     I.Wr = (float *)acc_ptr(s, 4);
     I.flag = s->d_flag;
+    if (runs_fused(s, mode)) {
+        const int R = p.fdorder / 2;
+        I.pp = 1;
+        I.f_w = fz_width(R);
+        I.f_tiles_x = (p.nx + I.f_w - 1) / I.f_w;
+        I.f_zc = s->fzc;
+        I.f_tiles = I.f_tiles_x * ((p.ny + s->fzc - 1) / s->fzc);
+        I.vx_b = s->fb[0];
+        I.vy_b = s->fb[1];
+        I.sxx_b = s->fb[2];
+        I.syy_b = s->fb[3];
+        I.sxy_b = s->fb[4];
+        I.psi_sxx_x_b = s->fpsi[0];
+        I.psi_sxy_x_b = s->fpsi[1];
+        I.psi_syy_y_b = s->fpsi[2];
+        I.psi_sxy_y_b = s->fpsi[3];
+    }
     return I;
 }
 
@@ -1060,7 +1132,8 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c, con
     c.pack = !c.tma && shots[0]->kern != DN_KERN_COLUMN;
     if (pk) c.pack = !c.tma && strcmp(pk, "0") != 0;
     c.any_surf = c.any_src_s = c.any_store = c.any_adj = c.any_rec = false;
-    int maxtiles = 0, maxsrc = 1, maxnx = 1, maxtr = 1;
+    c.any_fused = c.any_plain = false;
+    int maxtiles = 0, maxsrc = 1, maxnx = 1, maxtr = 1, maxft = 1;
     for (int k = 0; k < n; k++) {
         const dn_shot *s = shots[k];
         if (!s) return dn_fail(DN_EINVAL, "dn_run: null shot %d", k);
@@ -1077,6 +1150,13 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c, con
                     return dn_fail(DN_ENOTSUP, "moment-tensor sources are not supported in the adjoint pass");
         }
         maxtiles = std::max(maxtiles, s->tiles);
+        if (runs_fused(s, m)) {
+            c.any_fused = true;
+            const int fwd = fz_width(s->p.fdorder / 2);
+            maxft = std::max(maxft, ((s->p.nx + fwd - 1) / fwd) * ((s->p.ny + s->fzc - 1) / s->fzc));
+        } else {
+            c.any_plain = true;
+        }
         maxsrc = std::max(maxsrc, std::max(s->nsrc_cells, m == 1 ? s->ntr : 0));
         maxnx = std::max(maxnx, s->p.nx);
         maxtr = std::max(maxtr, s->ntr);
@@ -1086,6 +1166,7 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c, con
         if (m == 1) c.any_adj = true;
     }
     c.tile_grid = dim3(maxtiles, n);
+    c.fgrid = dim3(maxft, n);
     // pipelined velocity kernel (DN_VPIPE=1): strips of VP_W columns, about four CTAs per
     // resident slot (148 SMs x 3) over the batch, at least 32 rows tall (DN_VPIPE_ROWS sets it)
     const char *vp = getenv("DN_VPIPE");
@@ -1391,6 +1472,13 @@ static int run_direct(dn_shot *s, int mode, int nt0, int nt1, bool zero)
     st = prepare_launch(c);
     if (st) return st;
     Inst h = make_inst(s, mode);
+    if (h.pp && (nt0 != 1 || nt1 != s->p.nt)) {
+        // a partial range runs the separate kernels on the primary buffers, so that the state
+        // between calls stays where dn_shot_get_field and the next range read it
+        h.pp = 0;
+        c.any_fused = false;
+        c.any_plain = true;
+    }
     Inst *d = nullptr;
     CU(dn_malloc(&d, sizeof(Inst)));
     CU(cudaMemcpyAsync(d, &h, sizeof(Inst), cudaMemcpyHostToDevice, ds->stream));

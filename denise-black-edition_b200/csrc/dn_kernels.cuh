@@ -88,6 +88,13 @@ struct Inst {
     int fastdiv;                      // division by DH through div_markstein (verified for this DH)
     int t0;                           // step base when the instance joined: its step is *ntb + off - t0
     int snap_base;                    // snapshot k lives in slot k - snap_base (checkpointed segments)
+    // fused elastic step (k_step_el_fused): the fields and the velocity update's CPML memory
+    // alternate between the buffers above and these; step nt writes the second set when
+    // (nt_total - nt) is odd, so the last step leaves the state in the first
+    int pp;                           // this instance runs the fused step
+    int f_w, f_tiles_x, f_zc, f_tiles;   // its tiles: f_w columns x f_zc rows
+    float *vx_b, *vy_b, *sxx_b, *syy_b, *sxy_b;
+    float *psi_sxx_x_b, *psi_sxy_x_b, *psi_syy_y_b, *psi_sxy_y_b;
 };
 
 // ---------------------------------------------------------------------------
@@ -172,6 +179,7 @@ template <int R, bool X>
 __global__ void __maxnreg__(40) k_update_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
+    if (I.pp) return;   // the fused step handles this instance
     const int nt = *ntb + off - I.t0;   // the instance's own time step
     if (nt < 1 || nt > I.nt) return;
     TileLoc t;
@@ -330,6 +338,13 @@ template <bool X> __device__ __forceinline__ float2 SUB2(float2 a, float2 b) { r
 __device__ __forceinline__ float2 ld2(const float *p) { return __ldg(reinterpret_cast<const float2 *>(p)); }
 __device__ __forceinline__ float2 ldw2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 __device__ __forceinline__ void pf_l1(const float *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+// resident CTAs of 128 threads per SM the paired kernels are compiled for (8: 64 registers)
+#ifndef DN_V2_MINB
+#define DN_V2_MINB 8
+#endif
+#ifndef DN_S2_MINB
+#define DN_S2_MINB 8
+#endif
 #ifndef DN_PF_ROWS
 #define DN_PF_ROWS 1
 #endif
@@ -358,9 +373,10 @@ __device__ __forceinline__ float2 DIVH2(float2 a, bool fd, float DH, float rdh)
 }
 
 template <int R, bool X>
-__global__ void __launch_bounds__(128, 8) k_update_v2(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+__global__ void __launch_bounds__(128, DN_V2_MINB) k_update_v2(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
+    if (I.pp) return;   // the fused step handles this instance
     const int nt = *ntb + off - I.t0;   // the instance's own time step
     if (nt < 1 || nt > I.nt) return;
     const int b = blockIdx.x;
@@ -517,6 +533,7 @@ __global__ void __launch_bounds__(128, 8) k_update_v2(const Inst *__restrict__ i
 static __global__ void k_inject_v(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
+    if (I.pp) return;   // the fused step handles this instance
     const int nt = *ntb + off - I.t0;   // the instance's own time step
     if (nt < 1 || nt > I.nt) return;
     const long long P = I.pitch;
@@ -667,6 +684,7 @@ template <int R, bool X>
 __global__ void __launch_bounds__(256, 4) k_update_s_el(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
+    if (I.pp) return;   // the fused step handles this instance
     const int nt = *ntb + off - I.t0;   // the instance's own time step
     if (nt < 1 || nt > I.nt) return;
     TileLoc t;
@@ -811,9 +829,10 @@ __device__ __forceinline__ void vderiv2(const Inst &I, const float *hc, int i0, 
 
 // Paired-column elastic stress update (k_update_s_el for two columns per thread).
 template <int R, bool X>
-__global__ void __launch_bounds__(128, 8) k_update_s_el2(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
+__global__ void __launch_bounds__(128, DN_S2_MINB) k_update_s_el2(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
+    if (I.pp) return;   // the fused step handles this instance
     const int nt = *ntb + off - I.t0;   // the instance's own time step
     if (nt < 1 || nt > I.nt) return;
     const int b = blockIdx.x;
@@ -992,6 +1011,7 @@ __global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__
 static __global__ void k_inject_s(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
+    if (I.pp) return;   // the fused step handles this instance
     const int nt = *ntb + off - I.t0;   // the instance's own time step
     if (nt < 1 || nt > I.nt) return;
     const long long P = I.pitch;
@@ -1055,6 +1075,7 @@ template <int R, bool X>
 __global__ void k_surface_el(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
+    if (I.pp) return;   // the fused step handles this instance
     const int nt = *ntb + off - I.t0;   // the instance's own time step
     if (nt < 1 || nt > I.nt || !I.free_surf) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -1184,8 +1205,12 @@ __global__ void k_seismo(const Inst *__restrict__ insts, const int *__restrict__
     const int nt = *ntb + off - I.t0;   // the instance's own time step
     if (nt < 1 || nt > I.nt) return;
     const long long P = I.pitch;
+    // the buffers holding step nt's result (the second set after odd-distance steps of a fused instance)
+    const bool alt = I.pp && ((I.nt - nt) & 1) != 0;
+    const float *vxc = alt ? I.vx_b : I.vx, *vyc = alt ? I.vy_b : I.vy;
+    const float *sxxc = alt ? I.sxx_b : I.sxx, *syyc = alt ? I.syy_b : I.syy;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        float v = I.vy[(long long)(I.ny / 2) * P + I.nx / 2];
+        float v = vyc[(long long)(I.ny / 2) * P + I.nx / 2];
         if (isnan(v)) atomicOr(I.flag, 1);
     }
     if (I.mode == 1 || !I.seismo) return;
@@ -1196,18 +1221,18 @@ __global__ void k_seismo(const Inst *__restrict__ insts, const int *__restrict__
         const long long s = (long long)(nt - 1) * I.ntr + itr;
         const int S = I.seismo;
         if (S == 1 || S == 4) {
-            I.sec[0 * slab + s] = I.vx[o];
-            I.sec[1 * slab + s] = I.vy[o];
+            I.sec[0 * slab + s] = vxc[o];
+            I.sec[1 * slab + s] = vyc[o];
         }
-        if (S == 2 || S == 4) I.sec[2 * slab + s] = __fsub_rn(-I.sxx[o], I.syy[o]);
+        if (S == 2 || S == 4) I.sec[2 * slab + s] = __fsub_rn(-sxxc[o], syyc[o]);
         if (S == 3 || S == 4) {
             float vxx = 0.0f, vyy = 0.0f, vyx = 0.0f, vxy = 0.0f;
             for (int m = 1; m <= R; m++) {
                 const float h = I.hc[m];
-                vxx = __fadd_rn(vxx, __fmul_rn(h, __fsub_rn(I.vx[o + m - 1], I.vx[o - m])));
-                vyy = __fadd_rn(vyy, __fmul_rn(h, __fsub_rn(I.vy[o + (m - 1) * P], I.vy[o - m * P])));
-                vyx = __fadd_rn(vyx, __fmul_rn(h, __fsub_rn(I.vy[o + m], I.vy[o - m + 1])));
-                vxy = __fadd_rn(vxy, __fmul_rn(h, __fsub_rn(I.vx[o + m * P], I.vx[o - (m - 1) * P])));
+                vxx = __fadd_rn(vxx, __fmul_rn(h, __fsub_rn(vxc[o + m - 1], vxc[o - m])));
+                vyy = __fadd_rn(vyy, __fmul_rn(h, __fsub_rn(vyc[o + (m - 1) * P], vyc[o - m * P])));
+                vyx = __fadd_rn(vyx, __fmul_rn(h, __fsub_rn(vyc[o + m], vyc[o - m + 1])));
+                vxy = __fadd_rn(vxy, __fmul_rn(h, __fsub_rn(vxc[o + m * P], vxc[o - (m - 1) * P])));
             }
             const float dhi = I.dhi_el;
             vxx = __fmul_rn(vxx, dhi);

@@ -63,6 +63,7 @@ __global__ void __launch_bounds__(TMA_W) k_update_v_tma(const Inst *__restrict__
 {
     extern __shared__ __align__(128) float smem[];
     const Inst &I = insts[blockIdx.y];
+    if (I.pp) return;   // the fused step handles this instance
     const int nt = *ntb + off - I.t0;   // the instance's own time step
     if (nt < 1 || nt > I.nt) return;
     StripGeom g;
@@ -282,6 +283,7 @@ __global__ void __launch_bounds__(TMA_W) k_update_s_el_tma(const Inst *__restric
 {
     extern __shared__ __align__(128) float smem[];
     const Inst &I = insts[blockIdx.y];
+    if (I.pp) return;   // the fused step handles this instance
     const int nt = *ntb + off - I.t0;   // the instance's own time step
     if (nt < 1 || nt > I.nt) return;
     StripGeom g;

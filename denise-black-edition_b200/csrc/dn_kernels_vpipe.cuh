@@ -53,6 +53,7 @@ __global__ void __launch_bounds__(VP_THREADS, 3) k_update_v_pipe(const Inst *__r
 {
     extern __shared__ __align__(128) float smem[];
     const Inst &I = insts[blockIdx.y];
+    if (I.pp) return;   // the fused step handles this instance
     const int nt = *ntb + off - I.t0;   // the instance's own time step
     if (nt < 1 || nt > I.nt) return;
     const int tiles_x = (I.nx + VP_W - 1) / VP_W;

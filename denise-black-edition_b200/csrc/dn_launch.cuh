@@ -6,6 +6,7 @@
 
 #include "dn_kernels_tma.cuh"
 #include "dn_kernels_vpipe.cuh"
+#include "dn_kernels_fused.cuh"
 
 namespace dn {
 
@@ -20,6 +21,9 @@ struct LaunchCfg {
     dim3 vgrid; // its grid: strips of VP_W columns x vsh rows per instance
     int vsh;
     bool any_surf, any_src_s, any_store, any_adj, any_rec;
+    bool any_fused;   // some instance runs the fused elastic step (Inst::pp)
+    bool any_plain;   // some instance runs the separate velocity / stress kernels
+    dim3 fgrid;       // grid of the fused step: its tiles per instance
 };
 
 // marks (optional, profiling only): 9 events recorded around the 8 kernel slots

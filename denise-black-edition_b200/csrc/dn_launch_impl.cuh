@@ -11,15 +11,26 @@ void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int
                           cudaEvent_t *marks)
 {
     MARK(0);
-    if (c.vpipe) k_update_v_pipe<R, X><<<c.vgrid, VP_THREADS, vpipe_smem_bytes(), st>>>(d, ntb, off, c.vsh);
-    else if (c.tma) k_update_v_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QV>(slot_floats_v()), st>>>(d, ntb, off);
-    else if (c.pack) k_update_v2<R, X><<<c.tile_grid, c.bx / 2, 0, st>>>(d, ntb, off);
-    else k_update_v<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
+    if (c.any_fused) {   // velocity, sources, stress and free surface of the fused instances
+        k_step_el_fused<R, X><<<c.fgrid, FZ_NP, fz_ring_bytes(R), st>>>(d, ntb, off);
+        nl++;
+    }
+    if (c.any_plain) {
+        if (c.vpipe) k_update_v_pipe<R, X><<<c.vgrid, VP_THREADS, vpipe_smem_bytes(), st>>>(d, ntb, off, c.vsh);
+        else if (c.tma)
+            k_update_v_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QV>(slot_floats_v()), st>>>(d, ntb, off);
+        else if (c.pack) k_update_v2<R, X><<<c.tile_grid, c.bx / 2, 0, st>>>(d, ntb, off);
+        else k_update_v<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
+    }
     MARK(1);
-    k_inject_v<<<c.src_grid, 128, 0, st>>>(d, ntb, off);
+    if (c.any_plain) {
+        k_inject_v<<<c.src_grid, 128, 0, st>>>(d, ntb, off);
+        nl += 2;
+    }
     MARK(2);
-    nl += 2;
-    if (c.L == 0) {
+    if (!c.any_plain) {
+        // every instance took the fused step
+    } else if (c.L == 0) {
         if (c.tma)
             k_update_s_el_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QS_EL>(slot_floats_s_el()), st>>>(d, ntb, off);
         else if (c.pack) k_update_s_el2<R, X><<<c.tile_grid, c.bx / 2, 0, st>>>(d, ntb, off);
@@ -44,14 +55,14 @@ void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int
         default: k_update_s_vi<R, 5, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
         }
     }
-    nl++;
+    if (c.any_plain) nl++;
     MARK(3);
-    if (c.any_src_s) {
+    if (c.any_src_s && c.any_plain) {
         k_inject_s<<<c.src_grid, 128, 0, st>>>(d, ntb, off);
         nl++;
     }
     MARK(4);
-    if (c.any_surf) {
+    if (c.any_surf && c.any_plain) {
         if (c.L == 0) {
             k_surface_el<R, X><<<c.surf_grid, 128, 0, st>>>(d, ntb, off);
         } else {

@@ -35,7 +35,7 @@ MODE_FORWARD, MODE_ADJOINT, MODE_OBJECTIVE = 0, 1, 2
 SNAP_F32, SNAP_F16, SNAP_BF16 = 0, 1, 2
 ACC_F32, ACC_F64 = 0, 1
 ARITH_EXACT, ARITH_FMA = 0, 1
-KERN_PAIRED, KERN_COLUMN, KERN_VPIPE = 0, 1, 2
+KERN_PAIRED, KERN_COLUMN, KERN_VPIPE, KERN_FUSED = 0, 1, 2, 3
 SEC_VX, SEC_VY, SEC_P, SEC_CURL, SEC_DIV = 0, 1, 2, 3, 4
 
 
@@ -195,6 +195,7 @@ SIGNATURES = {
     "dn_set_kernel_rule": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
                                           ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "dn_get_kernel_choice": (ctypes.c_int, [_P(Params), _c_int_p, _c_int_p, _c_int_p]),
+    "dn_shot_kernel": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
     "dn_dot": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _c_double_p]),
     "dn_lbfgs_create": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int, _P(_vp)]),
     "dn_lbfgs_destroy": (ctypes.c_int, [_vp]),

@@ -312,6 +312,12 @@ class Shot:
     def run_steps(self, mode, nt0, nt1):
         check(lib.dn_run_steps(self.handle, mode, nt0, nt1))
 
+    def kernel(self):
+        """(kernel variant, whether forward runs take the fused elastic step)"""
+        v, f = ctypes.c_int(), ctypes.c_int()
+        check(lib.dn_shot_kernel(self.handle, ctypes.byref(v), ctypes.byref(f)))
+        return v.value, bool(f.value)
+
 
 def tdfilt(traces, dt, order, fc_low, fc_high=0.0, device=0):
     """apply_tdfilt: Butterworth low-pass at fc_low, then high-pass at fc_high if > 0, of

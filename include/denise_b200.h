@@ -432,6 +432,9 @@ int dn_get_tile_shape(const dn_params *p, int *bx, int *zch);
 #define DN_KERN_PAIRED 0   /* two adjacent columns per thread, packed FP32x2 arithmetic (default) */
 #define DN_KERN_COLUMN 1   /* one column per thread, z stencils in register windows */
 #define DN_KERN_VPIPE 2    /* paired, with the velocity update fed by a warp-specialised copy pipeline */
+#define DN_KERN_FUSED 3    /* elastic shots without snapshots: velocity, force sources, stress,
+                              explosive source and free surface of a time step in one kernel
+                              (fields in two alternating buffers; other shots fall back to PAIRED) */
 /* A rule as dn_set_tile_shape's, for shots that store snapshots (store 1), that
  * do not (0) or both (-1), which also picks the kernel variant (-1: default).
  * A batch runs the variant of its first shot. */
@@ -439,6 +442,10 @@ int dn_set_kernel_rule(int fdorder, int L, int store, long long cells_min, long 
                        int variant);
 /* the tile shape and kernel variant a new shot with these parameters gets */
 int dn_get_kernel_choice(const dn_params *p, int *bx, int *zch, int *variant);
+/* a shot's kernel variant, and 1 in *fused when its forward runs take the fused
+ * elastic step (DN_KERN_FUSED and eligible: elastic, no snapshots, at most 32
+ * source cells, no moment-tensor source; environment DN_FUSED=1 / 0 forces it) */
+int dn_shot_kernel(const dn_shot *s, int *variant, int *fused);
 
 /* ---- FWI outer loop (FP64) ------------------------------------------------- */
 /* Deterministic FP64 dot product of two device vectors (fixed reduction order). */
