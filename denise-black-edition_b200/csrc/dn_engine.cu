@@ -168,6 +168,7 @@ struct dn_shot {
     float *d_snap_scale = nullptr;
     int nsnap = 0, zch = 16, bx = 128, tiles_x = 0, tiles = 0;
     int kern = DN_KERN_PAIRED;     // stencil kernel variant (the batch runs its first shot's)
+    bool auto_rows = false;        // tile rows chosen per batch (batch_rows)
     // fused elastic step (DN_KERN_FUSED on an eligible shot): the second set of fields and
     // velocity CPML memory (inside dstate, so zeroed with it) and the tile rows
     bool fz = false;
@@ -492,9 +493,10 @@ static std::vector<TileRule> g_tile_rules;
 
 static bool tile_ok(int bx, int zch) { return bx >= 32 && bx <= 256 && (bx % 32) == 0 && zch >= 1 && zch <= 256; }
 
-static void tile_choice(const dn_params *p, int &bx, int &zch, int &variant)
+static void tile_choice(const dn_params *p, int &bx, int &zch, int &variant, bool *deflt = nullptr)
 {
     variant = DN_KERN_PAIRED;
+    bool from_rule = false;
     // default tiles: 128 x 8 for forward shots of 480 k cells and more (batches
     // of 32 and 64 shots of 2000 x 600 cells step 2.3-4.1 % faster than at
     // 128 x 4), 128 x 4 for smaller forward grids (32 shots of 600 x 300: 3-8 %
@@ -513,6 +515,7 @@ static void tile_choice(const dn_params *p, int &bx, int &zch, int &variant)
                 bx = r.bx;
                 zch = r.zch;
                 if (r.variant >= 0) variant = r.variant;
+                from_rule = true;
             }
     }
     const char *ev = getenv("DN_TILE");
@@ -521,8 +524,26 @@ static void tile_choice(const dn_params *p, int &bx, int &zch, int &variant)
         if (sscanf(ev, "%dx%d", &a, &b) == 2 && tile_ok(a, b)) {
             bx = a;
             zch = b;
+            from_rule = true;
         }
     }
+    if (deflt) *deflt = !from_rule;
+}
+
+// Rows per tile of a batch of shots that keep their tiles open (no snapshots, no
+// rule, no DN_TILE): the best of 1, 2, 4, 8 rows depends on the cells of the whole
+// batch, not of one shot.  Measured on a B200 (600 x 300 and 2000 x 600 grids, 1-32
+// shots, forward): one row up to 1.3 M cells (one 600 x 300 shot: 24.0 us a step
+// against 40.8 at 4 rows), two up to 5 M, four up to 16 M (viscoelastic: 30 M), eight
+// above (64 shots of 2000 x 600).  DN_AUTO_ROWS=0 keeps each shot's own tile.
+static int batch_rows(long long cells, int L)
+{
+    const char *ev = getenv("DN_AUTO_ROWS");
+    if (ev && strcmp(ev, "0") == 0) return 0;
+    if (cells < 1300000) return 1;
+    if (cells < 5000000) return 2;
+    if (cells < (L > 0 ? 30000000LL : 16000000LL)) return 4;
+    return 8;
 }
 
 static void tile_shape(const dn_params *p, int &bx, int &zch)
@@ -687,7 +708,9 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
     s->rec_i.assign(acq->rec_i, acq->rec_i + acq->ntr);
     s->rec_j.assign(acq->rec_j, acq->rec_j + acq->ntr);
     s->quelltyp_last = acq->nsrc > 0 ? s->src_type[acq->nsrc - 1] : 0;
-    tile_choice(p, s->bx, s->zch, s->kern);
+    bool deflt = false;
+    tile_choice(p, s->bx, s->zch, s->kern, &deflt);
+    s->auto_rows = deflt && !p->store_snapshots;
     shot_counts(p, s->bx, s->zch, s->tiles_x, s->tiles, s->nsnap);
     s->acc64 = p->grad_accum == DN_ACC_F64;
 
@@ -865,7 +888,18 @@ static void *acc_ptr(const dn_shot *s, int k)
 // a forward run (mode 0 or 2) of a shot with the second field set takes the fused step
 static bool runs_fused(const dn_shot *s, int mode) { return s->fz && (mode == 0 || mode == 2); }
 
-static Inst make_inst(const dn_shot *s, int mode)
+// rows per tile of shot s in a batch configured as c
+static int eff_rows(const dn_shot *s, const LaunchCfg *c)
+{
+    return (c && c->auto_zch > 0 && s->auto_rows) ? c->auto_zch : s->zch;
+}
+static int eff_tiles(const dn_shot *s, const LaunchCfg *c)
+{
+    const int z = eff_rows(s, c);
+    return ((s->p.nx + s->bx - 1) / s->bx) * ((s->p.ny + z - 1) / z);
+}
+
+static Inst make_inst(const dn_shot *s, int mode, const LaunchCfg *c = nullptr)
 {
     const dn_model *m = s->m;
     const dn_params &p = s->p;
@@ -879,9 +913,9 @@ static Inst make_inst(const dn_shot *s, int mode)
     I.free_surf = p.free_surf;
     I.L = p.L;
     I.mode = mode;
-    I.zch = s->zch;
+    I.zch = eff_rows(s, c);
     I.tiles_x = s->tiles_x;
-    I.tiles = s->tiles;
+    I.tiles = eff_tiles(s, c);
     I.store = (mode == 0) && p.store_snapshots && s->nsnap > 0;
     I.dtinv = std::max(p.dtinv, 1);
     I.nsnap = s->nsnap;
@@ -1134,6 +1168,12 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c, con
     c.any_surf = c.any_src_s = c.any_store = c.any_adj = c.any_rec = false;
     c.any_fused = c.any_plain = false;
     int maxtiles = 0, maxsrc = 1, maxnx = 1, maxtr = 1, maxft = 1;
+    {
+        long long cells = 0;
+        for (int k = 0; k < n; k++)
+            if (shots[k]) cells += (long long)shots[k]->p.nx * shots[k]->p.ny;
+        c.auto_zch = c.tma ? 0 : batch_rows(cells, p0.L);   // the row pipeline keeps its measured tiles
+    }
     for (int k = 0; k < n; k++) {
         const dn_shot *s = shots[k];
         if (!s) return dn_fail(DN_EINVAL, "dn_run: null shot %d", k);
@@ -1149,7 +1189,7 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c, con
                 if (s->src_type[l] == 5)
                     return dn_fail(DN_ENOTSUP, "moment-tensor sources are not supported in the adjoint pass");
         }
-        maxtiles = std::max(maxtiles, s->tiles);
+        maxtiles = std::max(maxtiles, eff_tiles(s, &c));
         if (runs_fused(s, m)) {
             c.any_fused = true;
             const int fwd = fz_width(s->p.fdorder / 2);
@@ -1408,7 +1448,7 @@ extern "C" int dn_run(dn_shot *const *shots, int n, int mode)
         b->device = device;
         b->mode = mode;
         b->shots.assign(shots, shots + n);
-        for (int k = 0; k < n; k++) b->h_insts.push_back(make_inst(shots[k], mode));
+        for (int k = 0; k < n; k++) b->h_insts.push_back(make_inst(shots[k], mode, &c));
         if (dn_malloc(&b->d_insts, sizeof(Inst) * n) != cudaSuccess) {
             delete b;
             return dn_fail(DN_ENOMEM, "dn_run: descriptor allocation failed");
@@ -1471,7 +1511,7 @@ static int run_direct(dn_shot *s, int mode, int nt0, int nt1, bool zero)
     CU(cudaSetDevice(s->m->device));
     st = prepare_launch(c);
     if (st) return st;
-    Inst h = make_inst(s, mode);
+    Inst h = make_inst(s, mode, &c);
     if (h.pp && (nt0 != 1 || nt1 != s->p.nt)) {
         // a partial range runs the separate kernels on the primary buffers, so that the state
         // between calls stays where dn_shot_get_field and the next range read it
@@ -1635,13 +1675,15 @@ static int queue_capture(dn_queue *q)
     for (int k = 0; k < n; k++) {
         shots[k] = q->active[k].s;
         modes[k] = q->active[k].mode;
-        Inst I = make_inst(shots[k], modes[k]);
-        I.t0 = (int)q->active[k].t0;
-        q->h_insts.push_back(I);
     }
     LaunchCfg c;
     int st = check_batch(shots.data(), n, 0, c, modes.data());
     if (st) return st;
+    for (int k = 0; k < n; k++) {
+        Inst I = make_inst(shots[k], modes[k], &c);
+        I.t0 = (int)q->active[k].t0;
+        q->h_insts.push_back(I);
+    }
     st = prepare_launch(c);
     if (st) return st;
     if (n > q->cap_insts) {
@@ -2193,7 +2235,7 @@ extern "C" int dn_profile_steps(dn_shot *const *shots, int n, int mode, int nste
     std::vector<Inst> h;
     int maxnt = 0;
     for (int k = 0; k < n; k++) {
-        h.push_back(make_inst(shots[k], mode));
+        h.push_back(make_inst(shots[k], mode, &c));
         maxnt = std::max(maxnt, shots[k]->p.nt);
     }
     nsteps = std::min(nsteps, maxnt);

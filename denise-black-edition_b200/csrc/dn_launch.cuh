@@ -13,6 +13,7 @@ namespace dn {
 struct LaunchCfg {
     dim3 tile_grid, src_grid, surf_grid, rec_grid;
     int bx;
+    int auto_zch;     // rows per tile of the shots whose tiles the batch chooses (0: their own)
     int R, L;
     bool exact;
     bool tma;   // stencil kernels fed by the bulk-copy row pipeline
