@@ -1773,17 +1773,55 @@ extern "C" int dn_queue_step(dn_queue *q, dn_shot **done, int *status, int cap, 
 // ---------------------------------------------------------------------------
 // results
 // ---------------------------------------------------------------------------
+static std::mutex g_sec_mu;
+static std::map<int, std::pair<float *, size_t>> g_sec_scratch;   // device -> (buffer, floats)
+
+// [nt][ntr] (the order the receiver kernel writes) to [ntr][nt] (trace order), 32 x 32 tiles
+__global__ void k_sec_transpose(const float *__restrict__ in, float *__restrict__ out, int nt, int ntr)
+{
+    __shared__ float tile[32][33];
+    const int r0 = blockIdx.x * 32, t0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int t = t0 + k, r = r0 + threadIdx.x;
+        if (t < nt && r < ntr) tile[k][threadIdx.x] = in[(size_t)t * ntr + r];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = r0 + k, t = t0 + threadIdx.x;
+        if (r < ntr && t < nt) out[(size_t)r * nt + t] = tile[threadIdx.x][k];
+    }
+}
+
 extern "C" int dn_shot_get_sections(const dn_shot *s, int comp, float *out)
 {
     if (!s || !out) return dn_fail(DN_EINVAL, "null argument");
     if (comp < 0 || comp > 4) return dn_fail(DN_EINVAL, "bad section component %d", comp);
     const int nt = s->p.nt, ntr = s->ntr;
     if (ntr == 0) return DN_OK;
-    std::vector<float> tmp((size_t)nt * ntr);
-    CU(cudaSetDevice(s->m->device));
-    CU(cudaMemcpy(tmp.data(), s->d_sec + (size_t)comp * nt * ntr, tmp.size() * 4, cudaMemcpyDeviceToHost));
-    for (int t = 0; t < nt; t++)
-        for (int r = 0; r < ntr; r++) out[(size_t)r * nt + t] = tmp[(size_t)t * ntr + r];
+    const int device = s->m->device;
+    CU(cudaSetDevice(device));
+    // transposed on the device into a per-device scratch buffer (kept between calls: a
+    // release would wait for the whole device, run queues in flight included), then one
+    // contiguous copy; the legacy default stream orders both after the runs, which end
+    // with a stream synchronisation, and does not wait for the library's other streams
+    const size_t n = (size_t)nt * ntr;
+    std::lock_guard<std::mutex> lk(g_sec_mu);
+    auto &sc = g_sec_scratch[device];
+    if (sc.second < n) {
+        if (sc.first) cudaFree(sc.first);
+        sc = {nullptr, 0};
+        if (cudaMalloc(&sc.first, n * 4) != cudaSuccess) {
+            cudaGetLastError();
+            sc.first = nullptr;
+            return dn_fail(DN_ENOMEM, "dn_shot_get_sections: device allocation failed");
+        }
+        sc.second = n;
+    }
+    k_sec_transpose<<<dim3((ntr + 31) / 32, (nt + 31) / 32), dim3(32, 8)>>>(s->d_sec + (size_t)comp * n, sc.first, nt,
+                                                                            ntr);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(out, sc.first, n * 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "dn_shot_get_sections: %s", cudaGetErrorString(e));
     return DN_OK;
 }
 

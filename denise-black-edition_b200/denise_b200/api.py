@@ -244,7 +244,7 @@ class Shot:
             pass
 
     def sections(self, comp=_lib.SEC_VX):
-        out = np.zeros((self.ntr, self.model.params.nt), np.float32)
+        out = np.empty((self.ntr, self.model.params.nt), np.float32)
         check(lib.dn_shot_get_sections(self.handle, comp, fptr(out)))
         return out
 
