@@ -18,6 +18,7 @@
 #include "dn_internal.h"
 #include "dn_precond.h"
 #include "dn_launch.cuh"
+#include "dn_materials.cuh"
 
 using namespace dn;
 
@@ -297,6 +298,61 @@ static int fastdiv_setup(int device, float dh, int *ok, float *y)
     return DN_OK;
 }
 
+// The material planes of m from the model files on the device (k_file_to_plane, k_materials),
+// enqueued on stream cs; the staging of the files is released in stream order.
+static cudaError_t device_materials(dn_model *m, const float *vp, const float *vs, const float *rho, const float *qp,
+                                    const float *qs, cudaStream_t cs)
+{
+    const dn_params &p = m->p;
+    const Layout &L = m->lay;
+    const size_t n = (size_t)p.nx * p.ny;
+    const bool visc = p.L > 0, q = visc && p.honor_q;
+    const int nraw = q ? 5 : 3;
+    cudaError_t e = cudaMemsetAsync(m->dmat, 0, (size_t)m->nfields * L.plane * 4, cs);
+    float *raw = nullptr, *qpl = nullptr;
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)&raw, n * nraw * 4, cs);
+    if (e == cudaSuccess && q) e = cudaMallocAsync((void **)&qpl, (size_t)2 * L.plane * 4, cs);
+    if (e == cudaSuccess && q) e = cudaMemsetAsync(qpl, 0, (size_t)2 * L.plane * 4, cs);
+    const float *src[5] = {rho, vs, vp, qs, qp};
+    for (int k = 0; k < nraw && e == cudaSuccess; k++)
+        e = cudaMemcpyAsync(raw + k * n, src[k], n * 4, cudaMemcpyHostToDevice, cs);
+    if (e == cudaSuccess) {
+        const dim3 tg((p.ny + 31) / 32, (p.nx + 31) / 32), tb(32, 8);
+        float *dst[5] = {m->field(MF_RHO), m->field(MF_VS), m->field(MF_VP), q ? qpl + L.origin : nullptr,
+                         q ? qpl + L.plane + L.origin : nullptr};
+        for (int k = 0; k < nraw; k++) k_file_to_plane<<<tg, tb, 0, cs>>>(raw + k * n, dst[k], p.nx, p.ny, L.pitch);
+        MatPlanes M;
+        M.rho = m->field(MF_RHO);
+        M.vs = m->field(MF_VS);
+        M.vp = m->field(MF_VP);
+        M.qs = q ? dst[3] : nullptr;
+        M.qp = q ? dst[4] : nullptr;
+        M.rip = m->field(MF_RIP);
+        M.rjp = m->field(MF_RJP);
+        M.uipjp = m->field(MF_UIPJP);
+        M.mu = m->field(MF_MU);
+        M.lam = m->field(MF_LAM);
+        M.gmuss = m->field(MF_GMUSS);
+        M.glamss = m->field(MF_GLAMSS);
+        M.c_muipjp = visc ? m->field(MF_CMUIPJP) : nullptr;
+        M.c_tausipjp = visc ? m->field(MF_CTAUSIPJP) : nullptr;
+        M.c_mu = visc ? m->field(MF_CMU) : nullptr;
+        M.c_taus = visc ? m->field(MF_CTAUS) : nullptr;
+        M.c_pi = visc ? m->field(MF_CPI) : nullptr;
+        M.c_taup = visc ? m->field(MF_CTAUP) : nullptr;
+        M.pitch = L.pitch;
+        M.nx = p.nx;
+        M.ny = p.ny;
+        M.visc = visc;
+        M.sumu = visc ? dn_visc_sumu(&p) : 0.0f;
+        k_materials<<<dim3((p.nx + 127) / 128, p.ny), 128, 0, cs>>>(M);
+        e = cudaGetLastError();
+    }
+    if (raw) cudaFreeAsync(raw, cs);
+    if (qpl) cudaFreeAsync(qpl, cs);
+    return e;
+}
+
 extern "C" int dn_model_create(const dn_params *p, const float *vp, const float *vs, const float *rho,
                                const float *qp, const float *qs, int device, dn_model **out)
 {
@@ -319,46 +375,57 @@ extern "C" int dn_model_create(const dn_params *p, const float *vp, const float 
     }
     const Layout &L = m->lay;
     const size_t n = (size_t)p->nx * p->ny;
-    std::vector<float> host((size_t)m->nfields * L.plane, 0.0f);
-    std::vector<float> uipjp(n), rip(n), rjp(n), mu(n), lam(n), gmuss(n), glamss(n);
-    st = dn_average_materials(p, vp, vs, rho, uipjp.data(), rip.data(), rjp.data());
-    if (st) {
-        delete m;
-        return st;
-    }
-    for (size_t k = 0; k < n; k++) {
-        // update_s_elastic_PML_PSV.c:442-444 and psv.c:333-334 (float, with the 2.0 promotion)
-        float u = vs[k], pi = vp[k], r = rho[k];
-        mu[k] = r * u * u;
-        lam[k] = r * ((pi * pi) - 2 * u * u);
-        float muss = r * u * u;
-        gmuss[k] = muss;
-        glamss[k] = (float)((double)(r * pi * pi) - 2.0 * (double)muss);
-    }
-    file_to_padded(L, rip.data(), host, MF_RIP * L.plane);
-    file_to_padded(L, rjp.data(), host, MF_RJP * L.plane);
-    file_to_padded(L, uipjp.data(), host, MF_UIPJP * L.plane);
-    file_to_padded(L, mu.data(), host, MF_MU * L.plane);
-    file_to_padded(L, lam.data(), host, MF_LAM * L.plane);
-    file_to_padded(L, rho, host, MF_RHO * L.plane);
-    file_to_padded(L, vp, host, MF_VP * L.plane);
-    file_to_padded(L, vs, host, MF_VS * L.plane);
-    file_to_padded(L, gmuss.data(), host, MF_GMUSS * L.plane);
-    file_to_padded(L, glamss.data(), host, MF_GLAMSS * L.plane);
-    std::vector<float> surf;
-    if (p->L > 0) {
-        std::vector<float> a(n), b(n), c(n), d(n), e(n), f(n);
-        st = dn_visc_cell_factors(p, vp, vs, rho, qp, qs, a.data(), b.data(), c.data(), d.data(), e.data(), f.data());
+    // the material planes come from the device (k_materials) unless DN_HOST_MATERIALS=1 asks
+    // for the host set-up below; both give the same bits
+    const char *hm = getenv("DN_HOST_MATERIALS");
+    const bool host_mat = hm && strcmp(hm, "0") != 0;
+    std::vector<float> host;
+    std::vector<float> uipjp, rip, rjp, mu, lam, gmuss, glamss;
+    if (host_mat) {
+        host.assign((size_t)m->nfields * L.plane, 0.0f);
+        uipjp.resize(n), rip.resize(n), rjp.resize(n), mu.resize(n), lam.resize(n), gmuss.resize(n), glamss.resize(n);
+        st = dn_average_materials(p, vp, vs, rho, uipjp.data(), rip.data(), rjp.data());
         if (st) {
             delete m;
             return st;
         }
-        file_to_padded(L, a.data(), host, MF_CMUIPJP * L.plane);
-        file_to_padded(L, b.data(), host, MF_CTAUSIPJP * L.plane);
-        file_to_padded(L, c.data(), host, MF_CMU * L.plane);
-        file_to_padded(L, d.data(), host, MF_CTAUS * L.plane);
-        file_to_padded(L, e.data(), host, MF_CPI * L.plane);
-        file_to_padded(L, f.data(), host, MF_CTAUP * L.plane);
+        for (size_t k = 0; k < n; k++) {
+            // update_s_elastic_PML_PSV.c:442-444 and psv.c:333-334 (float, with the 2.0 promotion)
+            float u = vs[k], pi = vp[k], r = rho[k];
+            mu[k] = r * u * u;
+            lam[k] = r * ((pi * pi) - 2 * u * u);
+            float muss = r * u * u;
+            gmuss[k] = muss;
+            glamss[k] = (float)((double)(r * pi * pi) - 2.0 * (double)muss);
+        }
+        file_to_padded(L, rip.data(), host, MF_RIP * L.plane);
+        file_to_padded(L, rjp.data(), host, MF_RJP * L.plane);
+        file_to_padded(L, uipjp.data(), host, MF_UIPJP * L.plane);
+        file_to_padded(L, mu.data(), host, MF_MU * L.plane);
+        file_to_padded(L, lam.data(), host, MF_LAM * L.plane);
+        file_to_padded(L, rho, host, MF_RHO * L.plane);
+        file_to_padded(L, vp, host, MF_VP * L.plane);
+        file_to_padded(L, vs, host, MF_VS * L.plane);
+        file_to_padded(L, gmuss.data(), host, MF_GMUSS * L.plane);
+        file_to_padded(L, glamss.data(), host, MF_GLAMSS * L.plane);
+    }
+    std::vector<float> surf;
+    if (p->L > 0) {
+        if (host_mat) {
+            std::vector<float> a(n), b(n), c(n), d(n), e(n), f(n);
+            st = dn_visc_cell_factors(p, vp, vs, rho, qp, qs, a.data(), b.data(), c.data(), d.data(), e.data(),
+                                      f.data());
+            if (st) {
+                delete m;
+                return st;
+            }
+            file_to_padded(L, a.data(), host, MF_CMUIPJP * L.plane);
+            file_to_padded(L, b.data(), host, MF_CTAUSIPJP * L.plane);
+            file_to_padded(L, c.data(), host, MF_CMU * L.plane);
+            file_to_padded(L, d.data(), host, MF_CTAUS * L.plane);
+            file_to_padded(L, e.data(), host, MF_CPI * L.plane);
+            file_to_padded(L, f.data(), host, MF_CTAUP * L.plane);
+        }
         float eta[DN_MAX_L];
         dn_visc_eta(p, eta, nullptr);
         for (int l = 0; l < p->L; l++) {
@@ -423,23 +490,32 @@ extern "C" int dn_model_create(const dn_params *p, const float *vp, const float 
         return dn_fail(DN_EDEVICE, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
     }
     size_t gbytes = 3 * n * (m->grad64 ? 8 : 4);
-    if (dn_malloc(&m->dmat, host.size() * 4) != cudaSuccess || dn_malloc(&m->dpml, pml.size() * 4) != cudaSuccess ||
+    const size_t mat_bytes = (size_t)m->nfields * L.plane * 4;
+    if (dn_malloc(&m->dmat, mat_bytes) != cudaSuccess || dn_malloc(&m->dpml, pml.size() * 4) != cudaSuccess ||
         dn_malloc(&m->dgrad, gbytes) != cudaSuccess ||
         (!surf.empty() && dn_malloc(&m->dsurf, surf.size() * 4) != cudaSuccess)) {
         cudaGetLastError();
         dn_model_destroy(m);
         return dn_fail(DN_ENOMEM, "dn_model_create: device allocation failed");
     }
-    if (cudaMemcpy(m->dmat, host.data(), host.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(m->dpml, pml.data(), pml.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(m->dgrad, 0, gbytes) != cudaSuccess ||
-        (!surf.empty() && cudaMemcpy(m->dsurf, surf.data(), surf.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)) {
+    // uploads on a private stream, so that creating a model does not wait for runs in flight
+    cudaStream_t cs = nullptr;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+        dn_model_destroy(m);
+        return dn_fail(DN_EDEVICE, "dn_model_create: stream creation failed");
+    }
+    bool up = cudaMemcpyAsync(m->dpml, pml.data(), pml.size() * 4, cudaMemcpyHostToDevice, cs) == cudaSuccess &&
+              cudaMemsetAsync(m->dgrad, 0, gbytes, cs) == cudaSuccess &&
+              (surf.empty() ||
+               cudaMemcpyAsync(m->dsurf, surf.data(), surf.size() * 4, cudaMemcpyHostToDevice, cs) == cudaSuccess);
+    if (up && host_mat) up = cudaMemcpyAsync(m->dmat, host.data(), mat_bytes, cudaMemcpyHostToDevice, cs) == cudaSuccess;
+    if (up && !host_mat) up = device_materials(m, vp, vs, rho, qp, qs, cs) == cudaSuccess;
+    const bool done = up && cudaStreamSynchronize(cs) == cudaSuccess;
+    cudaStreamDestroy(cs);
+    if (!done) {
+        cudaGetLastError();
         dn_model_destroy(m);
         return dn_fail(DN_EDEVICE, "dn_model_create: upload failed");
-    }
-    if (cudaDeviceSynchronize() != cudaSuccess) {
-        dn_model_destroy(m);
-        return dn_fail(DN_EDEVICE, "dn_model_create: upload did not complete");
     }
     st = fastdiv_setup(device, p->dh, &m->fastdiv, &m->rdh);
     if (st) {
@@ -466,6 +542,20 @@ extern "C" int dn_model_params(const dn_model *m, dn_params *out)
 {
     if (!m || !out) return dn_fail(DN_EINVAL, "null argument");
     *out = m->p;
+    return DN_OK;
+}
+
+extern "C" int dn_model_get_material(const dn_model *m, int which, float *out)
+{
+    if (!m || !out) return dn_fail(DN_EINVAL, "null argument");
+    if (which < 0 || which >= m->nfields)
+        return dn_fail(DN_EINVAL, "dn_model_get_material: plane %d of %d", which, m->nfields);
+    const Layout &L = m->lay;
+    std::vector<float> h(L.plane);
+    CU(cudaSetDevice(m->device));
+    CU(cudaMemcpy(h.data(), m->dmat + (long long)which * L.plane, L.plane * 4, cudaMemcpyDeviceToHost));
+    for (int i = 1; i <= L.nx; i++)
+        for (int j = 1; j <= L.ny; j++) out[(size_t)(i - 1) * L.ny + (j - 1)] = h[L.origin + (size_t)j * L.pitch + i];
     return DN_OK;
 }
 
@@ -1773,8 +1863,12 @@ extern "C" int dn_queue_step(dn_queue *q, dn_shot **done, int *status, int cap, 
 // ---------------------------------------------------------------------------
 // results
 // ---------------------------------------------------------------------------
+struct SecScratch {
+    float *d = nullptr, *h = nullptr;   // device and pinned host buffers of n floats
+    size_t n = 0;
+};
 static std::mutex g_sec_mu;
-static std::map<int, std::pair<float *, size_t>> g_sec_scratch;   // device -> (buffer, floats)
+static std::map<int, SecScratch> g_sec_scratch;
 
 // [nt][ntr] (the order the receiver kernel writes) to [ntr][nt] (trace order), 32 x 32 tiles
 __global__ void k_sec_transpose(const float *__restrict__ in, float *__restrict__ out, int nt, int ntr)
@@ -1806,22 +1900,25 @@ extern "C" int dn_shot_get_sections(const dn_shot *s, int comp, float *out)
     // with a stream synchronisation, and does not wait for the library's other streams
     const size_t n = (size_t)nt * ntr;
     std::lock_guard<std::mutex> lk(g_sec_mu);
-    auto &sc = g_sec_scratch[device];
-    if (sc.second < n) {
-        if (sc.first) cudaFree(sc.first);
-        sc = {nullptr, 0};
-        if (cudaMalloc(&sc.first, n * 4) != cudaSuccess) {
+    SecScratch &sc = g_sec_scratch[device];
+    if (sc.n < n) {
+        // grown, never shrunk: one transposed section on the device and its pinned host copy
+        if (sc.d) cudaFree(sc.d);
+        if (sc.h) cudaFreeHost(sc.h);
+        sc = SecScratch();
+        if (cudaMalloc(&sc.d, n * 4) != cudaSuccess || cudaMallocHost(&sc.h, n * 4) != cudaSuccess) {
             cudaGetLastError();
-            sc.first = nullptr;
-            return dn_fail(DN_ENOMEM, "dn_shot_get_sections: device allocation failed");
+            if (sc.d) cudaFree(sc.d);
+            sc = SecScratch();
+            return dn_fail(DN_ENOMEM, "dn_shot_get_sections: scratch allocation failed");
         }
-        sc.second = n;
+        sc.n = n;
     }
-    k_sec_transpose<<<dim3((ntr + 31) / 32, (nt + 31) / 32), dim3(32, 8)>>>(s->d_sec + (size_t)comp * n, sc.first, nt,
-                                                                            ntr);
+    k_sec_transpose<<<dim3((ntr + 31) / 32, (nt + 31) / 32), dim3(32, 8)>>>(s->d_sec + (size_t)comp * n, sc.d, nt, ntr);
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpy(out, sc.first, n * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(sc.h, sc.d, n * 4, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return dn_fail(DN_EDEVICE, "dn_shot_get_sections: %s", cudaGetErrorString(e));
+    memcpy(out, sc.h, n * 4);
     return DN_OK;
 }
 

@@ -14,6 +14,8 @@ int dn_fail(int code, const char *fmt, ...);
 int dn_visc_eta(const dn_params *p, float *eta, float *pts);
 float dn_visc_sum(const dn_params *p, float ws);
 float dn_visc_tau_from_q(float q);
+/* the sum dn_visc_cell_factors divides by: dn_visc_sum at ws = 2 pi FL[0] */
+float dn_visc_sumu(const dn_params *p);
 int dn_visc_cell_factors(const dn_params *p, const float *vp, const float *vs, const float *rho, const float *qp,
                          const float *qs, float *muipjp, float *tausipjp, float *mu, float *taus, float *pi,
                          float *taup);

@@ -404,6 +404,12 @@ int dn_prepare_visc(const dn_params *p, const float *vp, const float *vs, const 
  * coefficients from (fipjp, f, g, dip, d, e) without storing the 3L arrays:
  *   muipjp, tausipjp, mu, taus, pi, taup  (prepare_update_s_visc_PSV.c:46-60).
  * Outputs in file order. */
+float dn_visc_sumu(const dn_params *p)
+{
+    float ws = 2.0 * DN_PI * p->fl[0];
+    return dn_visc_sum(p, ws);
+}
+
 int dn_visc_cell_factors(const dn_params *p, const float *vp, const float *vs, const float *rho, const float *qp,
                          const float *qs, float *muipjp_o, float *tausipjp_o, float *mu_o, float *taus_o, float *pi_o,
                          float *taup_o)
@@ -427,8 +433,7 @@ int dn_visc_cell_factors(const dn_params *p, const float *vp, const float *vs, c
         free(T.a);
         return st;
     }
-    float ws = 2.0 * DN_PI * p->fl[0];
-    float sumu = dn_visc_sum(p, ws);
+    float sumu = dn_visc_sumu(p);
     for (int i = 1; i <= nx; i++) {       /* cells are independent: file order, contiguous in o */
         for (int j = 1; j <= ny; j++) {
             size_t o = (size_t)(i - 1) * ny + (j - 1);

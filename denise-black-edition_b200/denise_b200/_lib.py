@@ -196,6 +196,7 @@ SIGNATURES = {
                                           ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "dn_get_kernel_choice": (ctypes.c_int, [_P(Params), _c_int_p, _c_int_p, _c_int_p]),
     "dn_shot_kernel": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
+    "dn_model_get_material": (ctypes.c_int, [_vp, ctypes.c_int, _c_float_p]),
     "dn_dot": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _c_double_p]),
     "dn_lbfgs_create": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int, _P(_vp)]),
     "dn_lbfgs_destroy": (ctypes.c_int, [_vp]),

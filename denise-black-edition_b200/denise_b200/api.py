@@ -202,6 +202,16 @@ class Model:
         check(lib.dn_model_get_gradient(self.handle, *[fptr(a) for a in g]))
         return tuple(g)
 
+    MATERIALS = ("rip", "rjp", "uipjp", "mu", "lam", "rho", "vp", "vs", "muss", "lamss",
+                 "c_muipjp", "c_tausipjp", "c_mu", "c_taus", "c_pi", "c_taup")
+
+    def material(self, which):
+        """A material plane the kernels use (name from MATERIALS or its index), (nx, ny) file order."""
+        k = self.MATERIALS.index(which) if isinstance(which, str) else int(which)
+        out = np.empty((self.params.nx, self.params.ny), np.float32)
+        check(lib.dn_model_get_material(self.handle, k, fptr(out)))
+        return out
+
     def zero_gradient(self):
         check(lib.dn_model_zero_gradient(self.handle))
 

@@ -194,12 +194,21 @@ int dn_wavelet_ex(int quellart, int nt, float dt, float tshift, float fc, float 
                   float fc_spike_2, float ts_chirp, const float *file_signal, int file_ns, float *out);
 
 /* ---- models and shots (device) -------------------------------------------- */
-/* Builds every derived coefficient on the host (the functions above) and uploads
- * it to `device`.  vp, vs, rho (and qp, qs when p->L > 0) are in file order. */
+/* Uploads the model files to `device` and builds every derived coefficient
+ * there, with the float / double operations of the host functions above (the
+ * same bits; DN_HOST_MATERIALS=1 in the environment builds them on the host
+ * instead).  vp, vs, rho (and qp, qs when p->L > 0) are in file order. */
 int dn_model_create(const dn_params *p, const float *vp, const float *vs, const float *rho,
                     const float *qp, const float *qs, int device, dn_model **out);
 int dn_model_destroy(dn_model *m);
 int dn_model_params(const dn_model *m, dn_params *out);
+/* One of a model's material planes, nx*ny floats in file order:
+ * 0 rip, 1 rjp, 2 uipjp (av_rho / av_mue), 3 mu, 4 lambda, 5 rho, 6 vp, 7 vs,
+ * 8 muss, 9 lamss (the gradient's), and for L > 0: 10 mu at (i+1/2, j+1/2),
+ * 11 its tau_s, 12 mu, 13 tau_s, 14 pi, 15 tau_p (the relaxed moduli and
+ * relaxation times the viscoelastic stress update is formed from). */
+#define DN_MAT_COUNT 16
+int dn_model_get_material(const dn_model *m, int which, float *out);
 /* Bytes of device memory a model / a shot of this acquisition will hold. */
 int dn_model_footprint(const dn_params *p, size_t *bytes);
 int dn_shot_footprint(const dn_params *p, int ntr, int store_snapshots, size_t *bytes);
