@@ -906,8 +906,14 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
     s->d_signals = carve<float>(ac, std::max((size_t)acq->nsrc * p->nt, (size_t)1));
     s->d_flag = carve<int>(ac, 1);
     ok = true;
+    // uploads on a private stream, so that creating a shot does not wait for runs in flight
+    cudaStream_t us = nullptr;
+    if (cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking) != cudaSuccess) {
+        dn_shot_destroy(s);
+        return dn_fail(DN_EDEVICE, "dn_shot_create: stream creation failed");
+    }
     auto up = [&](void *dst, const void *src, size_t b) {
-        if (b && ok) ok = cudaMemcpy(dst, src, b, cudaMemcpyHostToDevice) == cudaSuccess;
+        if (b && ok) ok = cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, us) == cudaSuccess;
     };
     up(s->d_cell_i, ci.data(), ci.size() * 4);
     up(s->d_cell_j, cj.data(), cj.size() * 4);
@@ -920,16 +926,17 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
     up(s->d_nsin, nsin.data(), nsin.size() * 8);
     up(s->d_cos, cosv.data(), cosv.size() * 8);
     up(s->d_signals, s->signals.data(), s->signals.size() * 4);
-    if (ok) ok = cudaMemset(s->d_flag, 0, 4) == cudaSuccess && cudaMemset(s->d_sec, 0, sec_n * 4) == cudaSuccess &&
-                 cudaMemset(s->d_res, 0, res_n * 4) == cudaSuccess && cudaMemset(s->d_acc, 0, acc_bytes) == cudaSuccess &&
-                 cudaMemset(s->dstate, 0, s->state_bytes) == cudaSuccess;
-    if (!ok) {
+    if (ok) ok = cudaMemsetAsync(s->d_flag, 0, 4, us) == cudaSuccess &&
+                 cudaMemsetAsync(s->d_sec, 0, sec_n * 4, us) == cudaSuccess &&
+                 cudaMemsetAsync(s->d_res, 0, res_n * 4, us) == cudaSuccess &&
+                 cudaMemsetAsync(s->d_acc, 0, acc_bytes, us) == cudaSuccess &&
+                 cudaMemsetAsync(s->dstate, 0, s->state_bytes, us) == cudaSuccess;
+    const bool done = ok && cudaStreamSynchronize(us) == cudaSuccess;
+    cudaStreamDestroy(us);
+    if (!done) {
+        cudaGetLastError();
         dn_shot_destroy(s);
         return dn_fail(DN_EDEVICE, "dn_shot_create: upload failed");
-    }
-    if (cudaDeviceSynchronize() != cudaSuccess) {
-        dn_shot_destroy(s);
-        return dn_fail(DN_EDEVICE, "dn_shot_create: upload did not complete");
     }
     *out = s;
     return DN_OK;
