@@ -1689,13 +1689,24 @@ struct dn_queue {
     int device = 0, chunk = 50;
     cudaStream_t stream = nullptr;
     int *d_step = nullptr;
-    cudaEvent_t ev = nullptr;
-    bool inflight = false, dirty = true;
+    // up to two chunks in flight: while the host retires, admits and re-captures, the
+    // GPU runs the newer one; ev[head] marks the end of the older
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    long long ev_gstep[2] = {0, 0};
+    int nflight = 0, head = 0;
+    bool dirty = true;
     long long gstep = 0;                 // value of *d_step once the enqueued chunks have run
+    long long gstep_done = 0;            // value of *d_step after the chunks known to have completed
     std::vector<QSlot> active, pending;
     std::vector<Inst> h_insts;
     Inst *d_insts = nullptr;
     int cap_insts = 0;
+    // pinned staging of the descriptors, two buffers in turn: a pageable source could make the
+    // asynchronous copy wait for the chunk in flight, and the copy enqueued by the previous call
+    // may still be pending behind it
+    Inst *h_pin[2] = {nullptr, nullptr};
+    int pin_cap[2] = {0, 0};
+    int pin_k = 0;
     cudaGraphExec_t exec = nullptr;
     long long launches_per_chunk = 0;
 };
@@ -1711,7 +1722,8 @@ extern "C" int dn_queue_create(int device, int chunk, dn_queue **out)
     q->chunk = chunk;
     if (cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking) != cudaSuccess ||
         dn_malloc(&q->d_step, sizeof(int)) != cudaSuccess ||
-        cudaEventCreateWithFlags(&q->ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&q->ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&q->ev[1], cudaEventDisableTiming) != cudaSuccess ||
         cudaMemset(q->d_step, 0, sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         dn_queue_destroy(q);
@@ -1727,9 +1739,12 @@ extern "C" int dn_queue_destroy(dn_queue *q)
     cudaSetDevice(q->device);
     if (q->stream) cudaStreamSynchronize(q->stream);
     if (q->exec) cudaGraphExecDestroy(q->exec);
+    for (int k = 0; k < 2; k++)
+        if (q->h_pin[k]) cudaFreeHost(q->h_pin[k]);
     dn_free(q->d_insts);
     dn_free(q->d_step);
-    if (q->ev) cudaEventDestroy(q->ev);
+    for (int k = 0; k < 2; k++)
+        if (q->ev[k]) cudaEventDestroy(q->ev[k]);
     if (q->stream) cudaStreamDestroy(q->stream);
     delete q;
     return DN_OK;
@@ -1791,7 +1806,21 @@ static int queue_capture(dn_queue *q)
             return dn_fail(DN_ENOMEM, "dn_queue_step: descriptor allocation failed");
         q->cap_insts = n;
     }
-    CU(cudaMemcpyAsync(q->d_insts, q->h_insts.data(), sizeof(Inst) * n, cudaMemcpyHostToDevice, q->stream));
+    q->pin_k ^= 1;
+    const int pk = q->pin_k;
+    if (n > q->pin_cap[pk]) {
+        if (q->h_pin[pk]) cudaFreeHost(q->h_pin[pk]);
+        q->h_pin[pk] = nullptr;
+        q->pin_cap[pk] = 0;
+        if (cudaMallocHost(&q->h_pin[pk], sizeof(Inst) * n) != cudaSuccess) {
+            cudaGetLastError();
+            q->h_pin[pk] = nullptr;
+            return dn_fail(DN_ENOMEM, "dn_queue_step: pinned descriptor allocation failed");
+        }
+        q->pin_cap[pk] = n;
+    }
+    memcpy(q->h_pin[pk], q->h_insts.data(), sizeof(Inst) * n);
+    CU(cudaMemcpyAsync(q->d_insts, q->h_pin[pk], sizeof(Inst) * n, cudaMemcpyHostToDevice, q->stream));
     if (q->exec) {
         cudaGraphExecDestroy(q->exec);
         q->exec = nullptr;
@@ -1820,15 +1849,30 @@ extern "C" int dn_queue_step(dn_queue *q, dn_shot **done, int *status, int cap, 
     if (!q || !ndone || (cap > 0 && (!done || !status))) return dn_fail(DN_EINVAL, "dn_queue_step: bad arguments");
     *ndone = 0;
     CU(cudaSetDevice(q->device));
-    if (q->inflight) {
-        CU(cudaEventSynchronize(q->ev));
-        q->inflight = false;
+    // wait for the older of two chunks in flight; take the newer too if it has finished
+    if (q->nflight == 2) {
+        CU(cudaEventSynchronize(q->ev[q->head]));
+        q->gstep_done = q->ev_gstep[q->head];
+        q->head ^= 1;
+        q->nflight = 1;
         CU(cudaGetLastError());
     }
-    // retire the shots whose last step has run (as many as `done` holds)
+    if (q->nflight == 1) {
+        const cudaError_t r = cudaEventQuery(q->ev[q->head]);
+        if (r == cudaSuccess) {
+            q->gstep_done = q->ev_gstep[q->head];
+            q->head ^= 1;
+            q->nflight = 0;
+        } else if (r != cudaErrorNotReady) {
+            return dn_fail(DN_EDEVICE, "dn_queue_step: %s", cudaGetErrorString(r));
+        }
+        cudaGetLastError();   // a chunk still running is not an error
+    }
+    // retire the shots whose last step has run in a completed chunk (as many as `done` holds);
+    // their descriptors stay in the chunk in flight, where every kernel skips them (step > NT)
     for (size_t k = 0; k < q->active.size() && *ndone < cap;) {
         QSlot &x = q->active[k];
-        if (x.t0 + x.s->p.nt > q->gstep) {
+        if (x.t0 + x.s->p.nt > q->gstep_done) {
             k++;
             continue;
         }
@@ -1861,9 +1905,11 @@ extern "C" int dn_queue_step(dn_queue *q, dn_shot **done, int *status, int cap, 
         if (st) return st;
     }
     CU(cudaGraphLaunch(q->exec, q->stream));
-    CU(cudaEventRecord(q->ev, q->stream));
-    q->inflight = true;
+    const int slot = (q->head + q->nflight) & 1;
+    CU(cudaEventRecord(q->ev[slot], q->stream));
     q->gstep += q->chunk;
+    q->ev_gstep[slot] = q->gstep;
+    q->nflight++;
     return DN_OK;
 }
 
