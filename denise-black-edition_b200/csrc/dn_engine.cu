@@ -982,6 +982,9 @@ static void *acc_ptr(const dn_shot *s, int k)
     return b + 3 * a + (k - 3) * w;
 }
 
+// source cells per shot up to which the stencil kernels apply the forward sources themselves
+constexpr int SRC_IN_KERNEL = 8;
+
 // a forward run (mode 0 or 2) of a shot with the second field set takes the fused step
 static bool runs_fused(const dn_shot *s, int mode) { return s->fz && (mode == 0 || mode == 2); }
 
@@ -996,7 +999,9 @@ static int eff_tiles(const dn_shot *s, const LaunchCfg *c)
     return ((s->p.nx + s->bx - 1) / s->bx) * ((s->p.ny + z - 1) / z);
 }
 
-static Inst make_inst(const dn_shot *s, int mode, const LaunchCfg *c = nullptr)
+// the descriptor of shot s in mode `mode` for a batch configured as c (the configuration the
+// batch's kernels are launched with: tile rows, in-kernel sources)
+static Inst make_inst(const dn_shot *s, int mode, const LaunchCfg *c)
 {
     const dn_model *m = s->m;
     const dn_params &p = s->p;
@@ -1121,6 +1126,10 @@ static Inst make_inst(const dn_shot *s, int mode, const LaunchCfg *c = nullptr)
     I.Ws = (float *)acc_ptr(s, 3);
     I.Wr = (float *)acc_ptr(s, 4);
     I.flag = s->d_flag;
+    if (c && c->fuse_src && mode != 1 && !runs_fused(s, mode)) {
+        I.fsrc_v = 1;
+        I.fsrc_s = s->quelltyp_last == 1;
+    }
     if (runs_fused(s, mode)) {
         const int R = p.fdorder / 2;
         I.pp = 1;
@@ -1326,6 +1335,29 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c, con
             maxc = std::max(maxc, ((shots[k]->p.nx + VP_W - 1) / VP_W) * ((shots[k]->p.ny + c.vsh - 1) / c.vsh));
         c.vgrid = dim3(maxc, n);
     }
+    // forward sources inside the paired velocity kernel and the stress kernels, for batches
+    // whose shots have at most SRC_IN_KERNEL source cells each (every thread scans them per
+    // row); DN_SRC_IN_KERNEL=0 keeps them in k_inject_v / k_inject_s
+    {
+        const char *fs = getenv("DN_SRC_IN_KERNEL");
+        c.fuse_src = c.pack && !c.tma && !c.vpipe && !(fs && strcmp(fs, "0") == 0);
+        for (int k = 0; k < n; k++)
+            if (shots[k]->nsrc_cells > SRC_IN_KERNEL) c.fuse_src = false;
+        c.need_inject_v = false;
+        c.any_src_s = false;
+        for (int k = 0; k < n; k++) {
+            const dn_shot *s = shots[k];
+            const int m = modes ? modes[k] : mode;
+            if (runs_fused(s, m)) continue;   // the fused step injects its own sources
+            if (m == 1) {
+                c.need_inject_v = true;
+                if (s->p.quelltypb >= 4) c.any_src_s = true;
+            } else {
+                if (!c.fuse_src) c.need_inject_v = true;
+                if (s->quelltyp_last == 5 || (s->quelltyp_last == 1 && !c.fuse_src)) c.any_src_s = true;
+            }
+        }
+    }
     c.src_grid = dim3((maxsrc + 127) / 128, n);
     c.surf_grid = dim3((maxnx + 127) / 128, n);
     c.rec_grid = dim3((maxtr + 127) / 128, n);
@@ -1382,9 +1414,9 @@ static int graph_chunk(int maxnt)
 // states are bit-identical, so the gradient equals the one with every snapshot
 // stored.  Direct launches: the grids that need checkpoints are large.
 // ---------------------------------------------------------------------------
-static Inst make_inst_state2(const dn_shot *s, int mode)
+static Inst make_inst_state2(const dn_shot *s, int mode, const LaunchCfg *c)
 {
-    Inst I = make_inst(s, mode);
+    Inst I = make_inst(s, mode, c);
     const ptrdiff_t d = s->dstate2 - s->dstate;
     auto mv = [d](float *&p) {
         if (p) p = (float *)((char *)p + d);
@@ -1425,20 +1457,20 @@ static int run_ckpt(dn_shot *const *shots, int n, int mode, double &ms_total, lo
     std::vector<Inst> h;
     if (mode != 1) {
         for (int k = 0; k < n; k++) {
-            h.push_back(make_inst(shots[k], mode));
+            h.push_back(make_inst(shots[k], mode, &c));
             h.back().store = 0;
         }
     } else {
         // segment g: n recompute instances, then n adjoint instances
         for (int g = 0; g < nseg; g++) {
             for (int k = 0; k < n; k++) {
-                Inst f = make_inst(shots[k], 0);
+                Inst f = make_inst(shots[k], 0, &cf);
                 f.snap_base = g * per;
                 f.nsnap = shots[k]->nsnap;   // the segment buffer's slots (fewer than per when NT < ckpt_steps)
                 h.push_back(f);
             }
             for (int k = 0; k < n; k++) {
-                Inst a = make_inst_state2(shots[k], 1);
+                Inst a = make_inst_state2(shots[k], 1, &c);
                 a.snap_base = g * per;
                 a.nsnap = shots[k]->nsnap;
                 h.push_back(a);
@@ -1615,6 +1647,13 @@ static int run_direct(dn_shot *s, int mode, int nt0, int nt1, bool zero)
         h.pp = 0;
         c.any_fused = false;
         c.any_plain = true;
+        if (c.fuse_src && mode != 1) {   // its sources then come from the stencil kernels
+            h.fsrc_v = 1;
+            h.fsrc_s = s->quelltyp_last == 1;
+        } else {
+            c.need_inject_v = true;
+            if (s->quelltyp_last == 1) c.any_src_s = true;
+        }
     }
     Inst *d = nullptr;
     CU(dn_malloc(&d, sizeof(Inst)));

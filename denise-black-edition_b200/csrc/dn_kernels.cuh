@@ -92,6 +92,9 @@ struct Inst {
     // alternate between the buffers above and these; step nt writes the second set when
     // (nt_total - nt) is odd, so the last step leaves the state in the first
     int pp;                           // this instance runs the fused step
+    // forward sources applied inside the paired velocity kernel (force, QUELLTYP 2-4) and the
+    // stress kernels (explosive, QUELLTYP 1) instead of k_inject_v / k_inject_s
+    int fsrc_v, fsrc_s;
     int f_w, f_tiles_x, f_zc, f_tiles;   // its tiles: f_w columns x f_zc rows
     float *vx_b, *vy_b, *sxx_b, *syy_b, *sxy_b;
     float *psi_sxx_x_b, *psi_sxy_x_b, *psi_syy_y_b, *psi_sxy_y_b;
@@ -357,6 +360,69 @@ __device__ __forceinline__ void st2(float *p, float2 v, bool two)
     else *p = v.x;
 }
 
+// force sources of one cell (k_inject_v, forward modes), list order
+__device__ __forceinline__ void fz_force(const Inst &I, int s0, int ns, int nt, float &vx, float &vy)
+{
+    for (int k = 0; k < ns; k++) {
+        const int l = I.src_perm[s0 + k];
+        const int ty = I.src_type[l];
+        const float s = I.signals[(long long)l * I.nt + (nt - 1)];
+        if (ty == 2) vx = __fadd_rn(vx, s);
+        if (ty == 3) vy = __fadd_rn(vy, s);
+        if (ty == 4) {
+            vx = F(DADD((double)vx, DMUL(I.src_nsin[l], (double)s)));
+            vy = F(DADD((double)vy, DMUL(I.src_cos[l], (double)s)));
+        }
+    }
+}
+
+// explosive sources of one cell (k_inject_s, QUELLTYP 1), list order
+__device__ __forceinline__ void fz_explosive(const Inst &I, int s0, int ns, int nt, float &sxx, float &syy)
+{
+    const int NT = I.nt;
+    const float DT = I.DT;
+    for (int k = 0; k < ns; k++) {
+        const float *sg = I.signals + (long long)I.src_perm[s0 + k] * NT;
+        float amp = 0.0f;
+        if (nt == 1) amp = __fdiv_rn(sg[1], DT);
+        if (nt > 1 && nt < NT) amp = __fdiv_rn(__fsub_rn(sg[nt], sg[nt - 2]), DT);
+        if (nt == NT) amp = __fdiv_rn(-sg[nt - 2], DT);
+        sxx = __fadd_rn(sxx, amp);
+        syy = __fadd_rn(syy, amp);
+    }
+}
+
+// whether a source cell lies in columns (i0, i0 + two) of rows j0..j1
+__device__ __forceinline__ bool src_in_columns(const Inst &I, int i0, bool two, int j0, int j1)
+{
+    for (int c = 0; c < I.nsrc_cells; c++) {
+        const int ci = I.src_cell_i[c], cj = I.src_cell_j[c];
+        if (cj >= j0 && cj <= j1 && (ci == i0 || (two && ci == i0 + 1))) return true;
+    }
+    return false;
+}
+
+// forward sources of the source cells at row j in columns (i0, i0 + two) (fsrc_v / fsrc_s)
+__device__ __forceinline__ void src_force_pair(const Inst &I, int i0, bool two, int j, int nt, float2 &vx, float2 &vy)
+{
+    for (int c = 0; c < I.nsrc_cells; c++) {
+        const int cj = I.src_cell_j[c], ci = I.src_cell_i[c];
+        if (cj != j || (ci != i0 && !(two && ci == i0 + 1))) continue;
+        if (ci == i0) fz_force(I, I.src_cell_start[c], I.src_cell_count[c], nt, vx.x, vy.x);
+        else fz_force(I, I.src_cell_start[c], I.src_cell_count[c], nt, vx.y, vy.y);
+    }
+}
+__device__ __forceinline__ void src_explosive_pair(const Inst &I, int i0, bool two, int j, int nt, float2 &sxx,
+                                                   float2 &syy)
+{
+    for (int c = 0; c < I.nsrc_cells; c++) {
+        const int cj = I.src_cell_j[c], ci = I.src_cell_i[c];
+        if (cj != j || (ci != i0 && !(two && ci == i0 + 1))) continue;
+        if (ci == i0) fz_explosive(I, I.src_cell_start[c], I.src_cell_count[c], nt, sxx.x, syy.x);
+        else fz_explosive(I, I.src_cell_start[c], I.src_cell_count[c], nt, sxx.y, syy.y);
+    }
+}
+
 // division by DH of both lanes, as DIVH per lane
 template <bool X>
 __device__ __forceinline__ float2 DIVH2(float2 a, bool fd, float DH, float rdh)
@@ -397,6 +463,7 @@ __global__ void __launch_bounds__(128, DN_V2_MINB) k_update_v2(const Inst *__res
     const bool snapstep = (mode == 0) && I.store && ((nt - 1) % I.dtinv == 0);
     const int fw = I.fw, nx = I.nx, ny = I.ny, free_surf = I.free_surf;
     const bool xframe = fw > 0 && (i0 <= fw || i0 + 1 >= nx - fw + 1);
+    const bool srcs = I.fsrc_v && src_in_columns(I, i0, two, j0, j1);   // a source cell in this thread's rows
     for (int j = j0; j <= j1; j++) {
         const long long o = (long long)j * P + i0;
         // the lines row j + 1 reads first (its new z-stencil rows and its own-row operands) are
@@ -496,8 +563,9 @@ __global__ void __launch_bounds__(128, DN_V2_MINB) k_update_v2(const Inst *__res
         const float2 vxo = ldw2(I.vx + o), vyo = ldw2(I.vy + o);
         const float2 s1 = ADD2<X>(sxx_x, sxy_y);
         const float2 s2 = ADD2<X>(sxy_x, syy_y);
-        const float2 nvx = ADD2<X>(vxo, DIVH2<X>(MUL2<X>(MUL2<X>(bc2(DT), ripv), s1), fd, DH, rdh));
-        const float2 nvy = ADD2<X>(vyo, DIVH2<X>(MUL2<X>(MUL2<X>(bc2(DT), rjpv), s2), fd, DH, rdh));
+        float2 nvx = ADD2<X>(vxo, DIVH2<X>(MUL2<X>(MUL2<X>(bc2(DT), ripv), s1), fd, DH, rdh));
+        float2 nvy = ADD2<X>(vyo, DIVH2<X>(MUL2<X>(MUL2<X>(bc2(DT), rjpv), s2), fd, DH, rdh));
+        if (srcs) src_force_pair(I, i0, two, j, nt, nvx, nvy);
         float2 p1x, p1y;
         const bool wp = snapstep || mode == 1;
         if (snapstep) {
@@ -551,6 +619,7 @@ static __global__ void k_inject_v(const Inst *__restrict__ insts, const int *__r
         }
         return;
     }
+    if (I.fsrc_v) return;   // applied by the velocity kernel
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < I.nsrc_cells; c += gridDim.x * blockDim.x) {
         const long long o = (long long)I.src_cell_j[c] * P + I.src_cell_i[c];
         float vx = I.vx[o], vy = I.vy[o];
@@ -848,6 +917,7 @@ __global__ void __launch_bounds__(128, DN_S2_MINB) k_update_s_el2(const Inst *__
 #pragma unroll
     for (int m = 1; m <= R; m++) hc[m] = I.hc[m];
     const float dhi = I.dhi_el;
+    const bool srcs = I.fsrc_s && src_in_columns(I, i0, two, j0, j1);
     for (int j = j0; j <= j1; j++) {
         const long long o = (long long)j * P + i0;
         {
@@ -876,6 +946,7 @@ __global__ void __launch_bounds__(128, DN_S2_MINB) k_update_s_el2(const Inst *__
             nsyy.x = F(DADD((double)s_yy.x, DADD((double)gdiv.x, DMUL(f2x, (double)vyy.x))));
             nsyy.y = F(DADD((double)s_yy.y, DADD((double)gdiv.y, DMUL(f2y, (double)vyy.y))));
         }
+        if (srcs) src_explosive_pair(I, i0, two, j, nt, nsxx, nsyy);
         st2(I.sxy + o, nsxy, two);
         st2(I.sxx + o, nsxx, two);
         st2(I.syy + o, nsyy, two);
@@ -943,6 +1014,7 @@ __global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__
             nq[l] = qp[o + l * PL];
         }
     };
+    const bool srcs = I.fsrc_s && src_in_columns(I, i, false, t.j0, t.j1);
     fetch(t.j0);
     for (int j = t.j0; j <= t.j1; j++) {
         D.advance(j);
@@ -997,8 +1069,13 @@ __global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__
             sumq = ADD<X>(sumq, qv);
         }
         sxyp[o] = ADD<X>(sxy, MUL<X>(dthalbe, sumr));
-        sxxp[o] = ADD<X>(sxx, MUL<X>(dthalbe, sump));
-        syyp[o] = ADD<X>(syy, MUL<X>(dthalbe, sumq));
+        float fsxx = ADD<X>(sxx, MUL<X>(dthalbe, sump)), fsyy = ADD<X>(syy, MUL<X>(dthalbe, sumq));
+        if (srcs)
+            for (int c = 0; c < I.nsrc_cells; c++)
+                if (I.src_cell_j[c] == j && I.src_cell_i[c] == i)
+                    fz_explosive(I, I.src_cell_start[c], I.src_cell_count[c], nt, fsxx, fsyy);
+        sxxp[o] = fsxx;
+        syyp[o] = fsyy;
         D.shift();
     }
 }
@@ -1027,7 +1104,7 @@ static __global__ void k_inject_s(const Inst *__restrict__ insts, const int *__r
     }
     const int NT = I.nt;
     const float DT = I.DT;
-    if (I.quelltyp_last == 1) {
+    if (I.quelltyp_last == 1 && !I.fsrc_s) {   // fsrc_s: applied by the stress kernel
         for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < I.nsrc_cells; c += gridDim.x * blockDim.x) {
             const long long o = (long long)I.src_cell_j[c] * P + I.src_cell_i[c];
             float sxx = I.sxx[o], syy = I.syy[o];

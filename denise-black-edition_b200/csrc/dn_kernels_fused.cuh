@@ -187,38 +187,6 @@ __device__ __forceinline__ void fz_velocity(const Inst &I, const FzBufs &B, cons
     nvy = ADD2<X>(vyo, DIVH2<X>(MUL2<X>(MUL2<X>(bc2(DT), rjpv), s2), fd, DH, rdh));
 }
 
-// force sources of one cell (k_inject_v, forward modes), list order
-__device__ __forceinline__ void fz_force(const Inst &I, int s0, int ns, int nt, float &vx, float &vy)
-{
-    for (int k = 0; k < ns; k++) {
-        const int l = I.src_perm[s0 + k];
-        const int ty = I.src_type[l];
-        const float s = I.signals[(long long)l * I.nt + (nt - 1)];
-        if (ty == 2) vx = __fadd_rn(vx, s);
-        if (ty == 3) vy = __fadd_rn(vy, s);
-        if (ty == 4) {
-            vx = F(DADD((double)vx, DMUL(I.src_nsin[l], (double)s)));
-            vy = F(DADD((double)vy, DMUL(I.src_cos[l], (double)s)));
-        }
-    }
-}
-
-// explosive sources of one cell (k_inject_s, QUELLTYP 1), list order
-__device__ __forceinline__ void fz_explosive(const Inst &I, int s0, int ns, int nt, float &sxx, float &syy)
-{
-    const int NT = I.nt;
-    const float DT = I.DT;
-    for (int k = 0; k < ns; k++) {
-        const float *sg = I.signals + (long long)I.src_perm[s0 + k] * NT;
-        float amp = 0.0f;
-        if (nt == 1) amp = __fdiv_rn(sg[1], DT);
-        if (nt > 1 && nt < NT) amp = __fdiv_rn(__fsub_rn(sg[nt], sg[nt - 2]), DT);
-        if (nt == NT) amp = __fdiv_rn(-sg[nt - 2], DT);
-        sxx = __fadd_rn(sxx, amp);
-        syy = __fadd_rn(syy, amp);
-    }
-}
-
 template <int R, bool X>
 __global__ void __launch_bounds__(FZ_NP, DN_FZ_MINB) k_step_el_fused(const Inst *__restrict__ insts, const int *__restrict__ ntb,
                                                              int off)

@@ -22,6 +22,8 @@ struct LaunchCfg {
     dim3 vgrid; // its grid: strips of VP_W columns x vsh rows per instance
     int vsh;
     bool any_surf, any_src_s, any_store, any_adj, any_rec;
+    bool fuse_src;       // forward sources applied inside the velocity / stress kernels (Inst::fsrc_*)
+    bool need_inject_v;  // k_inject_v still has work (adjoint forces, or sources not in the kernels)
     bool any_fused;   // some instance runs the fused elastic step (Inst::pp)
     bool any_plain;   // some instance runs the separate velocity / stress kernels
     dim3 fgrid;       // grid of the fused step: its tiles per instance

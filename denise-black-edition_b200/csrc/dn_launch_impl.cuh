@@ -23,9 +23,10 @@ void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int
         else k_update_v<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
     }
     MARK(1);
-    if (c.any_plain) {
+    if (c.any_plain) nl++;
+    if (c.any_plain && c.need_inject_v) {
         k_inject_v<<<c.src_grid, 128, 0, st>>>(d, ntb, off);
-        nl += 2;
+        nl++;
     }
     MARK(2);
     if (!c.any_plain) {

@@ -18,8 +18,8 @@ from test_gpu_parity import gpu_shot, small_case
 pytestmark = pytest.mark.gpu
 
 
-def _case(fdorder=8, nx=300, ny=70, nt=200, styp=1, src_ij=None, free_surf=1, seed=3, **kw):
-    p, model, src, rec = small_case(L=0, fdorder=fdorder, nx=nx, ny=ny, nt=nt, styp=styp, free_surf=free_surf,
+def _case(fdorder=8, nx=300, ny=70, nt=200, styp=1, src_ij=None, free_surf=1, seed=3, L=0, **kw):
+    p, model, src, rec = small_case(L=L, fdorder=fdorder, nx=nx, ny=ny, nt=nt, styp=styp, free_surf=free_surf,
                                     seed=seed, **kw)
     if src_ij is not None:
         i, j = zip(*src_ij)
