@@ -1335,12 +1335,16 @@ static int check_batch(dn_shot *const *shots, int n, int mode, LaunchCfg &c, con
             maxc = std::max(maxc, ((shots[k]->p.nx + VP_W - 1) / VP_W) * ((shots[k]->p.ny + c.vsh - 1) / c.vsh));
         c.vgrid = dim3(maxc, n);
     }
-    // forward sources inside the paired velocity kernel and the stress kernels, for batches
-    // whose shots have at most SRC_IN_KERNEL source cells each (every thread scans them per
-    // row); DN_SRC_IN_KERNEL=0 keeps them in k_inject_v / k_inject_s
+    // forward sources inside the paired velocity kernel and the stress kernels (their SRC
+    // variants), for batches whose step is bound by launches (below 5 M cells: a 600 x 300
+    // shot steps in 20.4 instead of 24.0 us; the 64-shot batches were 3 % slower with the
+    // sources in the kernels) and whose shots have at most SRC_IN_KERNEL source cells each;
+    // DN_SRC_IN_KERNEL=0 / 1 turns them off / on for every batch
     {
         const char *fs = getenv("DN_SRC_IN_KERNEL");
-        c.fuse_src = c.pack && !c.tma && !c.vpipe && !(fs && strcmp(fs, "0") == 0);
+        long long cells = 0;
+        for (int k = 0; k < n; k++) cells += (long long)shots[k]->p.nx * shots[k]->p.ny;
+        c.fuse_src = c.pack && !c.tma && !c.vpipe && (fs ? strcmp(fs, "0") != 0 : cells < 5000000);
         for (int k = 0; k < n; k++)
             if (shots[k]->nsrc_cells > SRC_IN_KERNEL) c.fuse_src = false;
         c.need_inject_v = false;

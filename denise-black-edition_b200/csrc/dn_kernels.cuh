@@ -438,7 +438,8 @@ __device__ __forceinline__ float2 DIVH2(float2 a, bool fd, float DH, float rdh)
     return q1;
 }
 
-template <int R, bool X>
+// SRC: the variant that applies the forward sources of its cells (Inst::fsrc_v)
+template <int R, bool X, bool SRC = false>
 __global__ void __launch_bounds__(128, DN_V2_MINB) k_update_v2(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
@@ -463,7 +464,7 @@ __global__ void __launch_bounds__(128, DN_V2_MINB) k_update_v2(const Inst *__res
     const bool snapstep = (mode == 0) && I.store && ((nt - 1) % I.dtinv == 0);
     const int fw = I.fw, nx = I.nx, ny = I.ny, free_surf = I.free_surf;
     const bool xframe = fw > 0 && (i0 <= fw || i0 + 1 >= nx - fw + 1);
-    const bool srcs = I.fsrc_v && src_in_columns(I, i0, two, j0, j1);   // a source cell in this thread's rows
+    const bool srcs = SRC && I.fsrc_v && src_in_columns(I, i0, two, j0, j1);   // a source cell in this thread's rows
     for (int j = j0; j <= j1; j++) {
         const long long o = (long long)j * P + i0;
         // the lines row j + 1 reads first (its new z-stencil rows and its own-row operands) are
@@ -897,7 +898,7 @@ __device__ __forceinline__ void vderiv2(const Inst &I, const float *hc, int i0, 
 
 
 // Paired-column elastic stress update (k_update_s_el for two columns per thread).
-template <int R, bool X>
+template <int R, bool X, bool SRC = false>
 __global__ void __launch_bounds__(128, DN_S2_MINB) k_update_s_el2(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
@@ -917,7 +918,7 @@ __global__ void __launch_bounds__(128, DN_S2_MINB) k_update_s_el2(const Inst *__
 #pragma unroll
     for (int m = 1; m <= R; m++) hc[m] = I.hc[m];
     const float dhi = I.dhi_el;
-    const bool srcs = I.fsrc_s && src_in_columns(I, i0, two, j0, j1);
+    const bool srcs = SRC && I.fsrc_s && src_in_columns(I, i0, two, j0, j1);
     for (int j = j0; j <= j1; j++) {
         const long long o = (long long)j * P + i0;
         {
@@ -958,7 +959,7 @@ __global__ void __launch_bounds__(128, DN_S2_MINB) k_update_s_el2(const Inst *__
 // fipjp, f, g, dip, d, e are regenerated per cell from the six relaxed-modulus
 // factors exactly as prepare_update_s_visc_PSV.c:52-62 forms them.
 // ===========================================================================
-template <int R, int L, bool X>
+template <int R, int L, bool X, bool SRC = false>
 __global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
@@ -1014,7 +1015,7 @@ __global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__
             nq[l] = qp[o + l * PL];
         }
     };
-    const bool srcs = I.fsrc_s && src_in_columns(I, i, false, t.j0, t.j1);
+    const bool srcs = SRC && I.fsrc_s && src_in_columns(I, i, false, t.j0, t.j1);
     fetch(t.j0);
     for (int j = t.j0; j <= t.j1; j++) {
         D.advance(j);

@@ -19,6 +19,7 @@ void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int
         if (c.vpipe) k_update_v_pipe<R, X><<<c.vgrid, VP_THREADS, vpipe_smem_bytes(), st>>>(d, ntb, off, c.vsh);
         else if (c.tma)
             k_update_v_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QV>(slot_floats_v()), st>>>(d, ntb, off);
+        else if (c.pack && c.fuse_src) k_update_v2<R, X, true><<<c.tile_grid, c.bx / 2, 0, st>>>(d, ntb, off);
         else if (c.pack) k_update_v2<R, X><<<c.tile_grid, c.bx / 2, 0, st>>>(d, ntb, off);
         else k_update_v<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
     }
@@ -34,6 +35,7 @@ void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int
     } else if (c.L == 0) {
         if (c.tma)
             k_update_s_el_tma<R, X><<<c.tile_grid, TMA_W, pipe_smem_bytes<QS_EL>(slot_floats_s_el()), st>>>(d, ntb, off);
+        else if (c.pack && c.fuse_src) k_update_s_el2<R, X, true><<<c.tile_grid, c.bx / 2, 0, st>>>(d, ntb, off);
         else if (c.pack) k_update_s_el2<R, X><<<c.tile_grid, c.bx / 2, 0, st>>>(d, ntb, off);
         else k_update_s_el<R, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off);
     } else if (c.tma) {
@@ -48,13 +50,17 @@ void launch_step_R(const LaunchCfg &c, cudaStream_t st, const Inst *d, const int
         }
 #undef DN_VI_TMA
     } else {
+#define DN_VI(LL)                                                                                              \
+    (c.fuse_src ? k_update_s_vi<R, LL, X, true><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off)                        \
+                : k_update_s_vi<R, LL, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off))
         switch (c.L) {
-        case 1: k_update_s_vi<R, 1, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
-        case 2: k_update_s_vi<R, 2, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
-        case 3: k_update_s_vi<R, 3, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
-        case 4: k_update_s_vi<R, 4, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
-        default: k_update_s_vi<R, 5, X><<<c.tile_grid, c.bx, 0, st>>>(d, ntb, off); break;
+        case 1: DN_VI(1); break;
+        case 2: DN_VI(2); break;
+        case 3: DN_VI(3); break;
+        case 4: DN_VI(4); break;
+        default: DN_VI(5); break;
         }
+#undef DN_VI
     }
     if (c.any_plain) nl++;
     MARK(3);
