@@ -84,9 +84,6 @@ __device__ __forceinline__ FzBufs fz_bufs(const Inst &I, int nt)
     return b;
 }
 
-// the state buffers holding step nt's result (for the kernels that read it after the step)
-__device__ __forceinline__ bool fz_after_alt(const Inst &I, int nt) { return I.pp && ((I.nt - nt) & 1) != 0; }
-
 // New velocities of the pair (i0, i0 + 1) at row j from the old buffers, as
 // k_update_v2 computes them (mode 0 / 2 without snapshots); `own` cells also
 // write their CPML memory.
