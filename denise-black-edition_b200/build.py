@@ -83,6 +83,13 @@ def build(verbose=True):
         if _newer(exe, [s, lib] + headers):
             _run(["gcc"] + HOST_CFLAGS + ["-I", INC, "-I", CSRC, "-I", HOST, s, "-o", exe,
                                           "-L", LIB, "-ldenise_b200", "-Wl,-rpath,$ORIGIN/../lib", "-lm"])
+    # the per-kernel drop-ins with the reference's signatures: their own library, whose
+    # undefined symbols (the reference's globals and err) resolve in the reference program
+    shim_src = os.path.join(CSRC, "dn_fd_shims.cu")
+    shim = os.path.join(LIB, "libdenise_b200_fd.so")
+    if os.path.exists(shim_src) and _newer(shim, [shim_src] + headers):
+        _run([NVCC] + ARCH + EXTRA_NVCC + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
+                                           "-shared", "-I", INC, "-I", CSRC, shim_src, "-o", shim, "-lcudart"])
     return lib
 
 

@@ -170,6 +170,7 @@ struct dn_shot {
     int nsnap = 0, zch = 16, bx = 128, tiles_x = 0, tiles = 0;
     int kern = DN_KERN_PAIRED;     // stencil kernel variant (the batch runs its first shot's)
     bool auto_rows = false;        // tile rows chosen per batch (batch_rows)
+    bool rec_dup = false;          // two receivers share a cell
     // fused elastic step (DN_KERN_FUSED on an eligible shot): the second set of fields and
     // velocity CPML memory (inside dstate, so zeroed with it) and the tile rows
     bool fz = false;
@@ -797,6 +798,12 @@ extern "C" int dn_shot_create(dn_model *m, const dn_acq *acq, dn_shot **out)
     s->signals.assign(acq->signals, acq->signals + (size_t)acq->nsrc * p->nt);
     s->rec_i.assign(acq->rec_i, acq->rec_i + acq->ntr);
     s->rec_j.assign(acq->rec_j, acq->rec_j + acq->ntr);
+    {
+        std::vector<long long> cells(acq->ntr);
+        for (int l = 0; l < acq->ntr; l++) cells[l] = (long long)acq->rec_j[l] * (p->nx + 2) + acq->rec_i[l];
+        std::sort(cells.begin(), cells.end());
+        s->rec_dup = std::adjacent_find(cells.begin(), cells.end()) != cells.end();
+    }
     s->quelltyp_last = acq->nsrc > 0 ? s->src_type[acq->nsrc - 1] : 0;
     bool deflt = false;
     tile_choice(p, s->bx, s->zch, s->kern, &deflt);
@@ -1115,6 +1122,7 @@ static Inst make_inst(const dn_shot *s, int mode, const LaunchCfg *c)
     I.res_vy = s->d_res + rs;
     I.res_p = s->d_res + 2 * rs;
     I.ntr = s->ntr;
+    I.rec_dup = s->rec_dup;
     I.rec_i = s->d_rec_i;
     I.rec_j = s->d_rec_j;
     I.sec = s->d_sec;

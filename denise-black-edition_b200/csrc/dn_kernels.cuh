@@ -95,6 +95,7 @@ struct Inst {
     // forward sources applied inside the paired velocity kernel (force, QUELLTYP 2-4) and the
     // stress kernels (explosive, QUELLTYP 1) instead of k_inject_v / k_inject_s
     int fsrc_v, fsrc_s;
+    int rec_dup;                      // two receivers share a cell: adjoint sources added in list order
     int f_w, f_tiles_x, f_zc, f_tiles;   // its tiles: f_w columns x f_zc rows
     float *vx_b, *vy_b, *sxx_b, *syy_b, *sxy_b;
     float *psi_sxx_x_b, *psi_sxy_x_b, *psi_syy_y_b, *psi_sxy_y_b;
@@ -608,7 +609,11 @@ static __global__ void k_inject_v(const Inst *__restrict__ insts, const int *__r
     const long long P = I.pitch;
     if (I.mode == 1) {
         const int q = I.quelltypb;
-        for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < I.ntr; l += gridDim.x * blockDim.x) {
+        // receivers that share a cell add their forces one after the other in list order, as
+        // the reference's loop does (update_v_PML_PSV.c:755-768): one thread for them all
+        const int l0 = I.rec_dup ? (blockIdx.x == 0 && threadIdx.x == 0 ? 0 : I.ntr) : blockIdx.x * blockDim.x + threadIdx.x;
+        const int dl = I.rec_dup ? 1 : gridDim.x * blockDim.x;
+        for (int l = l0; l < I.ntr; l += dl) {
             const long long o = (long long)I.rec_j[l] * P + I.rec_i[l];
             const long long s = (long long)l * I.nt + (nt - 1);
             if (q == 1) {
@@ -1095,7 +1100,10 @@ static __global__ void k_inject_s(const Inst *__restrict__ insts, const int *__r
     const long long P = I.pitch;
     if (I.mode == 1) {
         if (I.quelltypb < 4) return;
-        for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < I.ntr; l += gridDim.x * blockDim.x) {
+        // receivers sharing a cell: one thread, list order (psource.c:41-53)
+        const int l0 = I.rec_dup ? (blockIdx.x == 0 && threadIdx.x == 0 ? 0 : I.ntr) : blockIdx.x * blockDim.x + threadIdx.x;
+        const int dl = I.rec_dup ? 1 : gridDim.x * blockDim.x;
+        for (int l = l0; l < I.ntr; l += dl) {
             const long long o = (long long)I.rec_j[l] * P + I.rec_i[l];
             const float s = I.res_p[(long long)l * I.nt + (nt - 1)];
             I.sxx[o] = __fadd_rn(I.sxx[o], s);

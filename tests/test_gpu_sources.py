@@ -38,3 +38,29 @@ def test_many_source_cells_and_switch(monkeypatch, env):
     dn.run([s for _, s in pairs], dn.MODE_FORWARD)
     for c, (m, s) in zip(cases, pairs):
         _check(*c, s)
+
+
+@pytest.mark.parametrize("quelltypb", [1, 4])
+def test_adjoint_sources_of_receivers_sharing_a_cell(quelltypb):
+    """Two receivers in one cell: their adjoint forces (QUELLTYPB 1) or pressures
+    (QUELLTYPB 4) add one after the other in list order, as the reference's
+    loop does, so the gradient is bit-identical to the restatement's."""
+    from test_gpu_parity import _residuals, small_case
+
+    p, model, src, rec = small_case(nt=200, store_snapshots=1, nx=80)
+    p = p.replace(quelltypb=quelltypb)
+    ri = np.concatenate([rec[0], rec[0][:3]]).astype(np.int32)   # the first three receivers twice
+    rj = np.concatenate([rec[1], rec[1][:3]]).astype(np.int32)
+    rec = (ri, rj)
+    ref = O.Restatement(p, model, src, rec, "f")
+    ref.forward(store=True)
+    m, s = gpu_shot(p, model, src, rec)
+    dn.run([s], dn.MODE_FORWARD)
+    rvx, rvy = _residuals(p, s.sections(0), s.sections(1))
+    rp = (0.5 * rvx).astype(np.float32) if quelltypb >= 4 else None
+    s.set_residuals(rvx, rvy, rp)
+    ref.adjoint(rvx, rvy, rp)
+    dn.run([s], dn.MODE_ADJOINT)
+    s.accumulate_gradient()
+    for a, b in zip(m.gradient(), ref.gradient()):
+        np.testing.assert_array_equal(a, b)
