@@ -48,3 +48,18 @@ def test_model_validation_without_gpu(bad, code):
     with pytest.raises(dn.DeniseError) as e:
         dn.Model(p, z * 2000, z * 1000, z * 2000, z * 50, z * 50)
     assert e.value.code == code
+
+
+def test_kernel_shim_library_loads_beside_the_reference():
+    """lib/libdenise_b200_fd.so defines update_v_PML_PSV and update_s_elastic_PML_PSV
+    and nothing else of the reference's; its references to the reference's globals
+    and err() resolve in a process that holds the reference (here, its build)."""
+    import oracles as O
+
+    shim = os.path.join(os.path.dirname(_lib.LIB_PATH), "libdenise_b200_fd.so")
+    assert os.path.exists(shim)
+    if not O.reference_available():
+        pytest.skip("the reference build (oracle/_ref) is not there")
+    ctypes.CDLL(O.REF_SO, mode=ctypes.RTLD_GLOBAL)
+    lib = ctypes.CDLL(shim)
+    assert hasattr(lib, "update_v_PML_PSV") and hasattr(lib, "update_s_elastic_PML_PSV")
