@@ -51,9 +51,9 @@ def test_model_validation_without_gpu(bad, code):
 
 
 def test_kernel_shim_library_loads_beside_the_reference():
-    """lib/libdenise_b200_fd.so defines update_v_PML_PSV and update_s_elastic_PML_PSV
-    and nothing else of the reference's; its references to the reference's globals
-    and err() resolve in a process that holds the reference (here, its build)."""
+    """lib/libdenise_b200_fd.so defines update_v_PML_PSV and update_s_elastic_PML_PSV;
+    its references to the reference's globals and err() resolve in a process that
+    holds the reference (here, its build)."""
     import oracles as O
 
     shim = os.path.join(os.path.dirname(_lib.LIB_PATH), "libdenise_b200_fd.so")
