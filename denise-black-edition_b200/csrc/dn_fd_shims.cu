@@ -1,8 +1,8 @@
 // Per-kernel drop-ins with the exact signatures of the reference's
-// update_v_PML_PSV (include/fd.h:324) and update_s_elastic_PML_PSV
-// (include/fd.h:309), built as their own library (libdenise_b200_fd.so).  A
-// reference build links it in place of src/PSV/update_v_PML_PSV.c and
-// src/PSV/update_s_elastic_PML_PSV.c to swap one kernel at a time and compare;
+// update_v_PML_PSV (include/fd.h:324), update_s_elastic_PML_PSV (:309) and
+// update_s_visc_PML_PSV (:316), built as their own library
+// (libdenise_b200_fd.so).  A reference build links it in place of those files
+// of src/PSV/ to swap one kernel at a time and compare;
 // the library reads the reference's globals (NX, NY, FDORDER, FW, DT, DH,
 // FREE_SURF, BOUNDARY, NPROCX, NPROCY, POS, GRAD_FORM, INVMAT1, QUELLTYPB, NT)
 // and reports failures through the reference's err(), as its own functions do.
@@ -11,7 +11,8 @@
 // halos of nd = FDORDER/2 + 1 cells that alloc_PSV gives the fields) into the
 // engine's padded device planes, runs the engine's kernel for that one step
 // (k_update_v2 with its force sources or k_inject_v's adjoint forces;
-// k_update_s_el2) and copies back what the reference function writes: the
+// k_update_s_el2; k_update_s_vi reading the prepared fipjp, f, g, d, e, dip
+// it is handed) and copies back what the reference function writes: the
 // interior of the updated fields, vxp1 / vyp1 and the CPML memory.  The kernels
 // are the ones dn_run uses, so the results are bit-identical to the
 // reference's; the copies make a call cost milliseconds, so this boundary is a
@@ -34,7 +35,7 @@
 
 extern "C" {
 // the reference's globals (include/globvar.h) and error exit (src/util.c:7)
-extern int NX, NY, NT, FDORDER, FW, FREE_SURF, BOUNDARY, NPROCX, NPROCY, GRAD_FORM, INVMAT1, QUELLTYP, QUELLTYPB;
+extern int NX, NY, NT, FDORDER, FW, FREE_SURF, BOUNDARY, NPROCX, NPROCY, GRAD_FORM, INVMAT1, QUELLTYP, QUELLTYPB, L;
 extern int POS[3];
 extern float DT, DH;
 void err(char err_text[]);
@@ -57,6 +58,8 @@ struct ShimState {
     int *d_zero = nullptr;            // step base 0 (the kernels' step is *ntb + off)
     Inst *d_inst = nullptr;
     std::vector<float> stage;         // one plane on the host
+    float *visc = nullptr;            // viscoelastic planes: r, p, q, d, e, dip (L each), fipjp, f, g
+    int visc_L = 0;
 };
 ShimState g;
 
@@ -96,6 +99,9 @@ void ensure_state()
     int dev = 0;
     cu(cudaGetDevice(&dev), "cudaGetDevice");
     if (g.planes && g.nx == NX && g.ny == NY && g.fw == fw && g.device == dev) return;
+    if (g.visc) cudaFree(g.visc);
+    g.visc = nullptr;
+    g.visc_L = 0;
     if (g.planes) {
         cudaFree(g.planes);
         cudaFree(g.psi);
@@ -450,6 +456,148 @@ extern "C" void update_s_elastic_PML_PSV(int nx1, int nx2, int ny1, int ny2, flo
     interior_out(P_SXX, sxx);
     interior_out(P_SYY, syy);
     interior_out(P_SXY, sxy);
+    psi_out(0, psi_vxx);
+    psi_out(1, psi_vyx);
+    psi_out(2, psi_vyy);
+    psi_out(3, psi_vxy);
+}
+
+namespace {
+
+// plane k of the viscoelastic buffer (origin pointer)
+float *vplane(int k) { return g.visc + (long long)k * g.plane + g.origin; }
+
+// an f3tensor t[j][i][1..L] (interior) into the L planes from vplane(k0), or back
+void tensor_in(int k0, float ***t)
+{
+    for (int l = 1; l <= L; l++) {
+        std::fill(g.stage.begin(), g.stage.end(), 0.0f);
+        float *s = g.stage.data() + g.origin;
+        for (int j = 1; j <= NY; j++)
+            for (int i = 1; i <= NX; i++) s[(long long)j * g.pitch + i] = t[j][i][l];
+        cu(cudaMemcpy(g.visc + (long long)(k0 + l - 1) * g.plane, g.stage.data(), g.plane * 4, cudaMemcpyHostToDevice),
+           "copy of a viscoelastic tensor");
+    }
+}
+void tensor_out(int k0, float ***t)
+{
+    for (int l = 1; l <= L; l++) {
+        cu(cudaMemcpy(g.stage.data(), g.visc + (long long)(k0 + l - 1) * g.plane, g.plane * 4, cudaMemcpyDeviceToHost),
+           "copy back of a viscoelastic tensor");
+        const float *s = g.stage.data() + g.origin;
+        for (int j = 1; j <= NY; j++)
+            for (int i = 1; i <= NX; i++) t[j][i][l] = s[(long long)j * g.pitch + i];
+    }
+}
+void vinterior_in(int k, float **m)
+{
+    std::fill(g.stage.begin(), g.stage.end(), 0.0f);
+    float *s = g.stage.data() + g.origin;
+    for (int j = 1; j <= NY; j++) memcpy(s + (long long)j * g.pitch + 1, &m[j][1], (size_t)NX * 4);
+    cu(cudaMemcpy(g.visc + (long long)k * g.plane, g.stage.data(), g.plane * 4, cudaMemcpyHostToDevice),
+       "copy of a prepared coefficient");
+}
+
+template <int LL>
+void launch_vi(const Inst *d, dim3 grid)
+{
+    switch (FDORDER / 2) {
+    case 1: dn::k_update_s_vi<1, LL, true, false, true><<<grid, 128>>>(d, g.d_zero, 1); break;
+    case 2: dn::k_update_s_vi<2, LL, true, false, true><<<grid, 128>>>(d, g.d_zero, 1); break;
+    case 3: dn::k_update_s_vi<3, LL, true, false, true><<<grid, 128>>>(d, g.d_zero, 1); break;
+    case 4: dn::k_update_s_vi<4, LL, true, false, true><<<grid, 128>>>(d, g.d_zero, 1); break;
+    case 5: dn::k_update_s_vi<5, LL, true, false, true><<<grid, 128>>>(d, g.d_zero, 1); break;
+    default: dn::k_update_s_vi<6, LL, true, false, true><<<grid, 128>>>(d, g.d_zero, 1); break;
+    }
+}
+
+}   // namespace
+
+extern "C" void update_s_visc_PML_PSV(int nx1, int nx2, int ny1, int ny2, float **vx, float **vy, float **ux,
+                                      float **uy, float **uxy, float **uyx, float **sxx, float **syy, float **sxy,
+                                      float **pi, float **u, float **uipjp, float **rho, float *hc, int infoout,
+                                      float ***r, float ***p, float ***q, float **fipjp, float **f, float **gg,
+                                      float *bip, float *bjm, float *cip, float *cjm, float ***d, float ***e,
+                                      float ***dip, float *K_x, float *a_x, float *b_x, float *K_x_half,
+                                      float *a_x_half, float *b_x_half, float *K_y, float *a_y, float *b_y,
+                                      float *K_y_half, float *a_y_half, float *b_y_half, float **psi_vxx,
+                                      float **psi_vyy, float **psi_vxy, float **psi_vyx, int mode)
+{
+    (void)ux, (void)uy, (void)uxy, (void)uyx, (void)pi, (void)u, (void)uipjp, (void)rho, (void)infoout, (void)mode;
+    check_domain(nx1, nx2, ny1, ny2);
+    if (L < 1 || L > DN_MAX_L) fail("update_s_visc_PML_PSV: L must be 1..5");
+    // the engine applies one pair (bip, cip) to r, p and q; prepare_update_s_visc_PSV gives bjm = bip, cjm = cip
+    for (int l = 1; l <= L; l++)
+        if (memcmp(&bip[l], &bjm[l], 4) || memcmp(&cip[l], &cjm[l], 4))
+            fail("update_s_visc_PML_PSV: bjm / cjm differ from bip / cip");
+    ensure_state();
+    if (!g.visc || g.visc_L != L) {
+        if (g.visc) cudaFree(g.visc);
+        cu(cudaMalloc(&g.visc, (size_t)(6 * L + 3) * g.plane * 4), "cudaMalloc viscoelastic planes");
+        g.visc_L = L;
+    }
+    field_in(P_VX, vx);
+    field_in(P_VY, vy);
+    interior_in(P_SXX, sxx);
+    interior_in(P_SYY, syy);
+    interior_in(P_SXY, sxy);
+    tensor_in(0 * L, r);
+    tensor_in(1 * L, p);
+    tensor_in(2 * L, q);
+    tensor_in(3 * L, d);
+    tensor_in(4 * L, e);
+    tensor_in(5 * L, dip);
+    vinterior_in(6 * L + 0, fipjp);
+    vinterior_in(6 * L + 1, f);
+    vinterior_in(6 * L + 2, gg);
+    psi_in(0, psi_vxx);
+    psi_in(1, psi_vyx);
+    psi_in(2, psi_vyy);
+    psi_in(3, psi_vxy);
+    float *v12[12] = {K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half, b_y_half};
+    Inst I = base_inst(hc, v12);
+    I.mode = 0;
+    I.L = L;
+    I.plane = g.plane;
+    I.dhi_vi = 1.0 / DH;       // update_s_visc_PML_PSV.c: dhi = 1.0/DH, dthalbe = DT/2.0
+    I.dthalbe = DT / 2.0;
+    for (int l = 0; l < L; l++) {
+        I.bip[l] = bip[l + 1];
+        I.cip[l] = cip[l + 1];
+    }
+    I.r = vplane(0 * L);
+    I.p = vplane(1 * L);
+    I.q = vplane(2 * L);
+    I.pre_d = vplane(3 * L);
+    I.pre_e = vplane(4 * L);
+    I.pre_dip = vplane(5 * L);
+    I.pre_fipjp = vplane(6 * L + 0);
+    I.pre_f = vplane(6 * L + 1);
+    I.pre_g = vplane(6 * L + 2);
+    I.psi_vxx = psi_slot(0);
+    I.psi_vyx = psi_slot(1);
+    I.psi_vyy = psi_slot(2);
+    I.psi_vxy = psi_slot(3);
+    // one-column tiles of 128 x 8 cells
+    I.tiles_x = (NX + 127) / 128;
+    I.tiles = I.tiles_x * ((NY + 7) / 8);
+    cu(cudaMemcpy(g.d_inst, &I, sizeof(Inst), cudaMemcpyHostToDevice), "copy of the descriptor");
+    const dim3 grid(I.tiles, 1);
+    switch (L) {
+    case 1: launch_vi<1>(g.d_inst, grid); break;
+    case 2: launch_vi<2>(g.d_inst, grid); break;
+    case 3: launch_vi<3>(g.d_inst, grid); break;
+    case 4: launch_vi<4>(g.d_inst, grid); break;
+    default: launch_vi<5>(g.d_inst, grid); break;
+    }
+    cu(cudaGetLastError(), "update_s_visc_PML_PSV launch");
+    cu(cudaDeviceSynchronize(), "update_s_visc_PML_PSV");
+    interior_out(P_SXX, sxx);
+    interior_out(P_SYY, syy);
+    interior_out(P_SXY, sxy);
+    tensor_out(0 * L, r);
+    tensor_out(1 * L, p);
+    tensor_out(2 * L, q);
     psi_out(0, psi_vxx);
     psi_out(1, psi_vyx);
     psi_out(2, psi_vyy);

@@ -96,6 +96,9 @@ struct Inst {
     // stress kernels (explosive, QUELLTYP 1) instead of k_inject_v / k_inject_s
     int fsrc_v, fsrc_s;
     int rec_dup;                      // two receivers share a cell: adjoint sources added in list order
+    // prepared viscoelastic coefficients (the per-kernel drop-in of update_s_visc_PML_PSV,
+    // which receives them): fipjp, f, g planes and d, e, dip planes per mechanism at + l * plane
+    const float *pre_fipjp, *pre_f, *pre_g, *pre_d, *pre_e, *pre_dip;
     int f_w, f_tiles_x, f_zc, f_tiles;   // its tiles: f_w columns x f_zc rows
     float *vx_b, *vy_b, *sxx_b, *syy_b, *sxy_b;
     float *psi_sxx_x_b, *psi_sxy_x_b, *psi_syy_y_b, *psi_sxy_y_b;
@@ -962,9 +965,10 @@ __global__ void __launch_bounds__(128, DN_S2_MINB) k_update_s_el2(const Inst *__
 // ===========================================================================
 // Viscoelastic stress update: update_s_visc_PML_PSV.c (case 8 = :391-511).
 // fipjp, f, g, dip, d, e are regenerated per cell from the six relaxed-modulus
-// factors exactly as prepare_update_s_visc_PSV.c:52-62 forms them.
+// factors exactly as prepare_update_s_visc_PSV.c:52-62 forms them; the PRE
+// variant reads them prepared (Inst::pre_*), as the reference function takes them.
 // ===========================================================================
-template <int R, int L, bool X, bool SRC = false>
+template <int R, int L, bool X, bool SRC = false, bool PRE = false>
 __global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__ insts, const int *__restrict__ ntb, int off)
 {
     const Inst &I = insts[blockIdx.y];
@@ -1002,14 +1006,28 @@ __global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__
     VDeriv<R, X> D;
     D.prime(I, i, t.j0);
     float nm[6], ns[3], nr[L], np_[L], nq[L];
+    float npre[PRE ? 3 * L : 1];
     auto fetch = [&](int j) {
         const long long o = (long long)j * P;
-        nm[0] = __ldg(c_muipjp + o);
-        nm[1] = __ldg(c_tausipjp + o);
-        nm[2] = __ldg(c_mu + o);
-        nm[3] = __ldg(c_taus + o);
-        nm[4] = __ldg(c_pi + o);
-        nm[5] = __ldg(c_taup + o);
+        if constexpr (PRE) {   // nm[0..2]: the prepared fipjp, f, g
+            nm[3] = nm[4] = nm[5] = 0.0f;
+            nm[0] = __ldg(I.pre_fipjp + i + o);
+            nm[1] = __ldg(I.pre_f + i + o);
+            nm[2] = __ldg(I.pre_g + i + o);
+#pragma unroll
+            for (int l = 0; l < L; l++) {
+                npre[l] = __ldg(I.pre_dip + i + o + l * PL);
+                npre[L + l] = __ldg(I.pre_d + i + o + l * PL);
+                npre[2 * L + l] = __ldg(I.pre_e + i + o + l * PL);
+            }
+        } else {
+            nm[0] = __ldg(c_muipjp + o);
+            nm[1] = __ldg(c_tausipjp + o);
+            nm[2] = __ldg(c_mu + o);
+            nm[3] = __ldg(c_taus + o);
+            nm[4] = __ldg(c_pi + o);
+            nm[5] = __ldg(c_taup + o);
+        }
         ns[0] = sxxp[o];
         ns[1] = syyp[o];
         ns[2] = sxyp[o];
@@ -1027,11 +1045,16 @@ __global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__
         const float muipjp = nm[0], tsij = nm[1], mu = nm[2], taus = nm[3], pi = nm[4], taup = nm[5];
         const float s_xx = ns[0], s_yy = ns[1], s_xy = ns[2];
         float rr[L], pp[L], qq[L];
+        float pre[PRE ? 3 * L : 1];
 #pragma unroll
         for (int l = 0; l < L; l++) {
             rr[l] = nr[l];
             pp[l] = np_[l];
             qq[l] = nq[l];
+        }
+        if constexpr (PRE) {
+#pragma unroll
+            for (int k = 0; k < 3 * L; k++) pre[k] = npre[k];
         }
         if (j < t.j1) {
             D.fetch(j + 1);
@@ -1040,9 +1063,9 @@ __global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__
         float vxx, vyx, vxy, vyy;
         D.compute(I, hc, i, j, dhi, vxx, vyx, vxy, vyy);
         const long long o = (long long)j * P;
-        const float fipjp = F(DMUL((double)__fmul_rn(muipjp, DT), DADD(1.0, (double)__fmul_rn(fL, tsij))));
-        const float f = F(DMUL((double)__fmul_rn(mu, DT), DADD(1.0, (double)__fmul_rn(fL, taus))));
-        const float g = F(DMUL((double)__fmul_rn(pi, DT), DADD(1.0, (double)__fmul_rn(fL, taup))));
+        const float fipjp = PRE ? muipjp : F(DMUL((double)__fmul_rn(muipjp, DT), DADD(1.0, (double)__fmul_rn(fL, tsij))));
+        const float f = PRE ? tsij : F(DMUL((double)__fmul_rn(mu, DT), DADD(1.0, (double)__fmul_rn(fL, taus))));
+        const float g = PRE ? mu : F(DMUL((double)__fmul_rn(pi, DT), DADD(1.0, (double)__fmul_rn(fL, taup))));
         float sumr = 0.0f, sump = 0.0f, sumq = 0.0f;
 #pragma unroll
         for (int l = 0; l < L; l++) {
@@ -1060,9 +1083,9 @@ __global__ void __launch_bounds__(256, 3) k_update_s_vi(const Inst *__restrict__
         sumr = sump = sumq = 0.0f;
 #pragma unroll
         for (int l = 0; l < L; l++) {
-            const float dip = MUL<X>(MUL<X>(muipjp, eta[l]), tsij);
-            const float dd = MUL<X>(MUL<X>(mu, eta[l]), taus);
-            const float ee = MUL<X>(MUL<X>(pi, eta[l]), taup);
+            const float dip = PRE ? pre[l] : MUL<X>(MUL<X>(muipjp, eta[l]), tsij);
+            const float dd = PRE ? pre[L + l] : MUL<X>(MUL<X>(mu, eta[l]), taus);
+            const float ee = PRE ? pre[2 * L + l] : MUL<X>(MUL<X>(pi, eta[l]), taup);
             const float r = MUL<X>(bip[l], SUB<X>(MUL<X>(rr[l], cip[l]), MUL<X>(dip, sh)));
             const double d2 = 2.0 * (double)dd;
             const float pv = F(DMUL((double)bip[l], DADD((double)SUB<X>(MUL<X>(pp[l], cip[l]), MUL<X>(ee, dv)), DMUL(d2, (double)vyy))));

@@ -51,7 +51,8 @@ def test_model_validation_without_gpu(bad, code):
 
 
 def test_kernel_shim_library_loads_beside_the_reference():
-    """lib/libdenise_b200_fd.so defines update_v_PML_PSV and update_s_elastic_PML_PSV;
+    """lib/libdenise_b200_fd.so defines update_v_PML_PSV, update_s_elastic_PML_PSV and
+    update_s_visc_PML_PSV;
     its references to the reference's globals and err() resolve in a process that
     holds the reference (here, its build)."""
     import oracles as O
@@ -62,4 +63,5 @@ def test_kernel_shim_library_loads_beside_the_reference():
         pytest.skip("the reference build (oracle/_ref) is not there")
     ctypes.CDLL(O.REF_SO, mode=ctypes.RTLD_GLOBAL)
     lib = ctypes.CDLL(shim)
-    assert hasattr(lib, "update_v_PML_PSV") and hasattr(lib, "update_s_elastic_PML_PSV")
+    for name in ("update_v_PML_PSV", "update_s_elastic_PML_PSV", "update_s_visc_PML_PSV"):
+        assert hasattr(lib, name)
